@@ -1,0 +1,208 @@
+/* me_b200.h -- C ABI of the B200 Milne-Eddington Stokes inversion library.
+ *
+ * Drop-in replacement for the per-pixel inversion of the reference
+ * (HaoLi-70/Milne-Eddington).  Every entry point names the reference function it
+ * replaces.  Conventions:
+ *   - status 0 = OK, negative = error (see me_strerror); nothing aborts;
+ *   - the caller owns host buffers, a plan owns its device memory and stream;
+ *   - one plan per host thread (a plan is not thread-safe);
+ *   - parameter order and units are the reference's Par[0..8]
+ *     (Src/ME_SOLVER.c:121-122): B [G], theta_B [rad], phi_B [rad], v_los [km/s],
+ *     Doppler width [mA], damping a, eta0, S0+S1, beta = S0/(S0+S1);
+ *   - profiles are pixel-major [pixel][I,Q,U,V][lambda] doubles and results
+ *     [pixel][10] doubles (9 parameters then chi^2, zeros for skipped pixels),
+ *     exactly the reference's profbuff/resbuff layout (Src/LM_FIT.c:767-808).
+ */
+#ifndef ME_B200_H
+#define ME_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ME_MAX_LINES 20   /* Src/RINPUT.h:15 NUM_LINES */
+#define ME_PATH_LEN 512   /* Src/STR.h:15 Max_Line_Length */
+#define ME_MAX_NL 512     /* largest wavelength grid a plan accepts */
+
+/* status codes */
+#define ME_OK 0
+#define ME_ERR_ARG -1        /* bad argument (null pointer, size out of range) */
+#define ME_ERR_CONFIG -2     /* control file missing keyword / malformed value */
+#define ME_ERR_IO -3         /* file could not be opened / read / written */
+#define ME_ERR_CUDA -4       /* CUDA runtime error */
+#define ME_ERR_NODEVICE -5   /* no CUDA device: the library has no CPU fallback */
+#define ME_ERR_TIMEOUT -6    /* device work exceeded its iteration budget */
+#define ME_ERR_NOMEM -7      /* allocation failed */
+#define ME_ERR_FORMAT -8     /* unsupported file format (FITS) */
+
+/* precision of the synthesis / Jacobian / normal equations on the device.
+ * The 9x9 SVD solve and the chi^2 accept test are FP64 in both modes. */
+#define ME_PREC_FP32 0
+#define ME_PREC_FP64 1
+
+/* Parsed control file.  Field meanings and defaults are the reference's
+ * keyword table (Src/RINPUT.c:400-458) after Get_Keys' unit handling
+ * (Src/RINPUT.c:48-357): Bounds_Btheta / Bounds_Bphi and the theta/phi
+ * regularisation targets are stored in radians (x pi). */
+typedef struct me_config {
+  int nline;                          /* `lines` repeats; only line 0 is used (Src/ME_SOLVER.c:131) */
+  double line_lambda0[ME_MAX_LINES];  /* [A] */
+  double line_geff[ME_MAX_LINES];
+  int verbose;                        /* verbose            (default 1)    */
+  int num_iter;                       /* num_iter           (60)           */
+  int num_run;                        /* num_run            (4)            */
+  double convg_criteria;              /* convg_criteria     (1e-3)         */
+  double chisq_criteria;              /* chisq_criteria     (1.0)          */
+  char data_path[ME_PATH_LEN];        /* data_path          (required)     */
+  char wavelength_path[ME_PATH_LEN];  /* wavelength_path    (required)     */
+  double weights[4];                  /* weights            (1,1,1,1)      */
+  int sol_box[4];                     /* sol_box x0,x1,y0,y1 (-1,-1,-1,-1) */
+  int output_fit;                     /* output_fit         (NO)           */
+  char cache_path[ME_PATH_LEN];       /* cache_path         (./cache)      */
+  char result_path[ME_PATH_LEN];      /* result_path        (./res.fits)   */
+  char fit_path[ME_PATH_LEN];         /* fit_path           (./fit.fits)   */
+  double damp;                        /* damp               (1e-3)         */
+  double lambda_accept;               /* lambda_accept      (5.0)          */
+  double lambda_reject;               /* lambda_reject      (5.0)          */
+  double lambda_limits[2];            /* lambda_limits      (1e-5, 1e3)    */
+  double bounds[9][2];                /* Bounds_*           (see table)    */
+  int fixed[9];                       /* *_fixed            (NO)           */
+  int regul[9];                       /* *_Regularization   (theta: YES)   */
+  double regul_value[9];
+  double regul_weight[9];
+  int regul_any;                      /* any regul[] set (Input->Regul)    */
+  double vcoeffi;                     /* VCoeffi            (100)          */
+  double lcoeffi;                     /* LCoeffi            (250)          */
+  double icriteria;                   /* Icriteria          (100)          */
+  double svd_threshold;               /* SVDthreshold       (1e-6)         */
+  int hmi_ref;                        /* HMI_REF            (No)           */
+  int cache_prof;                     /* Cache_prof         (No)           */
+  int nthreads;                       /* Nthreads           (4, unused)    */
+  int nfigures;                       /* Nfigures           (6)            */
+  double step[9];                     /* Step    (1000,2,2,2,20,0.3,30,1e5,0.3) */
+  int nprofiles;                      /* nprofiles          (20)           */
+  int cache_inv;                      /* Cache_inv          (No)           */
+  /* --- keywords of this library (not in the reference) --- */
+  int precision;                      /* precision = FP32 | FP64 (FP32)    */
+  unsigned long long rng_seed;        /* rng_seed (0): key of the per-(pixel, run) draws */
+  int lines_seen;                     /* bookkeeping: `lines` present      */
+  int data_path_seen, wavelength_path_seen;
+} me_config;
+
+/* Facts INIT_INV derives from the grid (Src/INV_INIT.c:121-177). */
+typedef struct me_plan_facts {
+  int nl, ncut, ic, i0, i1, npar;
+  double bshift;           /* 4.6686e-10 * g * lambda0^2 [mA/G] */
+  double limits[9][2];     /* after INIT_INV's v_los clip       */
+  double fadd_a;           /* Alg-916 spacing a for Nfigures    */
+} me_plan_facts;
+
+/* Counters of one me_invert_batch call (device-side event counts). */
+typedef struct me_stats {
+  long long pixels;        /* pixels in the batch                          */
+  long long valid;         /* pixels inverted (not skipped by the I gate)  */
+  long long runs;          /* LM_FIT runs (restarts included)              */
+  long long iterations;    /* LM iterations                                */
+  long long trials;        /* trial steps = SVD solves                     */
+  long long accepted;      /* accepted trials                              */
+  long long syntheses;     /* forward syntheses (trials)                   */
+  long long jacobians;     /* syntheses with Jacobian + normal equations   */
+  long long wavelengths;   /* wavelength points synthesised (both kinds)   */
+  long long redo_pixels;   /* pixels re-run to honour the carried LM chi^2 */
+  double kernel_ms;        /* device time of the inversion kernel(s)       */
+  double h2d_ms, d2h_ms;   /* host<->device copy time (host entry point)   */
+} me_stats;
+
+typedef struct me_plan me_plan;
+
+const char *me_version(void);
+const char *me_strerror(int status);
+/* Message of the last failure on the calling thread ("" if none). */
+const char *me_last_error(void);
+
+/* Defaults of every keyword.  Replaces the default table of RDINPUT
+ * (Src/RINPUT.c:400-458). */
+int me_config_init(me_config *cfg);
+
+/* Reads a control file (`key = value`, comments `#`/`!`/`*`, inline `!`) with
+ * the reference's keyword semantics.  Replaces RDINPUT + Get_Keys
+ * (Src/RINPUT.c:361-563, 48-357).  Unlike the reference it does not check that
+ * data_path / wavelength_path exist (the FITS entry points do), and reports
+ * malformed values as ME_ERR_CONFIG instead of exiting.  `errbuf` (may be
+ * NULL) receives a one-line message. */
+int me_config_parse(const char *ctl_path, me_config *cfg, char *errbuf, size_t errlen);
+int me_config_parse_text(const char *text, me_config *cfg, char *errbuf, size_t errlen);
+
+/* Builds a plan for one wavelength grid on CUDA device `device`: line
+ * constants, ncut/ic/i0/i1, v_los clip, Faddeeva constants, device buffers.
+ * Replaces INIT_INV (Src/INV_INIT.c:86-289).  Returns ME_ERR_NODEVICE when no
+ * GPU is visible (there is no CPU path). */
+int me_plan_create(const me_config *cfg, const double *lambda, int nl, int device,
+                   me_plan **out);
+void me_plan_destroy(me_plan *plan);
+int me_plan_get_facts(const me_plan *plan, me_plan_facts *out);
+
+/* The reference carries LM->chisq (the chi^2 of the last trial step) from one
+ * pixel to the next inside a process and uses it in the first regularisation
+ * ratio test of the next pixel (Src/LM_FIT.c:555-559).  A plan carries it the
+ * same way across pixels and batches; it starts at 0 (STRUCT_LM LM = {0},
+ * Src/ME_INV.c:91).  These read / reset it. */
+double me_plan_get_carry_chisq(const me_plan *plan);
+void me_plan_set_carry_chisq(me_plan *plan, double chisq);
+
+/* Persistent-grid size (CTAs) of the inversion kernel; set_grid overrides the
+ * occupancy-derived default (used by the autotuner and the benchmarks). */
+int me_plan_grid(const me_plan *plan);
+void me_plan_set_grid(me_plan *plan, int grid);
+
+/* Inverts npix pixels.  prof: host [npix][4][nl]; res: host [npix][10];
+ * fit: host [npix][4][nl] or NULL (best-fit profiles, zeros when skipped);
+ * stats may be NULL.  Replaces INVERSION_MULTI (Src/LM_FIT.c:746-811). */
+int me_invert_batch(me_plan *plan, const double *prof, long npix, double *res,
+                    double *fit, me_stats *stats);
+
+/* Same on device buffers (d_prof, d_res, d_fit device pointers; d_fit may be
+ * NULL); work is ordered on `stream` (a cudaStream_t, NULL = the plan's). */
+int me_invert_batch_device(me_plan *plan, const double *d_prof, long npix,
+                           double *d_res, double *d_fit, void *stream,
+                           me_stats *stats);
+
+/* Forward Stokes synthesis for npix parameter vectors par [npix][9] into
+ * prof [npix][4][nl] (host buffers).  Replaces Milne_Eddington_Single with
+ * Deriv=false (Src/ME_SOLVER.c:101-366). */
+int me_synthesize(me_plan *plan, const double *par, long npix, double *prof);
+
+/* Forward synthesis on device buffers d_par [npix][9] -> d_prof [npix][4][nl],
+ * ordered on `stream` (NULL = the plan's stream, waited for). */
+int me_synthesize_device(me_plan *plan, const double *d_par, long npix, double *d_prof,
+                         void *stream);
+
+/* Synthesis with the step-scaled analytic Jacobian (Deriv=true).  jac is
+ * [npix][4][9][nl] (the reference's Stk->Jacobian layout, Src/ME_SOLVER.c:169-177);
+ * step7 is the S step (Init_Guess sets 0.1*I_max per pixel). */
+int me_synthesize_jacobian(me_plan *plan, const double *par, long npix, double step7,
+                           double *prof, double *jac);
+
+/* Voigt H and Faraday-Voigt L for n (nu, a) pairs at accuracy Nfigures, on
+ * the device, in the given precision (ME_PREC_*).  Replaces Faddeeva
+ * (Src/FADDEEVA.c:440-590). */
+int me_faddeeva(int nfigures, int precision, const double *nu, const double *a, long n,
+                double *H, double *L, int device);
+
+/* Golub-Reinsch SVD of nmat n x n matrices (n <= 9) in FP64 on the device:
+ * a = u * diag(w) * v^T.  Replaces svdcmp_double (Src/SVD_TEMPLATE.h:84-344). */
+int me_svd(const double *a, long nmat, int n, double *u, double *w, double *v, int device);
+
+/* Initial guess for npix profiles: guess [npix][9]; extra [npix][5] =
+ * norm0, normp, S lower limit, S upper limit, S step; status [npix] (0 ok,
+ * 1 below Icriteria).  Replaces Init_Guess (Src/ME_SOLVER.c:445-676). */
+int me_init_guess(me_plan *plan, const double *prof, long npix, double *guess,
+                  double *extra, int *status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ME_B200_H */

@@ -1,0 +1,561 @@
+// me_api.cu -- host side of the C ABI (include/me_b200.h): plans, batches,
+// and the unit entry points.  No CPU compute path: every entry point that
+// computes runs CUDA kernels and fails with ME_ERR_NODEVICE without a GPU.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/me_b200.h"
+#include "me_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(ME_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+int check_device(int device) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(ME_ERR_NODEVICE, "no CUDA device visible: this library has no CPU path");
+  if (device < 0 || device >= n) return fail(ME_ERR_ARG, "device index out of range");
+  CK(cudaSetDevice(device));
+  return ME_OK;
+}
+
+// Device buffer that grows on demand.
+struct DevBuf {
+  void *p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+// Alg-916 constants of Faddeeva_init (Src/FADDEEVA.c:406-436) and the region
+// row of the accuracy table (Src/FADDEEVA.c:471-477).
+void fill_voigt_consts(me::DevPlan &P, int nfigures) {
+  static const double T[5][5] = {{1.6e4, 160.0, 107.0, 28.5, 3.5},
+                                 {1.5e5, 510.0, 110.0, 39., -0.1},
+                                 {1.451e6, 1.6e3, 180.0, 110.0, -0.1},
+                                 {1.5e7, 5.01e3, 380.0, 115.0, 114.0},
+                                 {1.3e8, 1.6e4, 810.0, 195.0, 116.0}};
+  P.nfigures = nfigures;
+  const double rmin0 = pow(10., -nfigures);
+  P.fa = M_PI / sqrt(-log(0.5 * rmin0));
+  P.faa = P.fa * P.fa;
+  P.flog_rmin0 = -log(rmin0);
+  P.fsqrt_log_rmin0 = sqrt(P.flog_rmin0);
+  P.fnmax = 50;
+  P.row = nfigures > 4 ? nfigures - 4 : 0;
+  P.exp_a2n2[0] = 1.;
+  for (int i = 1; i < 50; i++) P.exp_a2n2[i] = exp(-P.faa * i * i);
+  for (int i = 0; i < 5; i++) P.thr[i] = T[P.row][i];
+}
+
+}  // namespace
+
+struct me_plan {
+  me_config cfg;
+  me::DevPlan P;
+  me_plan_facts facts;
+  int device = 0;
+  int precision = ME_PREC_FP32;
+  int grid = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double carry = 0.0;  // LM->chisq carried between pixels (STRUCT_LM LM = {0})
+  DevBuf d_lambda, d_dlambda;
+  DevBuf d_prof, d_res, d_fit;  // staging of the host entry point
+  DevBuf d_flags, d_pen0, d_lastchi, d_counters, d_totals, d_next, d_stale, d_list;
+  std::vector<unsigned char> h_flags;
+  std::vector<double> h_pen0, h_lastchi, h_stale, h_used;
+  std::vector<long long> h_list;
+};
+
+extern "C" const char *me_version(void) { return "me_b200 0.1 (sm_100a)"; }
+
+extern "C" const char *me_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" const char *me_strerror(int status) {
+  switch (status) {
+    case ME_OK: return "ok";
+    case ME_ERR_ARG: return "invalid argument";
+    case ME_ERR_CONFIG: return "invalid control file";
+    case ME_ERR_IO: return "I/O error";
+    case ME_ERR_CUDA: return "CUDA error";
+    case ME_ERR_NODEVICE: return "no CUDA device (no CPU fallback)";
+    case ME_ERR_TIMEOUT: return "device work exceeded its budget";
+    case ME_ERR_NOMEM: return "out of memory";
+    case ME_ERR_FORMAT: return "unsupported file format";
+    default: return "unknown status";
+  }
+}
+
+extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl, int device,
+                              me_plan **out) {
+  if (!cfg || !lambda || !out) return fail(ME_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (nl < 4 || nl > ME_MAX_NL) return fail(ME_ERR_ARG, "nl must be in [4, 512]");
+  if (cfg->nline < 1) return fail(ME_ERR_CONFIG, "no spectral line (keyword lines)");
+  if (cfg->nfigures > 8) return fail(ME_ERR_CONFIG, "Nfigures above 8 has no accuracy row");
+  // the trial loop of an LM iteration ends only when the damping passes its
+  // upper limit (Src/LM_FIT.c:144-150)
+  if (!(cfg->damp > 0) || !(cfg->lambda_reject > 1) || !isfinite(cfg->lambda_limits[1]))
+    return fail(ME_ERR_CONFIG, "damp must be > 0, lambda_reject > 1, lambda_limits finite");
+  int st = check_device(device);
+  if (st) return st;
+
+  me_plan *p = new me_plan();
+  p->cfg = *cfg;
+  p->device = device;
+  p->precision = cfg->precision == ME_PREC_FP64 ? ME_PREC_FP64 : ME_PREC_FP32;
+  me::DevPlan &P = p->P;
+  memset(&P, 0, sizeof(P));
+  // INIT_INV (Src/INV_INIT.c:112-201)
+  const double lam0 = cfg->line_lambda0[0];
+  P.nl = nl;
+  P.lambda0 = lam0;
+  P.bshift = 4.6686e-10 * cfg->line_geff[0] * lam0 * lam0;
+  P.npar = 0;
+  for (int i = 0; i < 9; i++) {
+    P.fixed[i] = cfg->fixed[i] ? 1 : 0;
+    if (!P.fixed[i]) P.free_idx[P.npar++] = i;
+    P.limits[i][0] = cfg->bounds[i][0];
+    P.limits[i][1] = cfg->bounds[i][1];
+    P.step[i] = cfg->step[i];
+    P.regul[i] = cfg->regul[i] ? 1 : 0;
+    P.regul_value[i] = cfg->regul_value[i];
+    P.regul_weight[i] = cfg->regul_weight[i];
+  }
+  if (P.npar == 0) {
+    delete p;
+    return fail(ME_ERR_CONFIG, "all nine parameters are fixed");
+  }
+  P.ncut = nl / 5;
+  const double c = 299792458.0;
+  double t = (lambda[P.ncut] - lam0) * c / 1e3;  // the reference omits /lambda0 here
+  if (P.limits[3][0] < t) P.limits[3][0] = t;
+  t = (lambda[nl - 1 - P.ncut] - lam0) * c / 1e3;
+  if (P.limits[3][1] > t) P.limits[3][1] = t;
+  // line-centre index by the reference's boolean arithmetic (Src/INV_INIT.c:150-156):
+  // in practice the last iw < nl-1 with lambda[iw] < lambda0; 0 when none.
+  P.ic = 0;
+  for (int iw = 0; iw < nl - 1; iw++) {
+    const double t1 = lam0 > lambda[iw];
+    const double t2 = lambda[iw + 1] * lam0;
+    if (t1 > 0 && t2 > 0) P.ic = t1 < t2 ? iw : iw + 1;
+  }
+  int r1 = 2, r2 = 2;
+  if (P.ic - P.ncut >= 2) r1 = P.ic - P.ncut;
+  if (nl - 1 - P.ncut - P.ic >= 2) r2 = nl - 1 - P.ncut - P.ic;
+  int range = r1 > r2 ? r1 : r2;
+  P.i0 = P.ic - range;
+  if (P.i0 < 0) {
+    P.i0 = 0;
+    range = P.ic - P.i0;
+  }
+  P.i1 = P.ic + range;
+  if (P.i1 > nl - 1) {
+    P.i1 = nl - 1;
+    range = P.i1 - P.ic;
+    P.i0 = P.ic - range;
+  }
+  for (int s = 0; s < 4; s++) {
+    P.weights[s] = cfg->weights[s];
+    P.w2[s] = cfg->weights[s] * cfg->weights[s];
+  }
+  P.icriteria = cfg->icriteria;
+  P.convg = cfg->convg_criteria;
+  P.chisq_crit = cfg->chisq_criteria;
+  P.damp = cfg->damp;
+  P.lam_accept = cfg->lambda_accept;
+  P.lam_reject = cfg->lambda_reject;
+  P.lam_lim[0] = cfg->lambda_limits[0];
+  P.lam_lim[1] = cfg->lambda_limits[1];
+  P.svd_thr = cfg->svd_threshold;
+  P.vcoeffi = cfg->vcoeffi;
+  P.lcoeffi = cfg->lcoeffi;
+  P.niter = cfg->num_iter;
+  P.nruns = cfg->num_run;
+  P.hmi_ref = cfg->hmi_ref ? 1 : 0;
+  P.regul_any = cfg->regul_any ? 1 : 0;
+  P.seed = cfg->rng_seed;
+  fill_voigt_consts(P, cfg->nfigures);
+
+  std::vector<double> dl(nl);
+  for (int i = 0; i < nl; i++) dl[i] = lambda[i] - lam0;
+  if (p->d_lambda.ensure(sizeof(double) * nl) || p->d_dlambda.ensure(sizeof(double) * nl) ||
+      p->d_totals.ensure(sizeof(unsigned long long) * 8) ||
+      p->d_next.ensure(sizeof(unsigned long long)) ||
+      cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) ||
+      cudaEventCreate(&p->ev0) || cudaEventCreate(&p->ev1) ||
+      cudaMemcpy(p->d_lambda.p, lambda, sizeof(double) * nl, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(p->d_dlambda.p, dl.data(), sizeof(double) * nl, cudaMemcpyHostToDevice)) {
+    me_plan_destroy(p);
+    return fail(ME_ERR_CUDA, "plan allocation failed");
+  }
+  P.lambda = p->d_lambda.as<double>();
+  P.dlambda = p->d_dlambda.as<double>();
+  p->grid = me::invert_grid(p->precision, device);
+
+  me_plan_facts &f = p->facts;
+  f.nl = nl;
+  f.ncut = P.ncut;
+  f.ic = P.ic;
+  f.i0 = P.i0;
+  f.i1 = P.i1;
+  f.npar = P.npar;
+  f.bshift = P.bshift;
+  memcpy(f.limits, P.limits, sizeof(f.limits));
+  f.fadd_a = P.fa;
+  *out = p;
+  return ME_OK;
+}
+
+extern "C" void me_plan_destroy(me_plan *p) {
+  if (!p) return;
+  cudaSetDevice(p->device);
+  DevBuf *bufs[] = {&p->d_lambda, &p->d_dlambda, &p->d_prof,     &p->d_res,
+                    &p->d_fit,    &p->d_flags,   &p->d_pen0,     &p->d_lastchi,
+                    &p->d_counters, &p->d_totals, &p->d_next,    &p->d_stale,
+                    &p->d_list};
+  for (DevBuf *b : bufs) b->release();
+  if (p->ev0) cudaEventDestroy(p->ev0);
+  if (p->ev1) cudaEventDestroy(p->ev1);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+}
+
+extern "C" int me_plan_get_facts(const me_plan *p, me_plan_facts *out) {
+  if (!p || !out) return ME_ERR_ARG;
+  *out = p->facts;
+  return ME_OK;
+}
+
+extern "C" double me_plan_get_carry_chisq(const me_plan *p) { return p ? p->carry : 0.0; }
+extern "C" void me_plan_set_carry_chisq(me_plan *p, double v) {
+  if (p) p->carry = v;
+}
+
+extern "C" int me_plan_grid(const me_plan *p) { return p ? p->grid : 0; }
+extern "C" void me_plan_set_grid(me_plan *p, int grid) {
+  if (p && grid > 0) p->grid = grid;
+}
+
+extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npix, double *d_res,
+                                      double *d_fit, void *stream, me_stats *stats) {
+  if (!p || !d_prof || !d_res || npix < 0) return fail(ME_ERR_ARG, "null argument");
+  CK(cudaSetDevice(p->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (npix == 0) return ME_OK;
+  const size_t n = (size_t)npix;
+  CK(p->d_flags.ensure(n));
+  CK(p->d_pen0.ensure(n * sizeof(double)));
+  CK(p->d_lastchi.ensure(n * sizeof(double)));
+  CK(p->d_counters.ensure(n * 4 * sizeof(unsigned int)));
+  CK(cudaMemsetAsync(p->d_totals.p, 0, 8 * sizeof(unsigned long long), st));
+
+  me::InvertArgs A;
+  memset(&A, 0, sizeof(A));
+  A.prof = d_prof;
+  A.res = d_res;
+  A.fit = d_fit;
+  A.flags = p->d_flags.as<unsigned char>();
+  A.penalty0 = p->d_pen0.as<double>();
+  A.lastchi = p->d_lastchi.as<double>();
+  A.counters = p->d_counters.as<unsigned int>();
+  A.totals = p->d_totals.as<unsigned long long>();
+  A.next = p->d_next.as<unsigned long long>();
+  A.list = nullptr;
+  A.count = npix;
+  A.stale = nullptr;
+  A.carry = p->carry;
+  A.first_pixel = 0;
+
+  CK(cudaMemsetAsync(A.next, 0, sizeof(unsigned long long), st));
+  CK(cudaEventRecord(p->ev0, st));
+  CK(me::launch_invert(p->precision, p->P, A, p->grid, st));
+  CK(cudaEventRecord(p->ev1, st));
+
+  // The reference carries LM->chisq from pixel to pixel; it enters only the
+  // first regularisation ratio test of each pixel (Src/LM_FIT.c:555-559).  The
+  // launch above assumed the carried value for pixel 0 and "no ratio change"
+  // for every later pixel; pixels for which the true carried value (the last
+  // trial chi^2 of the previous inverted pixel) flips that test are re-run,
+  // until no flip remains.
+  p->h_flags.resize(n);
+  p->h_pen0.resize(n);
+  p->h_lastchi.resize(n);
+  CK(cudaMemcpyAsync(p->h_flags.data(), A.flags, n, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(p->h_lastchi.data(), A.lastchi, n * sizeof(double), cudaMemcpyDeviceToHost,
+                     st));
+  if (p->P.regul_any)
+    CK(cudaMemcpyAsync(p->h_pen0.data(), A.penalty0, n * sizeof(double), cudaMemcpyDeviceToHost,
+                       st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+  double kernel_ms = ms;
+  long long redo_total = 0;
+  p->h_used.assign(n, INFINITY);
+  if (n) p->h_used[0] = p->carry;
+  for (int pass = 0; pass < 1 << 20; pass++) {
+    double prev = p->carry;
+    p->h_list.clear();
+    for (size_t i = 0; i < n; i++) {
+      if (!(p->h_flags[i] & 1)) continue;
+      if (p->P.regul_any) {
+        const bool want = p->h_pen0[i] > 0.1 * prev;
+        const bool used = p->h_pen0[i] > 0.1 * p->h_used[i];
+        if (want != used) {
+          p->h_list.push_back((long long)i);
+          p->h_used[i] = prev;
+        }
+      }
+      if (p->h_flags[i] & 2) prev = p->h_lastchi[i];
+    }
+    if (p->h_list.empty()) {
+      p->carry = prev;
+      break;
+    }
+    redo_total += (long long)p->h_list.size();
+    const size_t m = p->h_list.size();
+    CK(p->d_list.ensure(m * sizeof(long long)));
+    CK(p->d_stale.ensure(n * sizeof(double)));
+    CK(cudaMemcpyAsync(p->d_list.p, p->h_list.data(), m * sizeof(long long),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(p->d_stale.p, p->h_used.data(), n * sizeof(double), cudaMemcpyHostToDevice,
+                       st));
+    me::InvertArgs B = A;
+    B.list = p->d_list.as<long long>();
+    B.count = (long long)m;
+    B.stale = p->d_stale.as<double>();
+    CK(cudaMemsetAsync(B.next, 0, sizeof(unsigned long long), st));
+    CK(cudaEventRecord(p->ev0, st));
+    const int g = (int)((m + me::kInvertBlock - 1) / me::kInvertBlock);
+    CK(me::launch_invert(p->precision, p->P, B, g < p->grid ? g : p->grid, st));
+    CK(cudaEventRecord(p->ev1, st));
+    CK(cudaMemcpyAsync(p->h_flags.data(), A.flags, n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(p->h_lastchi.data(), A.lastchi, n * sizeof(double),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+    kernel_ms += ms;
+  }
+  if (stats) {
+    unsigned long long tot[8];
+    CK(cudaMemcpy(tot, A.totals, sizeof(tot), cudaMemcpyDeviceToHost));
+    stats->pixels = npix;
+    stats->valid = (long long)tot[0];
+    stats->runs = (long long)tot[1];
+    stats->iterations = (long long)tot[2];
+    stats->trials = (long long)tot[3];
+    stats->accepted = (long long)tot[4];
+    stats->syntheses = (long long)tot[3];
+    stats->jacobians = (long long)tot[5];
+    stats->wavelengths = (long long)(tot[3] + tot[5]) * p->P.nl;
+    stats->redo_pixels = redo_total;
+    stats->kernel_ms = kernel_ms;
+  }
+  return ME_OK;
+}
+
+extern "C" int me_invert_batch(me_plan *p, const double *prof, long npix, double *res, double *fit,
+                               me_stats *stats) {
+  if (!p || !prof || !res || npix < 0) return fail(ME_ERR_ARG, "null argument");
+  if (npix == 0) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    return ME_OK;
+  }
+  CK(cudaSetDevice(p->device));
+  const size_t n = (size_t)npix;
+  const size_t pbytes = n * 4 * p->P.nl * sizeof(double);
+  CK(p->d_prof.ensure(pbytes));
+  CK(p->d_res.ensure(n * 10 * sizeof(double)));
+  if (fit) CK(p->d_fit.ensure(pbytes));
+  cudaEvent_t e0, e1, e2, e3;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventCreate(&e2);
+  cudaEventCreate(&e3);
+  cudaEventRecord(e0, p->stream);
+  CK(cudaMemcpyAsync(p->d_prof.p, prof, pbytes, cudaMemcpyHostToDevice, p->stream));
+  cudaEventRecord(e1, p->stream);
+  int rc = me_invert_batch_device(p, p->d_prof.as<double>(), npix, p->d_res.as<double>(),
+                                  fit ? p->d_fit.as<double>() : nullptr, p->stream, stats);
+  if (rc == ME_OK) {
+    cudaEventRecord(e2, p->stream);
+    cudaError_t e = cudaMemcpyAsync(res, p->d_res.p, n * 10 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, p->stream);
+    if (e == cudaSuccess && fit)
+      e = cudaMemcpyAsync(fit, p->d_fit.p, pbytes, cudaMemcpyDeviceToHost, p->stream);
+    cudaEventRecord(e3, p->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) rc = fail(ME_ERR_CUDA, cudaGetErrorString(e));
+    if (rc == ME_OK && stats) {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, e0, e1);
+      cudaEventElapsedTime(&b, e2, e3);
+      stats->h2d_ms = a;
+      stats->d2h_ms = b;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  cudaEventDestroy(e3);
+  return rc;
+}
+
+extern "C" int me_synthesize_jacobian(me_plan *p, const double *par, long npix, double step7,
+                                      double *prof, double *jac) {
+  if (!p || !par || !prof || npix < 0) return fail(ME_ERR_ARG, "null argument");
+  if (npix == 0) return ME_OK;
+  CK(cudaSetDevice(p->device));
+  const size_t n = (size_t)npix, nl = (size_t)p->P.nl;
+  DevBuf dp, dprof, djac;
+  CK(dp.ensure(n * 9 * sizeof(double)));
+  CK(dprof.ensure(n * 4 * nl * sizeof(double)));
+  if (jac) CK(djac.ensure(n * 36 * nl * sizeof(double)));
+  CK(cudaMemcpyAsync(dp.p, par, n * 9 * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  CK(me::launch_synth(p->precision, p->P, dp.as<double>(), npix, step7, dprof.as<double>(),
+                      jac ? djac.as<double>() : nullptr, p->stream));
+  CK(cudaMemcpyAsync(prof, dprof.p, n * 4 * nl * sizeof(double), cudaMemcpyDeviceToHost,
+                     p->stream));
+  if (jac)
+    CK(cudaMemcpyAsync(jac, djac.p, n * 36 * nl * sizeof(double), cudaMemcpyDeviceToHost,
+                       p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  dp.release();
+  dprof.release();
+  djac.release();
+  return ME_OK;
+}
+
+extern "C" int me_synthesize(me_plan *p, const double *par, long npix, double *prof) {
+  return me_synthesize_jacobian(p, par, npix, p ? p->P.step[7] : 0.0, prof, nullptr);
+}
+
+extern "C" int me_synthesize_device(me_plan *p, const double *d_par, long npix, double *d_prof,
+                                    void *stream) {
+  if (!p || !d_par || !d_prof || npix < 0) return fail(ME_ERR_ARG, "null argument");
+  CK(cudaSetDevice(p->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+  CK(me::launch_synth(p->precision, p->P, d_par, npix, p->P.step[7], d_prof, nullptr, st));
+  if (!stream) CK(cudaStreamSynchronize(st));
+  return ME_OK;
+}
+
+extern "C" int me_faddeeva(int nfigures, int precision, const double *nu, const double *a, long n,
+                           double *H, double *L, int device) {
+  if (!nu || !a || !H || !L || n < 0 || nfigures > 8) return fail(ME_ERR_ARG, "bad argument");
+  int st = check_device(device);
+  if (st) return st;
+  if (n == 0) return ME_OK;
+  me::DevPlan P;
+  memset(&P, 0, sizeof(P));
+  fill_voigt_consts(P, nfigures);
+  DevBuf dn, da, dh, dl;
+  const size_t b = (size_t)n * sizeof(double);
+  CK(dn.ensure(b));
+  CK(da.ensure(b));
+  CK(dh.ensure(b));
+  CK(dl.ensure(b));
+  CK(cudaMemcpy(dn.p, nu, b, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(da.p, a, b, cudaMemcpyHostToDevice));
+  CK(me::launch_voigt(precision == ME_PREC_FP64 ? 1 : 0, P, dn.as<double>(), da.as<double>(), n,
+                      dh.as<double>(), dl.as<double>(), 0));
+  CK(cudaMemcpy(H, dh.p, b, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(L, dl.p, b, cudaMemcpyDeviceToHost));
+  dn.release();
+  da.release();
+  dh.release();
+  dl.release();
+  return ME_OK;
+}
+
+extern "C" int me_svd(const double *a, long nmat, int n, double *u, double *w, double *v,
+                      int device) {
+  if (!a || !u || !w || !v || nmat < 0 || n < 1 || n > 9) return fail(ME_ERR_ARG, "bad argument");
+  int st = check_device(device);
+  if (st) return st;
+  if (nmat == 0) return ME_OK;
+  const size_t mb = (size_t)nmat * n * n * sizeof(double), wb = (size_t)nmat * n * sizeof(double);
+  DevBuf da, du, dw, dv, dh;
+  CK(da.ensure(mb));
+  CK(du.ensure(mb));
+  CK(dv.ensure(mb));
+  CK(dw.ensure(wb));
+  CK(dh.ensure(sizeof(int)));
+  CK(cudaMemset(dh.p, 0, sizeof(int)));
+  CK(cudaMemcpy(da.p, a, mb, cudaMemcpyHostToDevice));
+  CK(me::launch_svd(da.as<double>(), nmat, n, du.as<double>(), dw.as<double>(), dv.as<double>(),
+                    dh.as<int>(), 0));
+  CK(cudaMemcpy(u, du.p, mb, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(v, dv.p, mb, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(w, dw.p, wb, cudaMemcpyDeviceToHost));
+  da.release();
+  du.release();
+  dv.release();
+  dw.release();
+  dh.release();
+  return ME_OK;
+}
+
+extern "C" int me_init_guess(me_plan *p, const double *prof, long npix, double *guess,
+                             double *extra, int *status) {
+  if (!p || !prof || !guess || !extra || !status || npix < 0)
+    return fail(ME_ERR_ARG, "null argument");
+  if (npix == 0) return ME_OK;
+  CK(cudaSetDevice(p->device));
+  const size_t n = (size_t)npix, nl = (size_t)p->P.nl;
+  DevBuf dp, dg, de, ds;
+  CK(dp.ensure(n * 4 * nl * sizeof(double)));
+  CK(dg.ensure(n * 9 * sizeof(double)));
+  CK(de.ensure(n * 5 * sizeof(double)));
+  CK(ds.ensure(n * sizeof(int)));
+  CK(cudaMemcpyAsync(dp.p, prof, n * 4 * nl * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  CK(me::launch_init_guess(p->P, dp.as<double>(), npix, dg.as<double>(), de.as<double>(),
+                           ds.as<int>(), p->stream));
+  CK(cudaMemcpyAsync(guess, dg.p, n * 9 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaMemcpyAsync(extra, de.p, n * 5 * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaMemcpyAsync(status, ds.p, n * sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  dp.release();
+  dg.release();
+  de.release();
+  ds.release();
+  return ME_OK;
+}

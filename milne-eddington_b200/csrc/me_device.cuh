@@ -1,0 +1,1032 @@
+// me_device.cuh -- device functions of the per-pixel Milne-Eddington inversion.
+//
+// Everything here is written for sm_100a and templated on the synthesis type
+// T (float for the FP32 path, double for the FP64 path).  The 9x9 SVD solve
+// and the chi^2 accept test are always FP64.
+//
+// Reference functions restated (HaoLi-70/Milne-Eddington, Src/):
+//   voigt / voigt_alg916 / voigt_hui6 / voigt_humlicek_w4 / erfcx / dawson
+//       FADDEEVA.c:440-590, 286-402, 112-163, 167-281, 83-108, 29-79
+//   me_point               ME_SOLVER.c:101-366 (one wavelength of Milne_Eddington_Single)
+//   bounds_fold            ME_SOLVER.c:370-406 (bounds_check)
+//   init_guess             ME_SOLVER.c:445-676 (Init_Guess)
+//   gr_svd / gr_backsub    SVD_TEMPLATE.h:49-406 (svdcmp / svbksb, Golub-Reinsch)
+//   svd_solve              LM_FIT.c:400-469 (SVD_solve_mem)
+//   restart draws          LM_FIT.c:157-201 (Random_Jump) with per-(pixel, run)
+//                          Philox4x32-10 draws instead of a process-wide stream
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace me {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kLightSpeed = 299792458.0;
+constexpr double kSqrtPi = 1.77245385090551588191;
+constexpr int kMaxNl = 512;
+
+// Plan constants the kernels read (passed by value as a kernel parameter).
+struct DevPlan {
+  int nl, ncut, ic, i0, i1, npar;
+  int nfigures, row, fnmax;
+  int niter, nruns, hmi_ref, regul_any;
+  int fixed[9], regul[9];
+  int free_idx[9];  // reduced index -> full parameter index
+  double lambda0, bshift;
+  double limits[9][2];
+  double step[9];
+  double w2[4], weights[4];
+  double icriteria, convg, chisq_crit, damp, lam_accept, lam_reject, lam_lim[2], svd_thr;
+  double vcoeffi, lcoeffi;
+  double regul_value[9], regul_weight[9];
+  unsigned long long seed;
+  // Alg-916 constants (Faddeeva_init, FADDEEVA.c:406-436)
+  double fa, faa, flog_rmin0, fsqrt_log_rmin0;
+  double exp_a2n2[50];
+  double thr[5];  // |z|^2 region boundaries of this Nfigures row
+  const double *lambda;   // [nl] wavelength grid [A]
+  const double *dlambda;  // [nl] lambda - lambda0 [A]
+};
+
+// ---------------------------------------------------------------------------
+// precision-generic math
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float m_exp(float x) { return expf(x); }
+__device__ __forceinline__ double m_exp(double x) { return exp(x); }
+__device__ __forceinline__ float m_sin(float x) { return sinf(x); }
+__device__ __forceinline__ double m_sin(double x) { return sin(x); }
+__device__ __forceinline__ float m_cos(float x) { return cosf(x); }
+__device__ __forceinline__ double m_cos(double x) { return cos(x); }
+__device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float m_erfc(float x) { return erfcf(x); }
+__device__ __forceinline__ double m_erfc(double x) { return erfc(x); }
+__device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double m_abs(double x) { return fabs(x); }
+__device__ __forceinline__ float m_round(float x) { return roundf(x); }
+__device__ __forceinline__ double m_round(double x) { return round(x); }
+__device__ __forceinline__ float m_copysign(float a, float b) { return copysignf(a, b); }
+__device__ __forceinline__ double m_copysign(double a, double b) { return copysign(a, b); }
+__device__ __forceinline__ void m_sincos(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ void m_sincos(double x, double *s, double *c) { sincos(x, s, c); }
+
+// ---------------------------------------------------------------------------
+// Voigt H(nu, a) and Faraday-Voigt L(nu, a) = Re, Im of w(nu + i a)
+// ---------------------------------------------------------------------------
+template <class T>
+struct VoigtK {
+  T a, aa, log_rmin0, sqrt_log_rmin0;
+  int nmax, nfig;
+  T thr[5];
+  const T *ea2n2;  // exp(-a^2 n^2), n = 0..49 (shared memory)
+};
+
+// erfcx(a) = exp(a^2) erfc(a) with the a > 26.6 asymptotic series (FADDEEVA.c:83-108).
+template <class T>
+__device__ __forceinline__ T erfcx_t(T a) {
+  if (a > T(26.6)) {
+    T a2 = a * a;
+    return ((((((T(162.421875) / a2 - T(29.53125)) / a2 + T(6.5625)) / a2 - T(1.875)) / a2 +
+              T(0.75)) / a2 - T(0.5)) / a2 + T(1)) / T(kSqrtPi) / a;
+  }
+  return m_exp(a * a) * m_erfc(a);
+}
+
+// Dawson's integral by Rybicki's method (FADDEEVA.c:29-79); only reached for a == 0.
+template <class T>
+__device__ T dawson_t(T x) {
+  const T H = T(0.4);
+  T ax = m_abs(x);
+  if (ax < T(0.2)) {
+    T x2 = x * x;
+    return x * (T(1) - T(2.0 / 3.0) * x2 * (T(1) - T(0.4) * x2 * (T(1) - T(2.0 / 7.0) * x2)));
+  }
+  int n0 = 2 * (int)m_round(ax / (2 * H));
+  T xp = ax - n0 * H;
+  T e1 = m_exp(T(2) * xp * H);
+  T e2 = e1 * e1;
+  T d1 = T(n0 + 1);
+  T d2 = d1 - T(2);
+  T sum = 0;
+#pragma unroll
+  for (int i = 1; i <= 6; i++) {
+    T t = (T(2) * i - T(1)) * H;
+    sum += m_exp(-t * t) * (e1 / d1 + T(1) / (d2 * e1));
+    d1 += T(2);
+    d2 -= T(2);
+    e1 *= e2;
+  }
+  return T(0.5641895835) * m_copysign(m_exp(-xp * xp), x) * sum;
+}
+
+// Hui, Armstrong & Wray (1978) 6-pole rational approximation (FADDEEVA.c:112-163).
+template <class T>
+__device__ __forceinline__ void voigt_hui6(T nu, T y, T &H, T &L) {
+  const T A[7] = {T(122.607931777104326), T(214.382388694706425), T(181.928533092181549),
+                  T(93.155580458138441),  T(30.180142196210589),  T(5.912626209773153),
+                  T(0.564189583562615)};
+  const T B[7] = {T(122.60793177387535),  T(352.730625110963558), T(457.334478783897737),
+                  T(348.703917719495792), T(170.354001821091472), T(53.992906912940207),
+                  T(10.479857114260399)};
+  const T zr = y, zi = -nu;
+  T pr = A[6], pi = 0, qr = B[6] + zr, qi = zi;
+#pragma unroll
+  for (int k = 5; k >= 0; k--) {
+    T tr = pr * zr - pi * zi + A[k];
+    T ti = pr * zi + pi * zr;
+    pr = tr;
+    pi = ti;
+    tr = qr * zr - qi * zi + B[k];
+    ti = qr * zi + qi * zr;
+    qr = tr;
+    qi = ti;
+  }
+  T den = qr * qr + qi * qi;
+  H = (pr * qr + pi * qi) / den;
+  L = (pi * qr - pr * qi) / den;
+}
+
+// Humlicek (1982) W4 (FADDEEVA.c:167-281).  Reached only for Nfigures <= 5.
+template <class T>
+__device__ void voigt_humlicek_w4(T nu, T y, T &H, T &L) {
+  const T anu = m_abs(nu);
+  const T s = anu + y;
+  const T tr = y, ti = -nu;
+  if (s >= T(15)) {
+    T ur = tr * tr - ti * ti, ui = T(2) * tr * ti;
+    T dr = T(0.5) + ur, di = ui;
+    T den = dr * dr + di * di;
+    H = T(0.56418958355) * (tr * dr + ti * di) / den;
+    L = T(0.56418958355) * (ti * dr - tr * di) / den;
+  } else if (s >= T(5.5)) {
+    T ur = tr * tr - ti * ti, ui = T(2) * tr * ti;
+    T nr = T(1.4104739589) + T(0.5641896) * ur, ni = T(0.5641896) * ui;
+    T dr = T(0.75) + T(3) * ur + (ur * ur - ui * ui);
+    T di = T(3) * ui + T(2) * ur * ui;
+    T den = dr * dr + di * di;
+    T qr = (nr * dr + ni * di) / den, qi = (ni * dr - nr * di) / den;
+    H = tr * qr - ti * qi;
+    L = tr * qi + ti * qr;
+  } else if (y >= T(1.95) * anu - T(0.176)) {
+    const T c[5] = {T(0.5642236), T(3.778987), T(11.96482), T(20.20933), T(16.4955)};
+    const T d[6] = {T(1.0), T(6.699398), T(21.69274), T(39.27121), T(38.82363), T(16.4955)};
+    T nr = c[0], ni = 0, dr = d[0], di = 0;
+    for (int k = 1; k < 5; k++) {
+      T r = nr * tr - ni * ti + c[k], i = nr * ti + ni * tr;
+      nr = r;
+      ni = i;
+    }
+    for (int k = 1; k < 6; k++) {
+      T r = dr * tr - di * ti + d[k], i = dr * ti + di * tr;
+      dr = r;
+      di = i;
+    }
+    T den = dr * dr + di * di;
+    H = (nr * dr + ni * di) / den;
+    L = (ni * dr - nr * di) / den;
+  } else {
+    const T c[7] = {T(0.5641900381), T(1.320521697), T(35.7668278), T(219.0312964),
+                    T(1540.786893),  T(3321.990492), T(36183.30536)};
+    const T d[8] = {T(1),           T(1.841438936), T(61.57036588), T(364.2190727),
+                    T(2186.181081), T(9022.227659), T(24322.84021), T(32066.59372)};
+    T ur = tr * tr - ti * ti, ui = T(2) * tr * ti;
+    T eu = m_exp(ur), sn, cs;
+    m_sincos(ui, &sn, &cs);
+    T er = eu * cs, ei = eu * sn;
+    T nr = c[0], ni = 0, dr = d[0], di = 0;
+    for (int k = 1; k < 7; k++) {
+      T r = -(nr * ur - ni * ui) + c[k], i = -(nr * ui + ni * ur);
+      nr = r;
+      ni = i;
+    }
+    T r = nr * tr - ni * ti, i = nr * ti + ni * tr;
+    nr = r;
+    ni = i;
+    for (int k = 1; k < 8; k++) {
+      r = -(dr * ur - di * ui) + d[k];
+      i = -(dr * ui + di * ur);
+      dr = r;
+      di = i;
+    }
+    T den = dr * dr + di * di;
+    H = er - (nr * dr + ni * di) / den;
+    L = ei - (ni * dr - nr * di) / den;
+  }
+}
+
+// Zaghloul & Ali (2011) ACM Algorithm 916 (FADDEEVA.c:286-402).  erfcx_y is
+// erfcx(y), constant over one synthesis, computed once per call by the caller.
+template <class T>
+__device__ __forceinline__ void voigt_alg916(T nu, T y, T erfcx_y, T &H, T &L,
+                                             const VoigtK<T> &K) {
+  if (nu == T(0)) {
+    H = erfcx_y;
+    L = 0;
+    return;
+  } else if (y == T(0)) {
+    H = m_exp(-nu * nu);
+    L = T(2.0 / kSqrtPi) * dawson_t(nu);
+    return;
+  }
+  const T x = m_abs(nu), ya = m_abs(y);
+  if (x + ya > T(1e7)) {
+    if (x < ya) {
+      T xs = x / ya;
+      H = T(1) / T(kSqrtPi) / (xs * xs + T(1));
+      L = xs / T(kSqrtPi) / (xs * xs + T(1));
+    } else {
+      T ys = ya / x;
+      H = ys / T(kSqrtPi) / (ys * ys + T(1));
+      L = T(1) / T(kSqrtPi) / (ys * ys + T(1));
+    }
+    return;
+  }
+  const T xx = x * x, yy = y * y, xy = x * y;
+  const T xy2 = T(2) * xy;
+  T sin_xy, cos_xy;
+  m_sincos(xy, &sin_xy, &cos_xy);
+  // sin(2xy), cos(2xy) by the double-angle identities
+  const T sin_2xy = T(2) * sin_xy * cos_xy;
+  const T cos_2xy = (cos_xy - sin_xy) * (cos_xy + sin_xy);
+  const T exp_xx = m_exp(-xx);
+  const T k1 = exp_xx * erfcx_y;
+  const T a = K.a;
+  int nmax1 = (int)(m_sqrt(K.log_rmin0 - x * x) / a + T(0.5));
+  if (!(K.log_rmin0 - x * x >= T(0))) nmax1 = -2147483647;  // sqrt(<0) = NaN -> INT_MIN in C
+  const int nmax2 = (int)((K.sqrt_log_rmin0 - x) / a + T(0.5));
+  int nmax = nmax1 > nmax2 ? nmax1 : nmax2;
+  if (nmax >= K.nmax) nmax = K.nmax - 1;
+  const int nb = (int)(x / a + T(0.5));
+  const int nf = nb + 1;
+  const T dxf = a * nf - x;
+  const T dxb = x - a * nb;
+  int nmaxf = (int)((K.sqrt_log_rmin0 - dxf) / a);
+  int nmaxb = (int)((K.sqrt_log_rmin0 - dxb) / a);
+  if (nmaxf >= K.nmax) nmaxf = K.nmax - 1;
+  if (nmaxb >= K.nmax) nmaxb = K.nmax - 1;
+  const int nlo = (nb - nmaxb) > 1 ? (nb - nmaxb) : 1;
+  const T inv_pi = T(1.0 / kPi);
+  T re = k1 * cos_2xy + T(2) * a * x * sin_xy * exp_xx * sin_xy / xy * inv_pi;
+  T im = -k1 * sin_2xy + T(2) * a * x * exp_xx * sin_2xy / xy2 * inv_pi;
+  T s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
+  T e1 = m_exp(-dxf * dxf);
+  T e2 = m_exp(T(-2) * a * dxf);
+  T ep = 1;
+  for (int n = nf; n <= nf + nmaxf; n++) {
+    T t = e1 * K.ea2n2[n - nf] / (K.aa * T(n * n) + yy);
+    s3 += t * ep;
+    s5 += t * ep * a * T(n);
+    ep *= e2;
+  }
+  e1 = m_exp(-dxb * dxb);
+  e2 = m_exp(T(-2) * a * dxb);
+  ep = 1;
+  for (int n = nb; n >= nlo; n--) {
+    T t = e1 * K.ea2n2[nb - n] / (K.aa * T(n * n) + yy);
+    s3 += t * ep;
+    s5 += t * ep * a * T(n);
+    ep *= e2;
+  }
+  re += a * y * s3 * inv_pi;
+  im += a * s5 * inv_pi;
+  if (x < K.sqrt_log_rmin0 || x < T(10)) {
+    const T q = m_exp(T(-2) * a * x);  // 1 / exp(2 a x)
+    ep = 1;
+    for (int n = 1; n <= nmax; n++) {
+      T t = exp_xx * K.ea2n2[n] / (K.aa * T(n * n) + yy);
+      s1 += t;
+      ep *= q;
+      s2 += t * ep;
+      s4 += t * ep * a * T(n);
+    }
+    re += a * y * (T(-2) * cos_2xy * s1 + s2) * inv_pi;
+    im += a * (T(2) * y * sin_2xy * s1 - s4) * inv_pi;
+  }
+  H = re;
+  L = nu > T(0) ? im : -im;
+}
+
+// Accuracy-selected w(z) (Zaghloul 2018 regions; FADDEEVA.c:440-590).
+template <class T>
+__device__ __forceinline__ void voigt(T nu, T y, T erfcx_y, T &H, T &L, const VoigtK<T> &K) {
+  if (nu == T(0)) {
+    H = erfcx_y;
+    L = 0;
+    return;
+  } else if (y == T(0)) {
+    H = m_exp(-nu * nu);
+    L = T(2.0 / kSqrtPi) * dawson_t(nu);
+    return;
+  }
+  const T zr = nu, zi = y;
+  const T z2r = zr * zr - zi * zi;
+  const T z2i = T(2) * zr * zi;
+  const T r2 = zr * zr + zi * zi;
+  const T y2 = y * y;
+  if (r2 >= K.thr[0]) {
+    T den = T(kSqrtPi) * r2;
+    H = zi / den;
+    L = zr / den;
+  } else if (r2 >= K.thr[1]) {
+    T wr = z2r - T(0.5);
+    T den = T(kSqrtPi) * (wr * wr + z2i * z2i);
+    H = (-zi * wr + zr * z2i) / den;
+    L = (zr * wr + zi * z2i) / den;
+  } else if (r2 >= K.thr[2]) {
+    T wr = z2r - T(1.5);
+    T pr = wr * zr - z2i * zi, pi = wr * zi + z2i * zr;
+    T den = T(kSqrtPi) * (pr * pr + pi * pi);
+    wr = z2r - T(1);
+    H = (-z2i * pr + wr * pi) / den;
+    L = (wr * pr + z2i * pi) / den;
+  } else if (r2 >= K.thr[3]) {
+    if ((K.nfig <= 4 && y2 < T(6e-14)) || (K.nfig == 5 && r2 < T(39) && y2 < T(1e-9))) {
+      voigt_humlicek_w4(nu, y, H, L);
+      return;
+    }
+    T wr = z2r - T(2.5);
+    T ar = -(wr * zi + z2i * zr), ai = wr * zr - z2i * zi;
+    wr = z2r - T(3);
+    T br = wr * z2r - z2i * z2i + T(0.75), bi = (wr + z2r) * z2i;
+    T den = T(kSqrtPi) * (br * br + bi * bi);
+    H = (ar * br + ai * bi) / den;
+    L = (-ar * bi + ai * br) / den;
+  } else if (r2 >= K.thr[4]) {
+    if (K.nfig <= 4) {
+      if (y2 < T(0.026))
+        voigt_humlicek_w4(nu, y, H, L);
+      else
+        voigt_hui6(nu, y, H, L);
+      return;
+    } else if (K.nfig == 5) {
+      if (y2 >= T(0.27))
+        voigt_hui6(nu, y, H, L);
+      else if (y2 >= T(1e-9))
+        voigt_alg916(nu, y, erfcx_y, H, L, K);
+      else
+        voigt_humlicek_w4(nu, y, H, L);
+      return;
+    } else if (K.nfig == 6) {
+      if (y2 >= T(1))
+        voigt_hui6(nu, y, H, L);
+      else
+        voigt_alg916(nu, y, erfcx_y, H, L, K);
+      return;
+    }
+    T wr = z2r - T(4.5);
+    T ar = -(wr + z2r) * z2i, ai = wr * z2r - z2i * z2i + T(2);
+    wr = z2r - T(5);
+    T br = wr * z2r - z2i * z2i + T(3.75), bi = (wr + z2r) * z2i;
+    T cr = br * zr - bi * zi, ci = br * zi + bi * zr;
+    T den = T(kSqrtPi) * (cr * cr + ci * ci);
+    H = (ar * cr + ai * ci) / den;
+    L = (-ar * ci + ai * cr) / den;
+  } else {
+    if (K.nfig <= 4)
+      voigt_hui6(nu, y, H, L);
+    else
+      voigt_alg916(nu, y, erfcx_y, H, L, K);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Milne-Eddington synthesis at one wavelength (ME_SOLVER.c:189-362)
+// ---------------------------------------------------------------------------
+template <class T>
+struct SynthCall {
+  T p4, p5, p6, p7, p8;
+  T eta_half, b0, b1, bsh_n, lam_n;
+  T sth, cth, sth2, cth2p1, c2p, s2p, kq, ku, kt, kv;
+  T shift_b, vshift;  // Zeeman and Doppler shifts
+  T erfcx_y;
+  T step[9];
+};
+
+template <class T>
+__device__ __forceinline__ void synth_setup(SynthCall<T> &c, const double *mp, const DevPlan &P,
+                                            const double *step) {
+  c.p4 = T(mp[4]);
+  c.p5 = T(mp[5]);
+  c.p6 = T(mp[6]);
+  c.p7 = T(mp[7]);
+  c.p8 = T(mp[8]);
+  c.eta_half = T(0.5) * c.p6;
+  c.b0 = c.p7 * c.p8;
+  c.b1 = c.p7 - c.b0;
+  c.bsh_n = T(P.bshift / mp[4]);
+  c.lam_n = T(P.lambda0 / mp[4]);
+  double s1, c1, s2, c2;
+  sincos(mp[1], &s1, &c1);
+  sincos(2. * mp[2], &s2, &c2);
+  c.sth = T(s1);
+  c.cth = T(c1);
+  c.sth2 = c.sth * c.sth;
+  c.cth2p1 = c.cth * c.cth + T(1);
+  c.c2p = T(c2);
+  c.s2p = T(s2);
+  c.kq = c.eta_half * c.sth2 * c.c2p;
+  c.ku = c.eta_half * c.sth2 * c.s2p;
+  c.kt = c.eta_half * T(2) * c.sth * c.cth;
+  c.kv = c.eta_half * c.cth;
+  c.shift_b = T(mp[0] * (P.bshift / mp[4]));
+  // Doppler shift in Doppler widths: 1e3 (lambda - lambda0 - v lambda0 / c) / width
+  c.vshift = T(1e6 * mp[3] * P.lambda0 / kLightSpeed);
+  c.erfcx_y = erfcx_t<T>(c.p5);
+#pragma unroll
+  for (int k = 0; k < 9; k++) c.step[k] = T(step[k]);
+}
+
+// Reduced wavelength of grid point iw.
+template <class T>
+__device__ __forceinline__ T shift_w(const SynthCall<T> &c, const DevPlan &P, int iw);
+template <>
+__device__ __forceinline__ float shift_w<float>(const SynthCall<float> &c, const DevPlan &P,
+                                                int iw) {
+  return (1e3f * float(__ldg(P.dlambda + iw)) - c.vshift) / c.p4;
+}
+template <>
+__device__ __forceinline__ double shift_w<double>(const SynthCall<double> &c, const DevPlan &P,
+                                                  int iw) {
+  return (1e3 * __ldg(P.dlambda + iw) - c.vshift) / c.p4;
+}
+
+// syn[4] = I, Q, U, V; with DERIV also J[4][9] (derivatives scaled by step[]).
+template <class T, bool DERIV>
+__device__ __forceinline__ void me_point(const SynthCall<T> &c, T w0, const VoigtK<T> &K, T syn[4],
+                                         T J[4][9]) {
+  const T rsp = T(1.0 / kSqrtPi);
+  T phi[3], psi[3], dphi[3][4], dpsi[3][4];  // derivative slots: B, v, width, a
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int q = k - 1;
+    const T v = w0 + T(q) * c.shift_b;
+    T H, L;
+    voigt<T>(v, c.p5, c.erfcx_y, H, L, K);
+    phi[k] = H * rsp;
+    psi[k] = L * rsp;
+    if (DERIV) {
+      const T dH = T(2) * (-v * H + c.p5 * L) * rsp;
+      const T dL = T(-2) * (-rsp + c.p5 * H + v * L) * rsp;
+      dphi[k][0] = T(q) * c.bsh_n * dH;
+      dpsi[k][0] = T(q) * c.bsh_n * dL;
+      dphi[k][1] = T(-1e6 / kLightSpeed) * c.lam_n * dH;
+      dpsi[k][1] = T(-1e6 / kLightSpeed) * c.lam_n * dL;
+      dphi[k][2] = -v / c.p4 * dH;
+      dpsi[k][2] = -v / c.p4 * dL;
+      dphi[k][3] = -dL;
+      dpsi[k][3] = dH;
+    }
+  }
+  const T phis = T(0.5) * (phi[0] + phi[2]);
+  const T phit = phi[1] - phis;
+  const T psit = psi[1] - T(0.5) * (psi[0] + psi[2]);
+  T eta[4], rho[4];
+  eta[0] = c.eta_half * (phi[1] * c.sth2 + phis * c.cth2p1);
+  eta[1] = phit * c.kq;
+  eta[2] = phit * c.ku;
+  eta[3] = (phi[0] - phi[2]) * c.kv;
+  rho[1] = psit * c.kq;
+  rho[2] = psit * c.ku;
+  rho[3] = (psi[0] - psi[2]) * c.kv;
+  const T a1 = T(1) + eta[0];
+  const T a1s = a1 * a1;
+  const T e2 = eta[1] * eta[1] + eta[2] * eta[2] + eta[3] * eta[3];
+  const T r2 = rho[1] * rho[1] + rho[2] * rho[2] + rho[3] * rho[3];
+  const T er = eta[1] * rho[1] + eta[2] * rho[2] + eta[3] * rho[3];
+  const T del = a1s * (a1s - e2 + r2) - er * er;
+  const T idel = T(1) / del;
+  const T b1d = c.b1 * idel;
+  const T cc[4] = {T(0), eta[3] * rho[2] - eta[2] * rho[3], eta[1] * rho[3] - eta[3] * rho[1],
+                   eta[2] * rho[1] - eta[1] * rho[2]};
+  // numerators of the Unno-Rachkovsky solution: I ~ a1 (a1^2 + r2), P_s ~ ...
+  T num[4];
+  num[0] = a1 * (a1s + r2);
+#pragma unroll
+  for (int s = 1; s < 4; s++) num[s] = a1s * eta[s] + a1 * cc[s] + rho[s] * er;
+  syn[0] = c.b0 + b1d * num[0];
+#pragma unroll
+  for (int s = 1; s < 4; s++) syn[s] = -b1d * num[s];
+  if (!DERIV) return;
+
+  // d eta_s / d p_k and d rho_s / d p_k for k = B, theta, phi, v, width, a, eta0
+  T de[4][7], dr[4][7];
+  {
+    // B, v, width, a share the form of eta/rho in phi'/psi'
+    const int slot_k[4] = {0, 3, 4, 5};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = slot_k[j];
+      const T ps = T(0.5) * (dphi[0][j] + dphi[2][j]);
+      de[0][k] = c.eta_half * (dphi[1][j] * c.sth2 + ps * c.cth2p1);
+      const T t = dphi[1][j] - ps;
+      de[1][k] = t * c.kq;
+      de[2][k] = t * c.ku;
+      de[3][k] = (dphi[0][j] - dphi[2][j]) * c.kv;
+      const T u = dpsi[1][j] - T(0.5) * (dpsi[0][j] + dpsi[2][j]);
+      dr[1][k] = u * c.kq;
+      dr[2][k] = u * c.ku;
+      dr[3][k] = (dpsi[0][j] - dpsi[2][j]) * c.kv;
+    }
+  }
+  de[0][1] = phit * c.kt;
+  de[1][1] = de[0][1] * c.c2p;
+  de[2][1] = de[0][1] * c.s2p;
+  de[3][1] = c.eta_half * (phi[0] - phi[2]) * (-c.sth);
+  dr[1][1] = psit * c.kt * c.c2p;
+  dr[2][1] = psit * c.kt * c.s2p;
+  dr[3][1] = c.eta_half * (psi[0] - psi[2]) * (-c.sth);
+  de[0][2] = 0;
+  de[1][2] = T(-2) * eta[2];
+  de[2][2] = T(2) * eta[1];
+  de[3][2] = 0;
+  dr[1][2] = T(-2) * rho[2];
+  dr[2][2] = T(2) * rho[1];
+  dr[3][2] = 0;
+  const T ip6 = T(1) / c.p6;
+  de[0][6] = eta[0] * ip6;
+#pragma unroll
+  for (int s = 1; s < 4; s++) {
+    de[s][6] = eta[s] * ip6;
+    dr[s][6] = rho[s] * ip6;
+  }
+  const T b1dd = b1d * idel;
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    const T da1 = de[0][k];
+    const T de2 = T(2) * (eta[1] * de[1][k] + eta[2] * de[2][k] + eta[3] * de[3][k]);
+    const T dr2 = T(2) * (rho[1] * dr[1][k] + rho[2] * dr[2][k] + rho[3] * dr[3][k]);
+    const T der = de[1][k] * rho[1] + eta[1] * dr[1][k] + de[2][k] * rho[2] + eta[2] * dr[2][k] +
+                  de[3][k] * rho[3] + eta[3] * dr[3][k];
+    const T ddel = T(2) * a1 * da1 * (a1s - e2 + r2) + a1s * (T(2) * a1 * da1 - de2 + dr2) -
+                   T(2) * er * der;
+    J[0][k] = b1dd * (del * (da1 * (a1s + r2) + a1 * (T(2) * a1 * da1 + dr2)) - ddel * num[0]) *
+              c.step[k];
+    // d cc_s: cc1 = e3 r2 - e2 r3, cc2 = e1 r3 - e3 r1, cc3 = e2 r1 - e1 r2
+    const T dc1 = de[3][k] * rho[2] + eta[3] * dr[2][k] - de[2][k] * rho[3] - eta[2] * dr[3][k];
+    const T dc2 = de[1][k] * rho[3] + eta[1] * dr[3][k] - de[3][k] * rho[1] - eta[3] * dr[1][k];
+    const T dc3 = de[2][k] * rho[1] + eta[2] * dr[1][k] - de[1][k] * rho[2] - eta[1] * dr[2][k];
+    const T dcc[4] = {T(0), dc1, dc2, dc3};
+#pragma unroll
+    for (int s = 1; s < 4; s++) {
+      J[s][k] = -b1dd *
+                (del * (T(2) * a1 * da1 * eta[s] + a1s * de[s][k] + da1 * cc[s] + a1 * dcc[s] +
+                        dr[s][k] * er + rho[s] * der) -
+                 ddel * num[s]) *
+                c.step[k];
+    }
+  }
+  T t7 = (T(1) - c.p8) * idel;
+  J[0][7] = (c.p8 + t7 * num[0]) * c.step[7];
+#pragma unroll
+  for (int s = 1; s < 4; s++) J[s][7] = (-t7 * num[s]) * c.step[7];
+  T t8 = c.p7 * idel;
+  J[0][8] = (c.p7 - t8 * num[0]) * c.step[8];
+#pragma unroll
+  for (int s = 1; s < 4; s++) J[s][8] = (t8 * num[s]) * c.step[8];
+}
+
+// ---------------------------------------------------------------------------
+// bounds_check (ME_SOLVER.c:370-406)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double clampb(double x, double lo, double hi) {
+  return x < lo ? lo : (x > hi ? hi : x);
+}
+__device__ __forceinline__ void bounds_fold(double *p, const DevPlan &P, double l70, double l71) {
+  const double two_pi = 2.0 * kPi;
+  p[0] = clampb(p[0], P.limits[0][0], P.limits[0][1]);
+  double t = fmod(p[1], two_pi);
+  if (t < 0) t += two_pi;
+  if (t > kPi) t = two_pi - t;
+  p[1] = t;
+#pragma unroll
+  for (int i = 3; i < 9; i++) {
+    double lo = i == 7 ? l70 : P.limits[i][0];
+    double hi = i == 7 ? l71 : P.limits[i][1];
+    p[i] = clampb(p[i], lo, hi);
+  }
+  double ph = fmod(p[2], kPi);
+  if (ph < 0.0) ph += kPi;
+  p[2] = ph;
+}
+
+// ---------------------------------------------------------------------------
+// Init_Guess (ME_SOLVER.c:445-676), FP64, one thread per pixel
+// ---------------------------------------------------------------------------
+struct PixelInit {
+  double guess[9];
+  double norm0, normp, l70, l71, step7;
+};
+
+// Returns 1 when mean(I) < Icriteria (or the mean is NaN), as Init_Guess /
+// the INVERSION_MULTI gate.
+__device__ inline int init_guess(const double *prof, const DevPlan &P, PixelInit &o) {
+  const int nw = P.nl;
+  const double *pI = prof, *pQ = prof + nw, *pU = prof + 2 * nw, *pV = prof + 3 * nw;
+  const double lam0 = P.lambda0;
+  double isum = 0., imin = 1e10, qsum = 0., usum = 0., vsum = 0.;
+  double imax = 0, lmax = 0., vmax = 0., vmin = 0.;
+  int i_imin = 0, i_vmax = 0, i_vmin = 0;
+  for (int iw = 0; iw < nw; iw++) {
+    const double vi = pI[iw];
+    if (imax < vi) imax = vi;
+    if (imin > vi) {
+      i_imin = iw;
+      imin = vi;
+    }
+    isum += vi;
+    qsum += fabs(pQ[iw]);
+    usum += fabs(pU[iw]);
+    vsum += fabs(pV[iw]);
+  }
+  for (int iw = P.i0; iw <= P.i1; iw++) {
+    const double l = sqrt(pQ[iw] * pQ[iw] + pU[iw] * pU[iw]);
+    if (lmax < l) lmax = l;
+    if (vmin > pV[iw]) {
+      i_vmin = iw;
+      vmin = pV[iw];
+    } else if (vmax < pV[iw]) {
+      i_vmax = iw;
+      vmax = pV[iw];
+    }
+  }
+  const double imean = isum / nw;
+  if (isnan(imean) || imean < P.icriteria) return 1;
+  o.norm0 = 1e-2 * imean;
+  o.norm0 *= o.norm0;
+  const double is2 = isum * isum;
+  o.normp = 1 + qsum * qsum / is2 * P.w2[1] + usum * usum / is2 * P.w2[2] +
+            vsum * vsum / is2 * P.w2[3];
+  lmax = 100 * lmax / imean;
+  vmin = 100 * vmin / imean;
+  vmax = 100 * vmax / imean;
+  const bool ir_line = (lam0 > 15640 && lam0 < 15660);
+  const double thr_v = ir_line ? 1.5 : 5.0;
+  const double thr_l = ir_line ? 2.5 : 5.0;
+  double blos = 0.;
+  const double lv = 0.5 * (vmax - vmin);
+  const double factor = imin > 0.9 * imax ? 2. : 1.;
+  if (lv > 0.1) {
+    blos = 20 + P.vcoeffi * lv * factor;
+    if (i_vmin < i_vmax) blos = -blos;
+  }
+  double bpos = 100 + P.lcoeffi * lmax * factor;
+  bpos = bpos < 2200 ? bpos : 2200;
+  double *g = o.guess;
+  double tmp = 0;
+  if (lv > thr_v) {
+    tmp = 0.5 * (P.lambda[i_vmin] + P.lambda[i_vmax]) - lam0;
+  } else {
+    bool found = false;
+    // the reference reads pI[i_imin-2 .. i_imin+2] unchecked; out-of-grid
+    // reads (grids with nl < 10) count as a failed minimum test here
+    if (imin < 0.9 * imax && i_imin >= P.ncut && i_imin < nw - P.ncut && i_imin >= 2 &&
+        i_imin + 2 <= nw - 1) {
+      if (pI[i_imin - 1] < pI[i_imin - 2] && pI[i_imin] < pI[i_imin - 1] &&
+          pI[i_imin] < pI[i_imin + 1] && pI[i_imin + 1] < pI[i_imin + 2]) {
+        tmp = P.lambda[i_imin] - lam0;
+        found = true;
+      }
+    }
+    if (!found) {
+      double lsum = 0, wsum = 0.;
+      const int lo = (P.ic > 7) ? (P.ic - 7) : 0;
+      const int hi = (P.ic + 7 < nw) ? (P.ic + 7) : (nw - 1);
+      for (int iw = lo; iw <= hi; iw++) {
+        const double d = (imax - pI[iw]);
+        lsum += P.lambda[iw] * d;
+        wsum += d;
+      }
+      tmp = lsum / wsum - lam0;
+    }
+  }
+  g[3] = tmp / lam0 * kLightSpeed / 1e3;
+  g[0] = sqrt(blos * blos + bpos * bpos);
+  g[1] = acos(blos / g[0]);
+  if (g[0] > 3000) g[0] = 3000;
+  double wsum = 0., phi = 0.;
+  for (int iw = P.i0; iw <= P.i1; iw++) {
+    const double l = sqrt(pQ[iw] * pQ[iw] + pU[iw] * pU[iw]);
+    if (l > thr_l) {
+      double t = 0.5 * atan2(pU[iw], pQ[iw]);
+      t = t > 0 ? t : kPi + t;
+      phi += t * l;
+      wsum += l;
+    }
+  }
+  g[2] = (wsum > 2. * thr_l) ? phi / wsum : kPi / 2.;
+  if (ir_line) {
+    g[4] = 60.;
+    g[5] = 0.5;
+    g[6] = 15;
+    g[8] = 0.7;
+  } else if (g[0] > 1100) {
+    g[4] = 20;
+    g[5] = 0.5;
+    g[6] = 20;
+    g[8] = 0.3;
+  } else {
+    g[4] = 30;
+    g[5] = 0.5;
+    g[6] = 5;
+    g[8] = 0.15;
+  }
+  g[7] = imax;
+  o.l70 = imax * 0.6;
+  o.l71 = imax * 1.4;
+  o.step7 = imax * 0.1;
+  bounds_fold(g, P, o.l70, o.l71);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Golub-Reinsch SVD, FP64 (SVD_TEMPLATE.h:49-406).  a[n*n] -> U in place,
+// w[n], v[n*n]; returns 1 when a bidiagonal entry needed more than 50 QR sweeps
+// (the reference stops the program there).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double pythag_d(double a, double b) {
+  const double aa = fabs(a), ab = fabs(b);
+  const double mx = aa > ab ? aa : ab;
+  if (mx == 0) return 0;
+  if (mx < 1e150) return sqrt(a * a + b * b);
+  const double mn = aa > ab ? ab : aa;
+  const double r = mn / mx;
+  return mx * sqrt(1.0 + r * r);
+}
+
+__device__ inline int gr_svd(double *a, int n, double *w, double *v) {
+#define A_(i, j) a[(i) * n + (j)]
+#define V_(i, j) v[(i) * n + (j)]
+  const int m = n;
+  int l = 0, nm = 0;
+  double anorm = 0., c, f, g = 0., h, s, scale = 0., x, y, z;
+  double rv1[9];
+  int hit = 0;
+  for (int i = 0; i < n; i++) {
+    l = i + 1;
+    rv1[i] = scale * g;
+    g = s = scale = 0.0;
+    for (int k = i; k < m; k++) scale += fabs(A_(k, i));
+    if (scale) {
+      const double is = 1.0 / scale;
+      for (int k = i; k < m; k++) {
+        A_(k, i) *= is;
+        s += A_(k, i) * A_(k, i);
+      }
+      f = A_(i, i);
+      g = f >= 0 ? -sqrt(s) : sqrt(s);
+      h = f * g - s;
+      A_(i, i) = f - g;
+      const double ih = 1.0 / h;
+      for (int j = l; j < n; j++) {
+        s = 0.0;
+        for (int k = i; k < m; k++) s += A_(k, i) * A_(k, j);
+        f = s * ih;
+        for (int k = i; k < m; k++) A_(k, j) += f * A_(k, i);
+      }
+      for (int k = i; k < m; k++) A_(k, i) *= scale;
+    }
+    w[i] = scale * g;
+    g = s = scale = 0.0;
+    if (i != n - 1) {
+      for (int k = l; k < n; k++) scale += fabs(A_(i, k));
+      if (scale) {
+        const double is = 1.0 / scale;
+        for (int k = l; k < n; k++) {
+          A_(i, k) *= is;
+          s += A_(i, k) * A_(i, k);
+        }
+        f = A_(i, l);
+        g = f >= 0 ? -sqrt(s) : sqrt(s);
+        h = f * g - s;
+        A_(i, l) = f - g;
+        const double ih = 1.0 / h;
+        for (int k = l; k < n; k++) rv1[k] = A_(i, k) * ih;
+        for (int j = l; j < m; j++) {
+          s = 0.0;
+          for (int k = l; k < n; k++) s += A_(j, k) * A_(i, k);
+          for (int k = l; k < n; k++) A_(j, k) += s * rv1[k];
+        }
+        for (int k = l; k < n; k++) A_(i, k) *= scale;
+      }
+    }
+    const double t = fabs(w[i]) + fabs(rv1[i]);
+    if (anorm < t) anorm = t;
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    if (i < n - 1) {
+      if (g != 0.0) {
+        for (int j = l; j < n; j++) V_(j, i) = (A_(i, j) / A_(i, l)) / g;
+        for (int j = l; j < n; j++) {
+          s = 0.0;
+          for (int k = l; k < n; k++) s += A_(i, k) * V_(k, j);
+          for (int k = l; k < n; k++) V_(k, j) += s * V_(k, i);
+        }
+      }
+      for (int j = l; j < n; j++) V_(i, j) = V_(j, i) = 0.0;
+    }
+    V_(i, i) = 1.0;
+    g = rv1[i];
+    l = i;
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    l = i + 1;
+    g = w[i];
+    for (int j = l; j < n; j++) A_(i, j) = 0.0;
+    if (g != 0.0) {
+      g = 1.0 / g;
+      for (int j = l; j < n; j++) {
+        s = 0.0;
+        for (int k = l; k < m; k++) s += A_(k, i) * A_(k, j);
+        f = (s / A_(i, i)) * g;
+        for (int k = i; k < m; k++) A_(k, j) += f * A_(k, i);
+      }
+      for (int j = i; j < m; j++) A_(j, i) *= g;
+    } else {
+      for (int j = i; j < m; j++) A_(j, i) = 0.0;
+    }
+    A_(i, i) += 1.0;
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    for (int its = 0; its < 50; its++) {
+      int flag = 1;
+      for (l = k; l >= 0; l--) {
+        nm = l - 1;
+        if ((fabs(rv1[l]) + anorm) == anorm) {
+          flag = 0;
+          break;
+        }
+        if (nm >= 0 && (fabs(w[nm]) + anorm) == anorm) break;
+      }
+      if (flag) {
+        c = 0.0;
+        s = 1.0;
+        for (int i = l; i <= k; i++) {
+          f = s * rv1[i];
+          rv1[i] = c * rv1[i];
+          if ((fabs(f) + anorm) == anorm) break;
+          g = w[i];
+          h = pythag_d(f, g);
+          w[i] = h;
+          h = 1.0 / h;
+          c = g * h;
+          s = -f * h;
+          for (int j = 0; j < m; j++) {
+            y = A_(j, nm);
+            z = A_(j, i);
+            A_(j, nm) = y * c + z * s;
+            A_(j, i) = z * c - y * s;
+          }
+        }
+      }
+      z = w[k];
+      if (l == k) {
+        if (z < 0.0) {
+          w[k] = -z;
+          for (int j = 0; j < n; j++) V_(j, k) = -V_(j, k);
+        }
+        break;
+      }
+      if (its == 49) hit = 1;
+      x = w[l];
+      nm = k - 1;
+      y = w[nm];
+      g = rv1[nm];
+      h = rv1[k];
+      f = ((y - z) * (y + z) + (g - h) * (g + h)) / (2.0 * h * y);
+      g = pythag_d(f, 1.0);
+      f = ((x - z) * (x + z) + h * (y / (f + (f >= 0.0 ? g : -g)) - h)) / x;
+      c = s = 1.0;
+      for (int j = l; j <= nm; j++) {
+        const int i = j + 1;
+        g = rv1[i];
+        y = w[i];
+        h = s * g;
+        g *= c;
+        z = pythag_d(f, h);
+        rv1[j] = z;
+        c = f / z;
+        s = h / z;
+        f = x * c + g * s;
+        g = g * c - x * s;
+        h = y * s;
+        y *= c;
+        for (int jj = 0; jj < n; jj++) {
+          x = V_(jj, j);
+          z = V_(jj, i);
+          V_(jj, j) = x * c + z * s;
+          V_(jj, i) = z * c - x * s;
+        }
+        z = pythag_d(f, h);
+        w[j] = z;
+        if (z) {
+          z = 1.0 / z;
+          c = f * z;
+          s = h * z;
+        }
+        f = c * g + s * y;
+        x = c * y - s * g;
+        for (int jj = 0; jj < m; jj++) {
+          y = A_(jj, j);
+          z = A_(jj, i);
+          A_(jj, j) = y * c + z * s;
+          A_(jj, i) = z * c - y * s;
+        }
+      }
+      rv1[l] = 0.0;
+      rv1[k] = f;
+      w[k] = x;
+    }
+  }
+  return hit;
+#undef A_
+#undef V_
+}
+
+// x = V diag(1/w) U^T b, skipping w <= 1e-50 (svbksb, SVD_TEMPLATE.h:348-406).
+__device__ __forceinline__ void gr_backsub(const double *u, const double *v, const double *w,
+                                           const double *b, int n, double *x) {
+  double t[9];
+  for (int j = 0; j < n; j++) {
+    double s = 0.0;
+    if (w[j] > 1e-50) {
+      for (int i = 0; i < n; i++) s += u[i * n + j] * b[i];
+      s /= w[j];
+    }
+    t[j] = s;
+  }
+  for (int i = 0; i < n; i++) {
+    double s = 0.0;
+    for (int j = 0; j < n; j++) s += v[i * n + j] * t[j];
+    x[i] = s;
+  }
+}
+
+// SVD_solve_mem (LM_FIT.c:400-469): the SVD overwrites hess by U; singular
+// values below w_max * thr are dropped, thr x5 from SVDthreshold until the
+// step is inside +-0.5 or thr exceeds 2e-3, then the step is clamped.
+__device__ __forceinline__ int svd_solve(double *hess, double *v, const double *g, int n,
+                                         double thr, double *sol) {
+  double w[9];
+  const int hit = gr_svd(hess, n, w, v);
+  double wmax = w[0];
+  for (int i = 1; i < n; i++) wmax = wmax > w[i] ? wmax : w[i];
+  while (true) {
+    const double wthr = wmax * thr;
+    for (int i = 0; i < n; i++)
+      if (w[i] < wthr) w[i] = 0.;
+    gr_backsub(hess, v, w, g, n, sol);
+    bool inside = true;
+    for (int i = 0; i < n; i++)
+      if (sol[i] > 0.5 || sol[i] < -0.5) inside = false;
+    if (inside) break;
+    if (thr > 2e-3) {
+      for (int i = 0; i < n; i++) sol[i] = sol[i] > 0.5 ? 0.5 : (sol[i] < -0.5 ? -0.5 : sol[i]);
+      break;
+    }
+    thr *= 5.;
+  }
+  return hit;
+}
+
+// ---------------------------------------------------------------------------
+// Restart draws: Philox4x32-10 (Salmon et al., SC'11) keyed by the plan's
+// seed, counter (pixel, run, block); Box-Muller pairs -> 8 standard normals.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+    const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0;
+    c[1] = lo1;
+    c[2] = n2;
+    c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+__device__ inline void restart_draws(unsigned long long seed, long long pixel, int run,
+                                     double z[8]) {
+#pragma unroll
+  for (int blk = 0; blk < 2; blk++) {
+    uint32_t c[4] = {(uint32_t)((unsigned long long)pixel & 0xffffffffu),
+                     (uint32_t)((unsigned long long)pixel >> 32), (uint32_t)run, (uint32_t)blk};
+    philox10(c, (uint32_t)(seed & 0xffffffffu), (uint32_t)(seed >> 32));
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const double u1 = ((double)c[2 * h] + 0.5) * 2.3283064365386963e-10;
+      const double u2 = ((double)c[2 * h + 1] + 0.5) * 2.3283064365386963e-10;
+      const double r = sqrt(-2.0 * log(u1));
+      double sn, cs;
+      sincos(6.283185307179586 * u2, &sn, &cs);
+      z[blk * 4 + 2 * h] = r * cs;
+      z[blk * 4 + 2 * h + 1] = r * sn;
+    }
+  }
+}
+
+}  // namespace me

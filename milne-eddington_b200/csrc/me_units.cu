@@ -1,0 +1,177 @@
+// me_units.cu -- unit kernels (synthesis, Voigt, SVD, initial guess) and the
+// launch dispatch.  The inversion kernel itself lives in me_invert.cuh.
+//
+#include <cuda_runtime.h>
+
+#include "me_device.cuh"
+#include "me_kernels.h"
+
+namespace me {
+
+namespace {
+
+template <class T>
+__device__ __forceinline__ void load_voigt(VoigtK<T> &K, const DevPlan &P, T *s_tab) {
+  K.a = T(P.fa);
+  K.aa = T(P.faa);
+  K.log_rmin0 = T(P.flog_rmin0);
+  K.sqrt_log_rmin0 = T(P.fsqrt_log_rmin0);
+  K.nmax = P.fnmax;
+  K.nfig = P.nfigures;
+#pragma unroll
+  for (int i = 0; i < 5; i++) K.thr[i] = T(P.thr[i]);
+  K.ea2n2 = s_tab;
+}
+
+template <class T>
+__device__ __forceinline__ void fill_table(const DevPlan &P, T *s_tab) {
+  for (int i = threadIdx.x; i < 50; i += blockDim.x) s_tab[i] = T(P.exp_a2n2[i]);
+  __syncthreads();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Building blocks exposed for the unit entry points.
+// ---------------------------------------------------------------------------
+
+template <class T>
+__global__ void synth_kernel(const DevPlan P, const double *par, long long npix, double step7,
+                             double *prof, double *jac) {
+  __shared__ T s_tab[50];
+  fill_table<T>(P, s_tab);
+  VoigtK<T> K;
+  load_voigt<T>(K, P, s_tab);
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= npix) return;
+  const int nl = P.nl;
+  double step[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) step[k] = P.step[k];
+  step[7] = step7;
+  double mp[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) mp[k] = par[i * 9 + k];
+  SynthCall<T> c;
+  synth_setup<T>(c, mp, P, step);
+  for (int iw = 0; iw < nl; iw++) {
+    T syn[4], J[4][9];
+    const T w0 = shift_w<T>(c, P, iw);
+    if (jac) {
+      me_point<T, true>(c, w0, K, syn, J);
+      for (int s = 0; s < 4; s++)
+        for (int k = 0; k < 9; k++) jac[((size_t)i * 36 + s * 9 + k) * nl + iw] = (double)J[s][k];
+    } else {
+      me_point<T, false>(c, w0, K, syn, J);
+    }
+    for (int s = 0; s < 4; s++) prof[((size_t)i * 4 + s) * nl + iw] = (double)syn[s];
+  }
+}
+
+template <class T>
+__global__ void voigt_kernel(const DevPlan P, const double *nu, const double *a, long long n,
+                             double *H, double *L) {
+  __shared__ T s_tab[50];
+  fill_table<T>(P, s_tab);
+  VoigtK<T> K;
+  load_voigt<T>(K, P, s_tab);
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  T h, l;
+  const T y = T(a[i]);
+  voigt<T>(T(nu[i]), y, erfcx_t<T>(y), h, l, K);
+  H[i] = (double)h;
+  L[i] = (double)l;
+}
+
+__global__ void svd_kernel(const double *a, long long nmat, int n, double *u, double *w,
+                           double *v, int *limit_hits) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= nmat) return;
+  double am[81], vv[81], ww[9];
+  for (int k = 0; k < n * n; k++) am[k] = a[i * n * n + k];
+  const int hit = gr_svd(am, n, ww, vv);
+  for (int k = 0; k < n * n; k++) {
+    u[i * n * n + k] = am[k];
+    v[i * n * n + k] = vv[k];
+  }
+  for (int k = 0; k < n; k++) w[i * n + k] = ww[k];
+  if (hit && limit_hits) atomicAdd(limit_hits, 1);
+}
+
+__global__ void init_guess_kernel(const DevPlan P, const double *prof, long long npix,
+                                  double *guess, double *extra, int *status) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= npix) return;
+  PixelInit o;
+  const int st = init_guess(prof + (size_t)i * 4 * P.nl, P, o);
+  status[i] = st;
+  for (int k = 0; k < 9; k++) guess[i * 9 + k] = st ? 0.0 : o.guess[k];
+  extra[i * 5 + 0] = st ? 0.0 : o.norm0;
+  extra[i * 5 + 1] = st ? 0.0 : o.normp;
+  extra[i * 5 + 2] = st ? 0.0 : o.l70;
+  extra[i * 5 + 3] = st ? 0.0 : o.l71;
+  extra[i * 5 + 4] = st ? 0.0 : o.step7;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+int invert_grid_f32(int device);
+int invert_grid_f64(int device);
+cudaError_t launch_invert_f32(const DevPlan &P, const InvertArgs &A, int grid, cudaStream_t st);
+cudaError_t launch_invert_f64(const DevPlan &P, const InvertArgs &A, int grid, cudaStream_t st);
+
+int invert_grid(int precision, int device) {
+  return precision == 1 ? invert_grid_f64(device) : invert_grid_f32(device);
+}
+
+cudaError_t launch_invert(int precision, const DevPlan &P, const InvertArgs &A, int grid,
+                          cudaStream_t st) {
+  return precision == 1 ? launch_invert_f64(P, A, grid, st) : launch_invert_f32(P, A, grid, st);
+}
+
+cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,
+                         double step7, double *d_prof, double *d_jac, cudaStream_t st) {
+  const int b = 128;
+  const unsigned g = (unsigned)((npix + b - 1) / b);
+  if (g == 0) return cudaSuccess;
+  if (precision == 1)
+    synth_kernel<double><<<g, b, 0, st>>>(P, d_par, npix, step7, d_prof, d_jac);
+  else
+    synth_kernel<float><<<g, b, 0, st>>>(P, d_par, npix, step7, d_prof, d_jac);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_voigt(int precision, const DevPlan &P, const double *d_nu, const double *d_a,
+                         long long n, double *d_H, double *d_L, cudaStream_t st) {
+  const int b = 256;
+  const unsigned g = (unsigned)((n + b - 1) / b);
+  if (g == 0) return cudaSuccess;
+  if (precision == 1)
+    voigt_kernel<double><<<g, b, 0, st>>>(P, d_nu, d_a, n, d_H, d_L);
+  else
+    voigt_kernel<float><<<g, b, 0, st>>>(P, d_nu, d_a, n, d_H, d_L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_svd(const double *d_a, long long nmat, int n, double *d_u, double *d_w,
+                       double *d_v, int *d_hits, cudaStream_t st) {
+  const int b = 128;
+  const unsigned g = (unsigned)((nmat + b - 1) / b);
+  if (g == 0) return cudaSuccess;
+  svd_kernel<<<g, b, 0, st>>>(d_a, nmat, n, d_u, d_w, d_v, d_hits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_guess(const DevPlan &P, const double *d_prof, long long npix,
+                              double *d_guess, double *d_extra, int *d_status, cudaStream_t st) {
+  const int b = 128;
+  const unsigned g = (unsigned)((npix + b - 1) / b);
+  if (g == 0) return cudaSuccess;
+  init_guess_kernel<<<g, b, 0, st>>>(P, d_prof, npix, d_guess, d_extra, d_status);
+  return cudaGetLastError();
+}
+
+}  // namespace me

@@ -1,0 +1,355 @@
+"""Python binding of libme_b200.so (the C ABI declared in include/me_b200.h).
+
+A thin ctypes layer: it mirrors the C structures, converts numpy arrays to
+pointers and turns negative status codes into exceptions.  All computation
+happens in the CUDA library; there is no Python or CPU fallback, and loading
+fails loudly if the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libme_b200.so")
+
+ME_MAX_LINES = 20
+ME_PATH_LEN = 512
+ME_PREC_FP32 = 0
+ME_PREC_FP64 = 1
+
+STATUS = {
+    0: "ME_OK",
+    -1: "ME_ERR_ARG",
+    -2: "ME_ERR_CONFIG",
+    -3: "ME_ERR_IO",
+    -4: "ME_ERR_CUDA",
+    -5: "ME_ERR_NODEVICE",
+    -6: "ME_ERR_TIMEOUT",
+    -7: "ME_ERR_NOMEM",
+    -8: "ME_ERR_FORMAT",
+}
+
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+class MeConfig(ctypes.Structure):
+    """struct me_config (include/me_b200.h)."""
+
+    _fields_ = [
+        ("nline", ctypes.c_int),
+        ("line_lambda0", ctypes.c_double * ME_MAX_LINES),
+        ("line_geff", ctypes.c_double * ME_MAX_LINES),
+        ("verbose", ctypes.c_int),
+        ("num_iter", ctypes.c_int),
+        ("num_run", ctypes.c_int),
+        ("convg_criteria", ctypes.c_double),
+        ("chisq_criteria", ctypes.c_double),
+        ("data_path", ctypes.c_char * ME_PATH_LEN),
+        ("wavelength_path", ctypes.c_char * ME_PATH_LEN),
+        ("weights", ctypes.c_double * 4),
+        ("sol_box", ctypes.c_int * 4),
+        ("output_fit", ctypes.c_int),
+        ("cache_path", ctypes.c_char * ME_PATH_LEN),
+        ("result_path", ctypes.c_char * ME_PATH_LEN),
+        ("fit_path", ctypes.c_char * ME_PATH_LEN),
+        ("damp", ctypes.c_double),
+        ("lambda_accept", ctypes.c_double),
+        ("lambda_reject", ctypes.c_double),
+        ("lambda_limits", ctypes.c_double * 2),
+        ("bounds", (ctypes.c_double * 2) * 9),
+        ("fixed", ctypes.c_int * 9),
+        ("regul", ctypes.c_int * 9),
+        ("regul_value", ctypes.c_double * 9),
+        ("regul_weight", ctypes.c_double * 9),
+        ("regul_any", ctypes.c_int),
+        ("vcoeffi", ctypes.c_double),
+        ("lcoeffi", ctypes.c_double),
+        ("icriteria", ctypes.c_double),
+        ("svd_threshold", ctypes.c_double),
+        ("hmi_ref", ctypes.c_int),
+        ("cache_prof", ctypes.c_int),
+        ("nthreads", ctypes.c_int),
+        ("nfigures", ctypes.c_int),
+        ("step", ctypes.c_double * 9),
+        ("nprofiles", ctypes.c_int),
+        ("cache_inv", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("rng_seed", ctypes.c_ulonglong),
+        ("lines_seen", ctypes.c_int),
+        ("data_path_seen", ctypes.c_int),
+        ("wavelength_path_seen", ctypes.c_int),
+    ]
+
+
+class MePlanFacts(ctypes.Structure):
+    _fields_ = [
+        ("nl", ctypes.c_int),
+        ("ncut", ctypes.c_int),
+        ("ic", ctypes.c_int),
+        ("i0", ctypes.c_int),
+        ("i1", ctypes.c_int),
+        ("npar", ctypes.c_int),
+        ("bshift", ctypes.c_double),
+        ("limits", (ctypes.c_double * 2) * 9),
+        ("fadd_a", ctypes.c_double),
+    ]
+
+
+class MeStats(ctypes.Structure):
+    _fields_ = [
+        ("pixels", ctypes.c_longlong),
+        ("valid", ctypes.c_longlong),
+        ("runs", ctypes.c_longlong),
+        ("iterations", ctypes.c_longlong),
+        ("trials", ctypes.c_longlong),
+        ("accepted", ctypes.c_longlong),
+        ("syntheses", ctypes.c_longlong),
+        ("jacobians", ctypes.c_longlong),
+        ("wavelengths", ctypes.c_longlong),
+        ("redo_pixels", ctypes.c_longlong),
+        ("kernel_ms", ctypes.c_double),
+        ("h2d_ms", ctypes.c_double),
+        ("d2h_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+# every symbol include/me_b200.h declares
+EXPORTED = [
+    "me_version", "me_strerror", "me_last_error", "me_config_init", "me_config_parse",
+    "me_config_parse_text", "me_plan_create", "me_plan_destroy", "me_plan_get_facts",
+    "me_plan_get_carry_chisq", "me_plan_set_carry_chisq", "me_plan_grid", "me_plan_set_grid",
+    "me_invert_batch", "me_invert_batch_device", "me_synthesize", "me_synthesize_device",
+    "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess",
+]
+
+
+class MeError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS.get(status, status)} {detail}".strip())
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libme_b200.so (built by `make -C milne-eddington_b200`)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with make -C {HERE}")
+        L = ctypes.CDLL(LIB_PATH)
+        L.me_version.restype = ctypes.c_char_p
+        L.me_strerror.restype = ctypes.c_char_p
+        L.me_last_error.restype = ctypes.c_char_p
+        L.me_config_init.argtypes = [ctypes.POINTER(MeConfig)]
+        L.me_config_parse.argtypes = [ctypes.c_char_p, ctypes.POINTER(MeConfig), ctypes.c_char_p,
+                                      ctypes.c_size_t]
+        L.me_config_parse_text.argtypes = [ctypes.c_char_p, ctypes.POINTER(MeConfig),
+                                           ctypes.c_char_p, ctypes.c_size_t]
+        L.me_plan_create.argtypes = [ctypes.POINTER(MeConfig), _D, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_void_p)]
+        L.me_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.me_plan_destroy.restype = None
+        L.me_plan_get_facts.argtypes = [ctypes.c_void_p, ctypes.POINTER(MePlanFacts)]
+        L.me_plan_get_carry_chisq.argtypes = [ctypes.c_void_p]
+        L.me_plan_get_carry_chisq.restype = ctypes.c_double
+        L.me_plan_set_carry_chisq.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.me_plan_set_carry_chisq.restype = None
+        L.me_plan_grid.argtypes = [ctypes.c_void_p]
+        L.me_plan_set_grid.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_grid.restype = None
+        L.me_invert_batch.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
+                                      ctypes.POINTER(MeStats)]
+        L.me_invert_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.POINTER(MeStats)]
+        L.me_synthesize.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D]
+        L.me_synthesize_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                           ctypes.c_void_p, ctypes.c_void_p]
+        L.me_synthesize_jacobian.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, ctypes.c_double,
+                                             _D, _D]
+        L.me_faddeeva.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, ctypes.c_long, _D, _D,
+                                  ctypes.c_int]
+        L.me_svd.argtypes = [_D, ctypes.c_long, ctypes.c_int, _D, _D, _D, ctypes.c_int]
+        L.me_init_guess.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
+                                    ctypes.POINTER(ctypes.c_int)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_D)
+
+
+def _check(status: int, where: str):
+    if status != 0:
+        raise MeError(status, where, lib().me_last_error().decode(errors="replace"))
+
+
+def parse_config_text(text: str) -> MeConfig:
+    """me_config_parse_text: the reference's keyword semantics (Src/RINPUT.c:361-563)."""
+    cfg = MeConfig()
+    err = ctypes.create_string_buffer(512)
+    st = lib().me_config_parse_text(text.encode(), ctypes.byref(cfg), err, 512)
+    if st != 0:
+        raise MeError(st, "me_config_parse_text", err.value.decode(errors="replace"))
+    return cfg
+
+
+def parse_config(path: str) -> MeConfig:
+    cfg = MeConfig()
+    err = ctypes.create_string_buffer(512)
+    st = lib().me_config_parse(path.encode(), ctypes.byref(cfg), err, 512)
+    if st != 0:
+        raise MeError(st, "me_config_parse", err.value.decode(errors="replace"))
+    return cfg
+
+
+def default_config() -> MeConfig:
+    cfg = MeConfig()
+    _check(lib().me_config_init(ctypes.byref(cfg)), "me_config_init")
+    return cfg
+
+
+class Plan:
+    """me_plan: one wavelength grid + control file on one GPU (INIT_INV)."""
+
+    def __init__(self, cfg: MeConfig, wavelengths: np.ndarray, device: int = 0):
+        self.cfg = cfg
+        self.wavelengths = np.ascontiguousarray(wavelengths, dtype=np.float64)
+        self.nl = int(self.wavelengths.size)
+        h = ctypes.c_void_p()
+        _check(lib().me_plan_create(ctypes.byref(cfg), _ptr(self.wavelengths), self.nl, device,
+                                    ctypes.byref(h)), "me_plan_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().me_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def facts(self) -> dict:
+        f = MePlanFacts()
+        _check(lib().me_plan_get_facts(self._h, ctypes.byref(f)), "me_plan_get_facts")
+        return {"nl": f.nl, "ncut": f.ncut, "ic": f.ic, "i0": f.i0, "i1": f.i1, "npar": f.npar,
+                "bshift": f.bshift, "limits": np.array([[f.limits[i][0], f.limits[i][1]]
+                                                        for i in range(9)]),
+                "fadd_a": f.fadd_a}
+
+    @property
+    def carry_chisq(self) -> float:
+        return lib().me_plan_get_carry_chisq(self._h)
+
+    @carry_chisq.setter
+    def carry_chisq(self, v: float):
+        lib().me_plan_set_carry_chisq(self._h, float(v))
+
+    @property
+    def grid(self) -> int:
+        return lib().me_plan_grid(self._h)
+
+    @grid.setter
+    def grid(self, g: int):
+        lib().me_plan_set_grid(self._h, int(g))
+
+    def invert(self, prof: np.ndarray, want_fit: bool = False):
+        """me_invert_batch on host arrays: prof [npix][4][nl] -> res [npix][10] (+fit)."""
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        npix = prof.shape[0]
+        assert prof.shape[1:] == (4, self.nl)
+        res = np.zeros((npix, 10))
+        fit = np.zeros((npix, 4, self.nl)) if want_fit else None
+        st = MeStats()
+        _check(lib().me_invert_batch(self._h, _ptr(prof), npix, _ptr(res), _ptr(fit),
+                                     ctypes.byref(st)), "me_invert_batch")
+        return (res, fit, st.as_dict()) if want_fit else (res, st.as_dict())
+
+    def invert_device(self, d_prof: int, npix: int, d_res: int, d_fit: int = 0, stream: int = 0):
+        """me_invert_batch_device on raw device pointers (e.g. torch tensor .data_ptr())."""
+        st = MeStats()
+        _check(lib().me_invert_batch_device(self._h, ctypes.c_void_p(d_prof), npix,
+                                            ctypes.c_void_p(d_res),
+                                            ctypes.c_void_p(d_fit) if d_fit else None,
+                                            ctypes.c_void_p(stream) if stream else None,
+                                            ctypes.byref(st)), "me_invert_batch_device")
+        return st.as_dict()
+
+    def synthesize(self, par: np.ndarray) -> np.ndarray:
+        par = np.ascontiguousarray(par, dtype=np.float64).reshape(-1, 9)
+        out = np.zeros((par.shape[0], 4, self.nl))
+        _check(lib().me_synthesize(self._h, _ptr(par), par.shape[0], _ptr(out)), "me_synthesize")
+        return out
+
+    def synthesize_device(self, d_par: int, npix: int, d_prof: int, stream: int = 0):
+        _check(lib().me_synthesize_device(self._h, ctypes.c_void_p(d_par), npix,
+                                          ctypes.c_void_p(d_prof),
+                                          ctypes.c_void_p(stream) if stream else None),
+               "me_synthesize_device")
+
+    def synthesize_jacobian(self, par: np.ndarray, step7: float):
+        par = np.ascontiguousarray(par, dtype=np.float64).reshape(-1, 9)
+        n = par.shape[0]
+        prof = np.zeros((n, 4, self.nl))
+        jac = np.zeros((n, 4, 9, self.nl))
+        _check(lib().me_synthesize_jacobian(self._h, _ptr(par), n, float(step7), _ptr(prof),
+                                            _ptr(jac)), "me_synthesize_jacobian")
+        return prof, jac
+
+    def init_guess(self, prof: np.ndarray):
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        n = prof.shape[0]
+        guess = np.zeros((n, 9))
+        extra = np.zeros((n, 5))
+        status = np.zeros(n, dtype=np.int32)
+        _check(lib().me_init_guess(self._h, _ptr(prof), n, _ptr(guess), _ptr(extra),
+                                   status.ctypes.data_as(ctypes.POINTER(ctypes.c_int))),
+               "me_init_guess")
+        return guess, extra, status
+
+
+def faddeeva(nfigures: int, nu: np.ndarray, a: np.ndarray, precision: int = ME_PREC_FP64,
+             device: int = 0):
+    nu = np.ascontiguousarray(nu, dtype=np.float64).ravel()
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    H = np.zeros_like(nu)
+    L = np.zeros_like(nu)
+    _check(lib().me_faddeeva(nfigures, precision, _ptr(nu), _ptr(a), nu.size, _ptr(H), _ptr(L),
+                             device), "me_faddeeva")
+    return H, L
+
+
+def svd(a: np.ndarray, device: int = 0):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    nmat, n, _ = a.shape
+    u = np.zeros_like(a)
+    v = np.zeros_like(a)
+    w = np.zeros((nmat, n))
+    _check(lib().me_svd(_ptr(a), nmat, n, _ptr(u), _ptr(w), _ptr(v), device), "me_svd")
+    return u, w, v

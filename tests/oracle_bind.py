@@ -1,0 +1,281 @@
+"""ctypes bindings of the CPU checkers (test infrastructure only).
+
+* ``Oracle``     oracle/libme_oracle.so, this project's C++ restatement of the
+                 reference's per-pixel inversion.
+* ``Reference``  oracle/_ref/libmeref.so, the reference's own C core compiled
+                 unmodified with ref_harness.c; present only where it was built
+                 (it travels with the repository snapshot).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "milne-eddington_b200")
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)
+
+import me_b200  # noqa: E402
+
+ORACLE_SO = os.path.join(ROOT, "oracle", "libme_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libmeref.so")
+MEO_RNG_COUNTER = 0
+MEO_RNG_NR = 1
+
+_D = ctypes.POINTER(ctypes.c_double)
+_LL = ctypes.POINTER(ctypes.c_longlong)
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_D)
+
+
+_olib = None
+
+
+def oracle_lib():
+    global _olib
+    if _olib is None:
+        L = ctypes.CDLL(ORACLE_SO)
+        L.meo_plan_create.argtypes = [ctypes.POINTER(me_b200.MeConfig), _D, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_void_p)]
+        L.meo_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.meo_plan_destroy.restype = None
+        L.meo_plan_facts.argtypes = [ctypes.c_void_p, ctypes.POINTER(me_b200.MePlanFacts)]
+        L.meo_invert.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, ctypes.c_long, _D, _D,
+                                 ctypes.c_int, ctypes.c_int, _D, _LL]
+        L.meo_synth.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double, _D, _D]
+        L.meo_faddeeva.argtypes = [ctypes.c_int, _D, _D, ctypes.c_long, _D, _D]
+        L.meo_svd.argtypes = [_D, ctypes.c_int, _D, _D]
+        L.meo_svbksb.argtypes = [_D, _D, _D, _D, ctypes.c_int, _D]
+        L.meo_init_guess.argtypes = [ctypes.c_void_p, _D, _D, _D]
+        L.meo_normal_equations.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double,
+                                           ctypes.c_double, _D, _D, _D]
+        L.meo_restart_draws.argtypes = [ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_int, _D]
+        L.meo_restart_draws.restype = None
+        _olib = L
+    return _olib
+
+
+class Oracle:
+    def __init__(self, cfg: me_b200.MeConfig, wavelengths):
+        self.cfg = cfg
+        self.lam = np.ascontiguousarray(wavelengths, dtype=np.float64)
+        self.nl = self.lam.size
+        h = ctypes.c_void_p()
+        st = oracle_lib().meo_plan_create(ctypes.byref(cfg), _p(self.lam), self.nl,
+                                          ctypes.byref(h))
+        assert st == 0, st
+        self.h = h
+        self.carry = np.zeros(1)
+
+    def close(self):
+        if self.h:
+            oracle_lib().meo_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def facts(self):
+        f = me_b200.MePlanFacts()
+        oracle_lib().meo_plan_facts(self.h, ctypes.byref(f))
+        return {"nl": f.nl, "ncut": f.ncut, "ic": f.ic, "i0": f.i0, "i1": f.i1, "npar": f.npar,
+                "bshift": f.bshift,
+                "limits": np.array([[f.limits[i][0], f.limits[i][1]] for i in range(9)]),
+                "fadd_a": f.fadd_a}
+
+    def invert(self, prof, pixel_offset=0, rng_mode=MEO_RNG_COUNTER, nr_seed=0,
+               want_fit=False, counters=False):
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        n = prof.shape[0]
+        res = np.zeros((n, 10))
+        fit = np.zeros((n, 4, self.nl)) if want_fit else None
+        cnt = np.zeros((n, 8), dtype=np.int64) if counters else None
+        st = oracle_lib().meo_invert(self.h, _p(prof), n, pixel_offset, _p(res), _p(fit),
+                                     rng_mode, nr_seed, _p(self.carry),
+                                     cnt.ctypes.data_as(_LL) if counters else None)
+        assert st == 0
+        out = [res]
+        if want_fit:
+            out.append(fit)
+        if counters:
+            out.append(cnt)
+        return out[0] if len(out) == 1 else tuple(out)
+
+    def synth(self, par, deriv=False, step7=1e5):
+        par = np.ascontiguousarray(par, dtype=np.float64)
+        syn = np.zeros(4 * self.nl)
+        jac = np.zeros(36 * self.nl) if deriv else None
+        oracle_lib().meo_synth(self.h, _p(par), int(deriv), step7, _p(syn), _p(jac))
+        return (syn.reshape(4, self.nl), jac.reshape(4, 9, self.nl)) if deriv \
+            else syn.reshape(4, self.nl)
+
+    def synth_many(self, pars):
+        return np.stack([self.synth(p) for p in np.atleast_2d(pars)])
+
+    def init_guess(self, prof):
+        g = np.zeros(9)
+        e = np.zeros(5)
+        st = oracle_lib().meo_init_guess(self.h, _p(np.ascontiguousarray(prof, dtype=np.float64)),
+                                         _p(g), _p(e))
+        return st, g, e
+
+    def normal_equations(self, prof, par, step7, norm0):
+        n = 9 - sum(self.cfg.fixed)
+        H = np.zeros(n * n)
+        g = np.zeros(n)
+        chi = np.zeros(1)
+        oracle_lib().meo_normal_equations(self.h, _p(np.ascontiguousarray(prof, dtype=np.float64)),
+                                          _p(np.ascontiguousarray(par, dtype=np.float64)), step7,
+                                          norm0, _p(H), _p(g), _p(chi))
+        return H.reshape(n, n), g, chi[0]
+
+
+def oracle_faddeeva(nfigures, nu, a):
+    nu = np.ascontiguousarray(nu, dtype=np.float64).ravel()
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    H = np.zeros_like(nu)
+    L = np.zeros_like(nu)
+    oracle_lib().meo_faddeeva(nfigures, _p(nu), _p(a), nu.size, _p(H), _p(L))
+    return H, L
+
+
+def oracle_svd(a):
+    a = np.array(a, dtype=np.float64, copy=True, order="C")
+    n = a.shape[0]
+    w = np.zeros(n)
+    v = np.zeros((n, n))
+    hit = oracle_lib().meo_svd(_p(a), n, _p(w), _p(v))
+    return a, w, v, hit
+
+
+def restart_draws(seed, pixel, run):
+    out = np.zeros(8)
+    oracle_lib().meo_restart_draws(seed, pixel, run, _p(out))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# the reference's own C core
+# ---------------------------------------------------------------------------
+_rlib = None
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _rlib
+    if _rlib is None:
+        L = ctypes.CDLL(REF_SO)
+        L.meref_setup.argtypes = [ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_long, ctypes.c_int,
+                                  ctypes.c_char_p]
+        L.meref_invert.argtypes = [_D, ctypes.c_long, _D, _D]
+        L.meref_plan_facts.argtypes = [ctypes.POINTER(ctypes.c_int), _D]
+        L.meref_get_lm_chisq.restype = ctypes.c_double
+        L.meref_set_lm_chisq.argtypes = [ctypes.c_double]
+        L.meref_set_lm_chisq.restype = None
+        L.meref_synth.argtypes = [_D, ctypes.c_int, ctypes.c_double, _D, _D]
+        L.meref_faddeeva.argtypes = [ctypes.c_int, _D, _D, ctypes.c_long, _D, _D]
+        L.meref_svd.argtypes = [_D, ctypes.c_int, _D, _D]
+        L.meref_svbksb.argtypes = [_D, _D, _D, _D, ctypes.c_int, _D]
+        L.meref_init_guess.argtypes = [_D, _D, _D]
+        L.meref_bounds.argtypes = [_D, _D]
+        L.meref_rng_gauss.argtypes = [ctypes.c_int, ctypes.c_long, _D]
+        _rlib = L
+    return _rlib
+
+
+class Reference:
+    """The reference core, set up once per process (INIT_INV has no teardown)."""
+
+    def __init__(self, ctl_text: str, wavelengths, npix_max: int, seed: int = 12345):
+        self.dir = tempfile.mkdtemp(prefix="meref_")
+        self.ctl = os.path.join(self.dir, "input")
+        with open(self.ctl, "w") as f:
+            f.write(ctl_text.replace("./input", self.ctl))
+        self.lam = np.ascontiguousarray(wavelengths, dtype=np.float64)
+        self.nl = self.lam.size
+        self.npix_max = npix_max
+        st = ref_lib().meref_setup(self.ctl.encode(), _p(self.lam), self.nl, npix_max, seed,
+                                   self.dir.encode())
+        assert st == 0, f"meref_setup: {st}"
+
+    def invert(self, prof, want_fit=False):
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        n = prof.shape[0]
+        res = np.zeros((n, 10))
+        fit = np.zeros((n, 4, self.nl)) if want_fit else None
+        for s in range(0, n, self.npix_max):
+            e = min(n, s + self.npix_max)
+            st = ref_lib().meref_invert(_p(prof[s:e]), e - s, _p(res[s:e]),
+                                        _p(fit[s:e]) if want_fit else None)
+            assert st == 0, st
+        return (res, fit) if want_fit else res
+
+    @property
+    def lm_chisq(self):
+        return ref_lib().meref_get_lm_chisq()
+
+    @lm_chisq.setter
+    def lm_chisq(self, v):
+        ref_lib().meref_set_lm_chisq(float(v))
+
+    def facts(self):
+        ints = (ctypes.c_int * 5)()
+        lim = np.zeros(18)
+        ref_lib().meref_plan_facts(ints, _p(lim))
+        return {"ncut": ints[0], "ic": ints[1], "i0": ints[2], "i1": ints[3], "npar": ints[4],
+                "limits": lim.reshape(9, 2)}
+
+    def synth(self, par, deriv=False, step7=1e5):
+        par = np.ascontiguousarray(par, dtype=np.float64)
+        syn = np.zeros(4 * self.nl)
+        jac = np.zeros(36 * self.nl)
+        ref_lib().meref_synth(_p(par), int(deriv), step7, _p(syn), _p(jac))
+        return (syn.reshape(4, self.nl), jac.reshape(4, 9, self.nl)) if deriv \
+            else syn.reshape(4, self.nl)
+
+    def init_guess(self, prof):
+        g = np.zeros(9)
+        e = np.zeros(5)
+        st = ref_lib().meref_init_guess(_p(np.ascontiguousarray(prof, dtype=np.float64)), _p(g),
+                                        _p(e))
+        return st, g, e
+
+
+def ref_faddeeva(nfigures, nu, a):
+    nu = np.ascontiguousarray(nu, dtype=np.float64).ravel()
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    H = np.zeros_like(nu)
+    L = np.zeros_like(nu)
+    ref_lib().meref_faddeeva(nfigures, _p(nu), _p(a), nu.size, _p(H), _p(L))
+    return H, L
+
+
+def ref_svd(a):
+    a = np.array(a, dtype=np.float64, copy=True, order="C")
+    n = a.shape[0]
+    w = np.zeros(n)
+    v = np.zeros((n, n))
+    ref_lib().meref_svd(_p(a), n, _p(w), _p(v))
+    return a, w, v
+
+
+def ref_rng_gauss(seed, n):
+    out = np.zeros(n)
+    ref_lib().meref_rng_gauss(seed, n, _p(out))
+    return out
