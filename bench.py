@@ -1,0 +1,427 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Milne-Eddington inversion (one JSON line on stdout).
+
+Metric: converged pixels/s on B200 -- pixels inverted per second, counted as
+converged when their chi^2 is <= 1.05 x the chi^2 the reference's FP64 C code
+reaches on the same profile.  The converged share is measured on a seeded
+sample of the map against the reference core (oracle/_ref, the reference's own
+C sources compiled here; the oracle restatement where it was not built).
+
+A step is one inversion of the whole synthetic map (default: the 1024x1024
+Fe I 15648.5 A map, num_run = 5, chisq_criteria = 1.5, FP32 synthesis with FP64
+SVD solve and chi^2 test).  The map (2 GB of FP64 profiles, larger than L2) is
+resident in HBM when the timed region starts; `e2e` times the same step
+through the host entry point me_invert_batch with the profiles in pinned host
+memory (host->device copy, inversion, device->host copy of the results).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...   (one rank per GPU)
+
+With N GPUs every rank inverts its own map (pixels are independent; no
+collective on the data path): scaling is weak, value = all ranks' pixels /
+the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "milne-eddington_b200")
+sys.path.insert(0, PKG)
+
+import me_maps  # noqa: E402
+
+METRIC = "converged pixels/s on 1 B200 at chi2<=1.05x FP64 ref: learned-init vs plain LM"
+UNIT = "pixels/s"
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own C core (or the oracle port) on host cores.
+# ---------------------------------------------------------------------------
+_W = {}
+
+
+def _cpu_worker_init(kind, workload, npix_max, seed, extra):
+    sys.path[:0] = [os.path.join(ROOT, "tests"), PKG]
+    import oracle_bind as ob
+    import me_b200
+    lam = me_maps.wavelengths(workload)
+    _W["kind"] = kind
+    if kind == "reference":
+        _W["eng"] = ob.Reference(me_maps.reference_control_text(workload, extra=extra), lam,
+                                 npix_max, seed=seed)
+    else:
+        cfg = me_b200.parse_config_text(me_maps.control_text(workload, precision="FP64",
+                                                             extra=extra))
+        _W["eng"] = ob.Oracle(cfg, lam)
+
+
+def _cpu_worker_invert(prof):
+    eng = _W["eng"]
+    if _W["kind"] == "reference":
+        return eng.invert(prof)
+    import oracle_bind as ob
+    return eng.invert(prof, rng_mode=ob.MEO_RNG_NR, nr_seed=1)
+
+
+def cpu_kind():
+    return "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libmeref.so")) \
+        else "port"
+
+
+def cpu_invert(prof, workload, procs, extra=None):
+    """Inverts prof [n][4][nl] with `procs` processes of the reference core;
+    returns (results, seconds)."""
+    kind = cpu_kind()
+    n = prof.shape[0]
+    procs = max(1, min(procs, n))
+    chunks = np.array_split(np.arange(n), procs)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs, initializer=_cpu_worker_init,
+                  initargs=(kind, workload, max(len(c) for c in chunks), 4242, extra or {})) as pool:
+        pool.map(_cpu_worker_invert, [prof[c[:1]] for c in chunks])  # warm every worker
+        t0 = time.perf_counter()
+        parts = pool.map(_cpu_worker_invert, [prof[c] for c in chunks])
+        dt = time.perf_counter() - t0
+    return np.concatenate(parts), dt, kind
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_sample_profiles(workload, npix, seed):
+    """Seeded profiles synthesised on the CPU by the oracle (FP64)."""
+    sys.path[:0] = [os.path.join(ROOT, "tests")]
+    import me_b200
+    import oracle_bind as ob
+    lam = me_maps.wavelengths(workload)
+    cfg = me_b200.parse_config_text(me_maps.control_text(workload, precision="FP64"))
+    o = ob.Oracle(cfg, lam)
+    par = me_maps.draw_parameters(workload, npix, seed)
+    return me_maps.add_noise(o.synth_many(par), me_maps.WORKLOADS[workload]["noise"], seed)
+
+
+# ---------------------------------------------------------------------------
+# GPU clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}",
+                                          f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r]
+        except Exception:
+            rows = []
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="fe15648_1024x1024", choices=list(me_maps.WORKLOADS))
+    ap.add_argument("--npix", type=int, default=0, help="override the map size (testing)")
+    ap.add_argument("--precision", default="FP32", choices=["FP32", "FP64"])
+    ap.add_argument("--sample", type=int, default=2048,
+                    help="pixels of the CPU sample (reference timing + converged share)")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="override --sample")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    return ap.parse_args()
+
+
+def reference_arm(args):
+    """The reference's own CPU implementation on this host's cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = me_maps.WORKLOADS[args.workload]
+    cores = host_cores()
+    # ~7 ms of one core per pixel at num_run = 5: a step of ~2 s on all cores
+    npix = args.npix or max(cores * 48, 256)
+    prof = cpu_sample_profiles(args.workload, npix, seed=99)
+    times = []
+    kind = None
+    for i in range(args.warmup + args.steps):
+        _, dt, kind = cpu_invert(prof, args.workload, cores)
+        if i >= args.warmup:
+            times.append(dt)
+    step = max(times)
+    value = npix / step
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded draws of the workload's parameter distributions)",
+            "config": {"workload": args.workload, "pixels_per_step": npix,
+                       "num_run": int(w["ctl"].get("num_run", 4)), "nl": w["nl"],
+                       "cpu_processes": cores},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"{npix} pixels of {args.workload} per step, "
+                                       f"{cores} processes of the reference core"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import me_b200
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    w = me_maps.WORKLOADS[args.workload]
+    name = args.workload
+    npix = args.npix or w["npix"]
+    lam = me_maps.wavelengths(name)
+    nl = lam.size
+    seed = 1000 + rank
+
+    # ---- synthetic map resident in HBM: seeded draws -> GPU FP64 synthesis + noise
+    gen = me_b200.Plan(me_b200.parse_config_text(me_maps.control_text(name, precision="FP64")),
+                       lam, device=local)
+    par_true = me_maps.draw_parameters(name, npix, seed)
+    d_par = torch.from_numpy(par_true).cuda()
+    prof = torch.empty((npix, 4, nl), dtype=torch.float64, device="cuda")
+    gen.synthesize_device(d_par.data_ptr(), npix, prof.data_ptr())
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    prof += w["noise"] * torch.randn(prof.shape, dtype=torch.float64, device="cuda", generator=g)
+    torch.cuda.synchronize()
+    gen.close()
+    res = torch.zeros((npix, 10), dtype=torch.float64, device="cuda")
+
+    cfg = me_b200.parse_config_text(me_maps.control_text(name, precision=args.precision,
+                                                         seed=seed))
+    plan = me_b200.Plan(cfg, lam, device=local)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return plan.invert_device(prof.data_ptr(), npix, res.data_ptr(), 0, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        st = step()
+
+    # ---- timed region: K device-resident steps
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stats = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    step_s = elapsed / args.steps
+    kernel_ms = statistics.mean(s["kernel_ms"] for s in stats)
+    last = stats[-1]
+
+    # ---- end to end through the host entry point (pinned host buffers)
+    e2e = None
+    if args.e2e_steps > 0:
+        h_prof = torch.empty((npix, 4, nl), dtype=torch.float64, pin_memory=True)
+        h_prof.copy_(prof)
+        h_res = np.zeros((npix, 10))
+        h_prof_np = h_prof.numpy()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            r_host, st_e2e = plan.invert(h_prof_np)
+        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"npix": npix, "seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"],
+               "d2h_ms": st_e2e["d2h_ms"]}
+
+    res_np = res.cpu().numpy()
+    out = {}
+    if rank == 0:
+        # ---- CPU leg: the reference core on a seeded sample of this map, timed on
+        # the host cores (cpu_baseline); its chi^2 also decides which of the
+        # GPU's pixels count as converged (chi^2 <= 1.05 x the reference's)
+        cores = host_cores()
+        nb = min(npix, args.cpu_sample or max(args.sample, cores * 32))
+        rng = np.random.default_rng(7)
+        idx = np.sort(rng.choice(npix, size=nb, replace=False))
+        sample_prof = prof[idx].cpu().numpy()
+        ref_res, base_dt, base_kind = cpu_invert(sample_prof, name, cores)
+        cpu_value = nb / base_dt
+        valid = ref_res[:, 9] > 0
+        ratio = res_np[idx, 9][valid] / ref_res[valid, 9]
+        frac = float(np.mean(ratio <= 1.05)) if valid.any() else 0.0
+        ref_kind = base_kind
+
+        # ---- roofline of the inversion kernel: algorithmic FLOPs per launch
+        fc = json.load(open(os.path.join(ROOT, "tests", "golden", "flop_counts.json")))[name]
+
+        def flops(c):
+            return c.get("add", 0) + c.get("mul", 0) + c.get("div", 0) + c.get("sqrt", 0)
+
+        first = last["iterations"]
+        later = last["trials"] - first
+        alg = (last["trials"] * nl * (flops(fc["forward_per_lambda"]) + flops(fc["loss_per_lambda"]))
+               + first * flops(fc["svd_solve_normal_matrix"])
+               + later * flops(fc["svd_solve_orthogonal"])
+               + last["jacobians"] * nl * (flops(fc["jacobian_per_lambda"])
+                                           + flops(fc["normal_equations_per_lambda"])))
+        achieved = alg / (kernel_ms / 1e3) / 1e12
+        clk = clk.summary()
+        peak = fp32_peak_tflops(torch)
+        out = {"ratio_q": [float(np.quantile(ratio, q)) for q in (0.01, 0.5, 0.99)],
+               "frac": frac, "cpu_value": cpu_value, "nb": nb, "base_kind": base_kind,
+               "cores": cores, "achieved": achieved, "alg": alg, "clk": clk, "peak": peak,
+               "ref_kind": ref_kind}
+
+    if dist:
+        dist.barrier()
+    if rank == 0:
+        pix_per_s = npix * world / step_s
+        value = pix_per_s * out["frac"]
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "FP32" else "f64",
+            "data": "synthetic (seeded draws of the workload's parameter distributions, "
+                    "GPU FP64 synthesis + Gaussian noise)",
+            "config": {"workload": name, "pixels_per_gpu": npix, "nl": nl,
+                       "num_run": int(w["ctl"].get("num_run", 4)),
+                       "precision": args.precision, "init": "Init_Guess (plain LM)",
+                       "parallelism": f"pixel shards x{world}",
+                       "l2": "inputs larger than L2 (2 GB of profiles per GPU)",
+                       "raw_pixels_per_s": pix_per_s,
+                       "converged_fraction": out["frac"],
+                       "converged_sample": f"{out['nb']} seeded pixels vs the "
+                                           f"{out['ref_kind']} FP64 chi^2",
+                       "chi2_ratio_q01_q50_q99": out["ratio_q"]},
+            "gpu_launches": int(sum(s["launches"] for s in stats)),
+            "e2e": None, "clocks": out["clk"],
+            "roofline": {"bound": "fp32", "achieved": out["achieved"], "peak": out["peak"],
+                         "unit": "TFLOP/s", "frac": out["achieved"] / out["peak"],
+                         "traffic": None,
+                         "note": "algorithmic FLOPs of the reference algorithm (counted with a "
+                                 "counting scalar type) / inversion-kernel time; peak = FP32 "
+                                 "FFMA throughput measured with cuBLAS SGEMM (TF32 off)",
+                         "algorithmic_flop_per_launch": out["alg"]},
+            "cpu_baseline": {"value": out["cpu_value"], "unit": UNIT, "cores": out["cores"],
+                             "kind": out["base_kind"],
+                             "sample": f"{out['nb']} seeded pixels of the map, "
+                                       f"{out['cores']} processes of the reference core"},
+            "stats": {k: last[k] for k in ("valid", "runs", "iterations", "trials", "accepted",
+                                           "jacobians", "redo_pixels", "launches")},
+        }
+        if e2e:
+            line["e2e"] = {"value": npix * world / e2e["seconds"] * out["frac"], "unit": UNIT,
+                           "h2d_bytes_per_step": npix * 4 * nl * 8,
+                           "d2h_bytes_per_step": npix * 10 * 8,
+                           "h2d_ms": e2e["h2d_ms"], "d2h_ms": e2e["d2h_ms"]}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def fp32_peak_tflops(torch):
+    """FP32 FFMA throughput of this GPU: cuBLAS SGEMM with TF32 disabled."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, device="cuda")
+        b = torch.randn(n, n, device="cuda")
+        for _ in range(2):
+            torch.mm(a, b)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        best = 0.0
+        for _ in range(3):
+            e0.record()
+            torch.mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12)
+        return best
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+
+
+if __name__ == "__main__":
+    sys.exit(main())

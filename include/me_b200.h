@@ -111,6 +111,7 @@ typedef struct me_stats {
   long long jacobians;     /* syntheses with Jacobian + normal equations   */
   long long wavelengths;   /* wavelength points synthesised (both kinds)   */
   long long redo_pixels;   /* pixels re-run to honour the carried LM chi^2 */
+  long long launches;      /* inversion kernel launches made by the call     */
   double kernel_ms;        /* device time of the inversion kernel(s)       */
   double h2d_ms, d2h_ms;   /* host<->device copy time (host entry point)   */
 } me_stats;
@@ -194,6 +195,13 @@ int me_faddeeva(int nfigures, int precision, const double *nu, const double *a, 
 /* Golub-Reinsch SVD of nmat n x n matrices (n <= 9) in FP64 on the device:
  * a = u * diag(w) * v^T.  Replaces svdcmp_double (Src/SVD_TEMPLATE.h:84-344). */
 int me_svd(const double *a, long nmat, int n, double *u, double *w, double *v, int device);
+
+/* Device-buffer variants (work ordered on `stream`, a cudaStream_t; NULL =
+ * the default stream, waited for before returning). */
+int me_svd_device(const double *d_a, long nmat, int n, double *d_u, double *d_w, double *d_v,
+                  void *stream);
+int me_synthesize_jacobian_device(me_plan *plan, const double *d_par, long npix, double step7,
+                                  double *d_prof, double *d_jac, void *stream);
 
 /* Initial guess for npix profiles: guess [npix][9]; extra [npix][5] =
  * norm0, normp, S lower limit, S upper limit, S step; status [npix] (0 ok,

@@ -328,7 +328,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   float ms = 0.f;
   cudaEventElapsedTime(&ms, p->ev0, p->ev1);
   double kernel_ms = ms;
-  long long redo_total = 0;
+  long long redo_total = 0, launches = 1;
   p->h_used.assign(n, INFINITY);
   if (n) p->h_used[0] = p->carry;
   for (int pass = 0; pass < 1 << 20; pass++) {
@@ -351,6 +351,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
       break;
     }
     redo_total += (long long)p->h_list.size();
+    launches++;
     const size_t m = p->h_list.size();
     CK(p->d_list.ensure(m * sizeof(long long)));
     CK(p->d_stale.ensure(n * sizeof(double)));
@@ -387,6 +388,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     stats->jacobians = (long long)tot[5];
     stats->wavelengths = (long long)(tot[3] + tot[5]) * p->P.nl;
     stats->redo_pixels = redo_total;
+    stats->launches = launches;
     stats->kernel_ms = kernel_ms;
   }
   return ME_OK;
@@ -557,5 +559,26 @@ extern "C" int me_init_guess(me_plan *p, const double *prof, long npix, double *
   dg.release();
   de.release();
   ds.release();
+  return ME_OK;
+}
+
+extern "C" int me_svd_device(const double *d_a, long nmat, int n, double *d_u, double *d_w,
+                             double *d_v, void *stream) {
+  if (!d_a || !d_u || !d_w || !d_v || nmat < 0 || n < 1 || n > 9)
+    return fail(ME_ERR_ARG, "bad argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(me::launch_svd(d_a, nmat, n, d_u, d_w, d_v, nullptr, st));
+  if (!stream) CK(cudaStreamSynchronize(st));
+  return ME_OK;
+}
+
+extern "C" int me_synthesize_jacobian_device(me_plan *p, const double *d_par, long npix,
+                                             double step7, double *d_prof, double *d_jac,
+                                             void *stream) {
+  if (!p || !d_par || !d_prof || npix < 0) return fail(ME_ERR_ARG, "null argument");
+  CK(cudaSetDevice(p->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+  CK(me::launch_synth(p->precision, p->P, d_par, npix, step7, d_prof, d_jac, st));
+  if (!stream) CK(cudaStreamSynchronize(st));
   return ME_OK;
 }

@@ -83,6 +83,12 @@ struct VoigtK {
   const T *ea2n2;  // exp(-a^2 n^2), n = 0..49 (shared memory)
 };
 
+// (H, L) pair returned by the Voigt evaluators.
+template <class T>
+struct HL {
+  T h, l;
+};
+
 // erfcx(a) = exp(a^2) erfc(a) with the a > 26.6 asymptotic series (FADDEEVA.c:83-108).
 template <class T>
 __device__ __forceinline__ T erfcx_t(T a) {
@@ -123,7 +129,7 @@ __device__ T dawson_t(T x) {
 
 // Hui, Armstrong & Wray (1978) 6-pole rational approximation (FADDEEVA.c:112-163).
 template <class T>
-__device__ __forceinline__ void voigt_hui6(T nu, T y, T &H, T &L) {
+__device__ __forceinline__ HL<T> voigt_hui6(T nu, T y) {
   const T A[7] = {T(122.607931777104326), T(214.382388694706425), T(181.928533092181549),
                   T(93.155580458138441),  T(30.180142196210589),  T(5.912626209773153),
                   T(0.564189583562615)};
@@ -144,13 +150,13 @@ __device__ __forceinline__ void voigt_hui6(T nu, T y, T &H, T &L) {
     qi = ti;
   }
   T den = qr * qr + qi * qi;
-  H = (pr * qr + pi * qi) / den;
-  L = (pi * qr - pr * qi) / den;
+  return {(pr * qr + pi * qi) / den, (pi * qr - pr * qi) / den};
 }
 
 // Humlicek (1982) W4 (FADDEEVA.c:167-281).  Reached only for Nfigures <= 5.
 template <class T>
-__device__ void voigt_humlicek_w4(T nu, T y, T &H, T &L) {
+__device__ HL<T> voigt_humlicek_w4(T nu, T y) {
+  T H, L;
   const T anu = m_abs(nu);
   const T s = anu + y;
   const T tr = y, ti = -nu;
@@ -214,34 +220,26 @@ __device__ void voigt_humlicek_w4(T nu, T y, T &H, T &L) {
     H = er - (nr * dr + ni * di) / den;
     L = ei - (ni * dr - nr * di) / den;
   }
+  return {H, L};
 }
 
 // Zaghloul & Ali (2011) ACM Algorithm 916 (FADDEEVA.c:286-402).  erfcx_y is
 // erfcx(y), constant over one synthesis, computed once per call by the caller.
 template <class T>
-__device__ __forceinline__ void voigt_alg916(T nu, T y, T erfcx_y, T &H, T &L,
-                                             const VoigtK<T> &K) {
+__device__ __forceinline__ HL<T> voigt_alg916(T nu, T y, T erfcx_y, const VoigtK<T> &K) {
   if (nu == T(0)) {
-    H = erfcx_y;
-    L = 0;
-    return;
+    return {erfcx_y, T(0)};
   } else if (y == T(0)) {
-    H = m_exp(-nu * nu);
-    L = T(2.0 / kSqrtPi) * dawson_t(nu);
-    return;
+    return {m_exp(-nu * nu), T(2.0 / kSqrtPi) * dawson_t(nu)};
   }
   const T x = m_abs(nu), ya = m_abs(y);
   if (x + ya > T(1e7)) {
     if (x < ya) {
       T xs = x / ya;
-      H = T(1) / T(kSqrtPi) / (xs * xs + T(1));
-      L = xs / T(kSqrtPi) / (xs * xs + T(1));
-    } else {
-      T ys = ya / x;
-      H = ys / T(kSqrtPi) / (ys * ys + T(1));
-      L = T(1) / T(kSqrtPi) / (ys * ys + T(1));
+      return {T(1) / T(kSqrtPi) / (xs * xs + T(1)), xs / T(kSqrtPi) / (xs * xs + T(1))};
     }
-    return;
+    T ys = ya / x;
+    return {ys / T(kSqrtPi) / (ys * ys + T(1)), T(1) / T(kSqrtPi) / (ys * ys + T(1))};
   }
   const T xx = x * x, yy = y * y, xy = x * y;
   const T xy2 = T(2) * xy;
@@ -304,21 +302,17 @@ __device__ __forceinline__ void voigt_alg916(T nu, T y, T erfcx_y, T &H, T &L,
     re += a * y * (T(-2) * cos_2xy * s1 + s2) * inv_pi;
     im += a * (T(2) * y * sin_2xy * s1 - s4) * inv_pi;
   }
-  H = re;
-  L = nu > T(0) ? im : -im;
+  return {re, nu > T(0) ? im : -im};
 }
 
 // Accuracy-selected w(z) (Zaghloul 2018 regions; FADDEEVA.c:440-590).
 template <class T>
-__device__ __forceinline__ void voigt(T nu, T y, T erfcx_y, T &H, T &L, const VoigtK<T> &K) {
+__device__ __noinline__ HL<T> voigt(T nu, T y, T erfcx_y, const VoigtK<T> K) {
+  T H, L;
   if (nu == T(0)) {
-    H = erfcx_y;
-    L = 0;
-    return;
+    return {erfcx_y, T(0)};
   } else if (y == T(0)) {
-    H = m_exp(-nu * nu);
-    L = T(2.0 / kSqrtPi) * dawson_t(nu);
-    return;
+    return {m_exp(-nu * nu), T(2.0 / kSqrtPi) * dawson_t(nu)};
   }
   const T zr = nu, zi = y;
   const T z2r = zr * zr - zi * zi;
@@ -343,8 +337,7 @@ __device__ __forceinline__ void voigt(T nu, T y, T erfcx_y, T &H, T &L, const Vo
     L = (wr * pr + z2i * pi) / den;
   } else if (r2 >= K.thr[3]) {
     if ((K.nfig <= 4 && y2 < T(6e-14)) || (K.nfig == 5 && r2 < T(39) && y2 < T(1e-9))) {
-      voigt_humlicek_w4(nu, y, H, L);
-      return;
+      return voigt_humlicek_w4(nu, y);
     }
     T wr = z2r - T(2.5);
     T ar = -(wr * zi + z2i * zr), ai = wr * zr - z2i * zi;
@@ -356,24 +349,21 @@ __device__ __forceinline__ void voigt(T nu, T y, T erfcx_y, T &H, T &L, const Vo
   } else if (r2 >= K.thr[4]) {
     if (K.nfig <= 4) {
       if (y2 < T(0.026))
-        voigt_humlicek_w4(nu, y, H, L);
+        return voigt_humlicek_w4(nu, y);
       else
-        voigt_hui6(nu, y, H, L);
-      return;
+        return voigt_hui6(nu, y);
     } else if (K.nfig == 5) {
       if (y2 >= T(0.27))
-        voigt_hui6(nu, y, H, L);
+        return voigt_hui6(nu, y);
       else if (y2 >= T(1e-9))
-        voigt_alg916(nu, y, erfcx_y, H, L, K);
+        return voigt_alg916(nu, y, erfcx_y, K);
       else
-        voigt_humlicek_w4(nu, y, H, L);
-      return;
+        return voigt_humlicek_w4(nu, y);
     } else if (K.nfig == 6) {
       if (y2 >= T(1))
-        voigt_hui6(nu, y, H, L);
+        return voigt_hui6(nu, y);
       else
-        voigt_alg916(nu, y, erfcx_y, H, L, K);
-      return;
+        return voigt_alg916(nu, y, erfcx_y, K);
     }
     T wr = z2r - T(4.5);
     T ar = -(wr + z2r) * z2i, ai = wr * z2r - z2i * z2i + T(2);
@@ -385,10 +375,11 @@ __device__ __forceinline__ void voigt(T nu, T y, T erfcx_y, T &H, T &L, const Vo
     L = (-ar * ci + ai * cr) / den;
   } else {
     if (K.nfig <= 4)
-      voigt_hui6(nu, y, H, L);
+      return voigt_hui6(nu, y);
     else
-      voigt_alg916(nu, y, erfcx_y, H, L, K);
+      return voigt_alg916(nu, y, erfcx_y, K);
   }
+  return {H, L};
 }
 
 // ---------------------------------------------------------------------------
@@ -431,8 +422,15 @@ __device__ __forceinline__ void synth_setup(SynthCall<T> &c, const double *mp, c
   c.kt = c.eta_half * T(2) * c.sth * c.cth;
   c.kv = c.eta_half * c.cth;
   c.shift_b = T(mp[0] * (P.bshift / mp[4]));
-  // Doppler shift in Doppler widths: 1e3 (lambda - lambda0 - v lambda0 / c) / width
-  c.vshift = T(1e6 * mp[3] * P.lambda0 / kLightSpeed);
+  if (sizeof(T) == sizeof(double)) {
+    // FP64: the reference's own form, ShiftW = 1e3 lambda / width + ShiftV
+    // (Src/ME_SOLVER.c:160-161, 190)
+    c.vshift = T(1e3 * (-1e3 * mp[3] / kLightSpeed * P.lambda0 - P.lambda0) / mp[4]);
+  } else {
+    // FP32: the same quantity without its cancellation,
+    // ShiftW = (1e3 (lambda - lambda0) - 1e6 v lambda0 / c) / width
+    c.vshift = T(1e6 * mp[3] * P.lambda0 / kLightSpeed);
+  }
   c.erfcx_y = erfcx_t<T>(c.p5);
 #pragma unroll
   for (int k = 0; k < 9; k++) c.step[k] = T(step[k]);
@@ -449,7 +447,7 @@ __device__ __forceinline__ float shift_w<float>(const SynthCall<float> &c, const
 template <>
 __device__ __forceinline__ double shift_w<double>(const SynthCall<double> &c, const DevPlan &P,
                                                   int iw) {
-  return (1e3 * __ldg(P.dlambda + iw) - c.vshift) / c.p4;
+  return 1e3 * __ldg(P.lambda + iw) / c.p4 + c.vshift;
 }
 
 // syn[4] = I, Q, U, V; with DERIV also J[4][9] (derivatives scaled by step[]).
@@ -462,8 +460,8 @@ __device__ __forceinline__ void me_point(const SynthCall<T> &c, T w0, const Voig
   for (int k = 0; k < 3; k++) {
     const int q = k - 1;
     const T v = w0 + T(q) * c.shift_b;
-    T H, L;
-    voigt<T>(v, c.p5, c.erfcx_y, H, L, K);
+    const HL<T> hl = voigt<T>(v, c.p5, c.erfcx_y, K);
+    const T H = hl.h, L = hl.l;
     phi[k] = H * rsp;
     psi[k] = L * rsp;
     if (DERIV) {
@@ -621,7 +619,8 @@ struct PixelInit {
 
 // Returns 1 when mean(I) < Icriteria (or the mean is NaN), as Init_Guess /
 // the INVERSION_MULTI gate.
-__device__ inline int init_guess(const double *prof, const DevPlan &P, PixelInit &o) {
+static __device__ __noinline__ int init_guess(const double *prof, const DevPlan &P, PixelInit &o,
+                                       bool nan_gate) {
   const int nw = P.nl;
   const double *pI = prof, *pQ = prof + nw, *pU = prof + 2 * nw, *pV = prof + 3 * nw;
   const double lam0 = P.lambda0;
@@ -652,7 +651,9 @@ __device__ inline int init_guess(const double *prof, const DevPlan &P, PixelInit
     }
   }
   const double imean = isum / nw;
-  if (isnan(imean) || imean < P.icriteria) return 1;
+  // Init_Guess tests only Imean < Icriteria; INVERSION_MULTI also rejects a
+  // NaN mean before calling it (Src/LM_FIT.c:783)
+  if ((nan_gate && isnan(imean)) || imean < P.icriteria) return 1;
   o.norm0 = 1e-2 * imean;
   o.norm0 *= o.norm0;
   const double is2 = isum * isum;
@@ -755,7 +756,7 @@ __device__ __forceinline__ double pythag_d(double a, double b) {
   return mx * sqrt(1.0 + r * r);
 }
 
-__device__ inline int gr_svd(double *a, int n, double *w, double *v) {
+static __device__ __noinline__ int gr_svd(double *a, int n, double *w, double *v) {
 #define A_(i, j) a[(i) * n + (j)]
 #define V_(i, j) v[(i) * n + (j)]
   const int m = n;

@@ -97,7 +97,7 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, const VoigtK<T> &
 // residuals and their squares accumulate in FP64.  fit (nullable) receives
 // the synthetic profile.
 template <class T>
-__device__ __forceinline__ double forward_pass(const DevPlan &P, const VoigtK<T> &K,
+__device__ __noinline__ double forward_pass(const DevPlan &P, const VoigtK<T> &K,
                                                const double *par, const double *step,
                                                const double *prof, const double sw[4],
                                                double *fit) {
@@ -139,7 +139,7 @@ enum : int { S_FETCH = 0, S_START = 1, S_NEXT = 2, S_TRIAL = 3, S_DONE = 4 };
 using namespace detail;
 
 template <class T>
-__global__ void __launch_bounds__(kInvertBlock) invert_kernel(const DevPlan P, InvertArgs A) {
+__global__ void __launch_bounds__(kInvertBlock, ME_INV_MINB) invert_kernel(const DevPlan P, InvertArgs A) {
   __shared__ T s_tab[50];
   fill_table<T>(P, s_tab);
   VoigtK<T> K;
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kInvertBlock) invert_kernel(const DevPlan P, I
       }
       pix = A.list ? A.list[k] : (long long)k;
       pp = A.prof + (size_t)pix * 4 * nl;
-      const int bad = init_guess(pp, P, pin);  // also the INVERSION_MULTI gate
+      const int bad = init_guess(pp, P, pin, true);  // also the INVERSION_MULTI gate
       if (bad || P.nruns <= 0) {
 #pragma unroll
         for (int i = 0; i < 10; i++) A.res[(size_t)pix * 10 + i] = 0.0;

@@ -9,6 +9,11 @@
 namespace me {
 
 constexpr int kInvertBlock = 128;
+// minimum resident CTAs per SM the inversion kernel is compiled for (caps
+// its registers at 65536 / (128 * ME_INV_MINB))
+#ifndef ME_INV_MINB
+#define ME_INV_MINB 3
+#endif
 
 // Buffers of one inversion launch (all device pointers).
 struct InvertArgs {

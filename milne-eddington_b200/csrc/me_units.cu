@@ -77,11 +77,10 @@ __global__ void voigt_kernel(const DevPlan P, const double *nu, const double *a,
   load_voigt<T>(K, P, s_tab);
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  T h, l;
   const T y = T(a[i]);
-  voigt<T>(T(nu[i]), y, erfcx_t<T>(y), h, l, K);
-  H[i] = (double)h;
-  L[i] = (double)l;
+  const HL<T> r = voigt<T>(T(nu[i]), y, erfcx_t<T>(y), K);
+  H[i] = (double)r.h;
+  L[i] = (double)r.l;
 }
 
 __global__ void svd_kernel(const double *a, long long nmat, int n, double *u, double *w,
@@ -104,7 +103,7 @@ __global__ void init_guess_kernel(const DevPlan P, const double *prof, long long
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= npix) return;
   PixelInit o;
-  const int st = init_guess(prof + (size_t)i * 4 * P.nl, P, o);
+  const int st = init_guess(prof + (size_t)i * 4 * P.nl, P, o, false);
   status[i] = st;
   for (int k = 0; k < 9; k++) guess[i * 9 + k] = st ? 0.0 : o.guess[k];
   extra[i * 5 + 0] = st ? 0.0 : o.norm0;

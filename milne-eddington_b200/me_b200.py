@@ -111,6 +111,7 @@ class MeStats(ctypes.Structure):
         ("jacobians", ctypes.c_longlong),
         ("wavelengths", ctypes.c_longlong),
         ("redo_pixels", ctypes.c_longlong),
+        ("launches", ctypes.c_longlong),
         ("kernel_ms", ctypes.c_double),
         ("h2d_ms", ctypes.c_double),
         ("d2h_ms", ctypes.c_double),
@@ -126,7 +127,8 @@ EXPORTED = [
     "me_config_parse_text", "me_plan_create", "me_plan_destroy", "me_plan_get_facts",
     "me_plan_get_carry_chisq", "me_plan_set_carry_chisq", "me_plan_grid", "me_plan_set_grid",
     "me_invert_batch", "me_invert_batch_device", "me_synthesize", "me_synthesize_device",
-    "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess",
+    "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
+    "me_synthesize_jacobian_device",
 ]
 
 
@@ -179,6 +181,12 @@ def lib() -> ctypes.CDLL:
         L.me_faddeeva.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, ctypes.c_long, _D, _D,
                                   ctypes.c_int]
         L.me_svd.argtypes = [_D, ctypes.c_long, ctypes.c_int, _D, _D, _D, ctypes.c_int]
+        L.me_svd_device.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.me_synthesize_jacobian_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_long, ctypes.c_double,
+                                                    ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p]
         L.me_init_guess.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                     ctypes.POINTER(ctypes.c_int)]
         _lib = L
@@ -313,6 +321,14 @@ class Plan:
                                           ctypes.c_void_p(stream) if stream else None),
                "me_synthesize_device")
 
+    def synthesize_jacobian_device(self, d_par: int, npix: int, step7: float, d_prof: int,
+                                   d_jac: int, stream: int = 0):
+        _check(lib().me_synthesize_jacobian_device(self._h, ctypes.c_void_p(d_par), npix,
+                                                   float(step7), ctypes.c_void_p(d_prof),
+                                                   ctypes.c_void_p(d_jac) if d_jac else None,
+                                                   ctypes.c_void_p(stream) if stream else None),
+               "me_synthesize_jacobian_device")
+
     def synthesize_jacobian(self, par: np.ndarray, step7: float):
         par = np.ascontiguousarray(par, dtype=np.float64).reshape(-1, 9)
         n = par.shape[0]
@@ -343,6 +359,12 @@ def faddeeva(nfigures: int, nu: np.ndarray, a: np.ndarray, precision: int = ME_P
     _check(lib().me_faddeeva(nfigures, precision, _ptr(nu), _ptr(a), nu.size, _ptr(H), _ptr(L),
                              device), "me_faddeeva")
     return H, L
+
+
+def svd_device(d_a: int, nmat: int, n: int, d_u: int, d_w: int, d_v: int, stream: int = 0):
+    _check(lib().me_svd_device(ctypes.c_void_p(d_a), nmat, n, ctypes.c_void_p(d_u),
+                               ctypes.c_void_p(d_w), ctypes.c_void_p(d_v),
+                               ctypes.c_void_p(stream) if stream else None), "me_svd_device")
 
 
 def svd(a: np.ndarray, device: int = 0):

@@ -10,6 +10,7 @@
 // change of its inputs for about a quarter of the pixels of a configs-0 map).
 // Build: oracle/Makefile (-ffp-contract=off).
 #include "me_oracle.h"
+#include "flop_count.h"
 
 #include <math.h>
 #include <stdint.h>
@@ -48,36 +49,38 @@ struct VoigtTables {  // STRUCT_FADDEEVA, Src/FADDEEVA.h; Faddeeva_init Src/FADD
 };
 
 // Dawson's integral, Rybicki's method as in Numerical Recipes (Src/FADDEEVA.c:29-79).
-double dawson(double x) {
-  const double A1 = 2.0 / 3.0, A2 = 0.4, A3 = 2.0 / 7.0, H = 0.4;
-  double ax = fabs(x);
+template <class R>
+R dawson(R x) {
+  const R A1 = 2.0 / 3.0, A2 = 0.4, A3 = 2.0 / 7.0, H = 0.4;
+  R ax = fabs(x);
   if (ax < 0.2) {
-    double x2 = x * x;
+    R x2 = x * x;
     return x * (1.0 - A1 * x2 * (1.0 - A2 * x2 * (1.0 - A3 * x2)));
   }
-  double c[7];
+  R c[7];
   for (int i = 1; i <= 6; i++) {
-    double t = (2.0 * i - 1.0) * H;
+    R t = (2.0 * i - 1.0) * H;
     c[i] = exp(-t * t);
   }
   int n0 = 2 * (int)round(ax / (2 * H));
-  double xp = ax - n0 * H;
-  double e1 = exp(2.0 * xp * H);
-  double e2 = e1 * e1;
-  double d1 = n0 + 1;
-  double d2 = d1 - 2.0;
-  double sum = 0.0;
+  R xp = ax - n0 * H;
+  R e1 = exp(2.0 * xp * H);
+  R e2 = e1 * e1;
+  R d1 = n0 + 1;
+  R d2 = d1 - 2.0;
+  R sum = 0.0;
   for (int i = 1; i <= 6; i++, d1 += 2.0, d2 -= 2.0, e1 *= e2)
     sum += c[i] * (e1 / d1 + 1.0 / (d2 * e1));
-  double t = exp(-xp * xp);
+  R t = exp(-xp * xp);
   return 0.5641895835 * copysign(t, x) * sum;
 }
 
 // erfcx(a) = exp(a^2) erfc(a), with the large-argument asymptotic series
 // (Src/FADDEEVA.c:83-108).
-double erfcx_ref(double a) {
+template <class R>
+R erfcx_ref(R a) {
   if (a > 26.6) {
-    double a2 = a * a;
+    R a2 = a * a;
     return ((((((162.421875 / a2 - 29.53125) / a2 + 6.5625) / a2 - 1.875) / a2 + 0.75) / a2 -
              0.5) / a2 + 1) / kSqrtPi / a;
   }
@@ -85,19 +88,20 @@ double erfcx_ref(double a) {
 }
 
 // Hui, Armstrong & Wray (1978) 6-pole rational approximation (Src/FADDEEVA.c:112-163).
-void voigt_hui6(double nu, double y, double *H, double *L) {
-  static const double A[7] = {122.607931777104326, 214.382388694706425, 181.928533092181549,
+template <class R>
+void voigt_hui6(R nu, R y, R *H, R *L) {
+  static const R A[7] = {122.607931777104326, 214.382388694706425, 181.928533092181549,
                               93.155580458138441,  30.180142196210589,  5.912626209773153,
                               0.564189583562615};
-  static const double B[7] = {122.60793177387535,  352.730625110963558, 457.334478783897737,
+  static const R B[7] = {122.60793177387535,  352.730625110963558, 457.334478783897737,
                               348.703917719495792, 170.354001821091472, 53.992906912940207,
                               10.479857114260399};
-  const double zr = y, zi = -nu;
-  double pr = A[6], pi = 0.0;
-  double qr = B[6] + zr, qi = zi;
+  const R zr = y, zi = -nu;
+  R pr = A[6], pi = 0.0;
+  R qr = B[6] + zr, qi = zi;
   for (int k = 5; k >= 0; k--) {
-    double tr = pr * zr - pi * zi + A[k];
-    double ti = pr * zi + pi * zr;
+    R tr = pr * zr - pi * zi + A[k];
+    R ti = pr * zi + pi * zr;
     pr = tr;
     pi = ti;
     tr = qr * zr - qi * zi + B[k];
@@ -105,69 +109,70 @@ void voigt_hui6(double nu, double y, double *H, double *L) {
     qr = tr;
     qi = ti;
   }
-  double den = qr * qr + qi * qi;
+  R den = qr * qr + qi * qi;
   *H = (pr * qr + pi * qi) / den;
   *L = (pi * qr - pr * qi) / den;
 }
 
 // Humlicek (1982) W4, four regions (Src/FADDEEVA.c:167-281).
-void voigt_humlicek_w4(double nu, double y, double *H, double *L) {
-  const double anu = fabs(nu);
-  const double s = anu + y;
-  const double tr = y, ti = -nu;
+template <class R>
+void voigt_humlicek_w4(R nu, R y, R *H, R *L) {
+  const R anu = fabs(nu);
+  const R s = anu + y;
+  const R tr = y, ti = -nu;
   if (s >= 15) {
-    const double ur = tr * tr - ti * ti, ui = 2.0 * tr * ti;
-    double dr = 0.5 + ur, di = ui;
-    double den = dr * dr + di * di;
+    const R ur = tr * tr - ti * ti, ui = 2.0 * tr * ti;
+    R dr = 0.5 + ur, di = ui;
+    R den = dr * dr + di * di;
     *H = 0.56418958355 * (tr * dr + ti * di) / den;
     *L = 0.56418958355 * (ti * dr - tr * di) / den;
   } else if (s >= 5.5) {
-    const double ur = tr * tr - ti * ti, ui = 2.0 * tr * ti;
-    double nr = 1.4104739589 + 0.5641896 * ur;
-    double ni = 0.5641896 * ui;
-    double dr = 0.75 + 3.0 * ur + (ur * ur - ui * ui);
-    double di = 3.0 * ui + 2.0 * ur * ui;
-    double den = dr * dr + di * di;
-    double qr = (nr * dr + ni * di) / den;
-    double qi = (ni * dr - nr * di) / den;
+    const R ur = tr * tr - ti * ti, ui = 2.0 * tr * ti;
+    R nr = 1.4104739589 + 0.5641896 * ur;
+    R ni = 0.5641896 * ui;
+    R dr = 0.75 + 3.0 * ur + (ur * ur - ui * ui);
+    R di = 3.0 * ui + 2.0 * ur * ui;
+    R den = dr * dr + di * di;
+    R qr = (nr * dr + ni * di) / den;
+    R qi = (ni * dr - nr * di) / den;
     *H = tr * qr - ti * qi;
     *L = tr * qi + ti * qr;
   } else if (y >= 1.95 * anu - 0.176) {
-    const double c[5] = {0.5642236, 3.778987, 11.96482, 20.20933, 16.4955};
-    const double d[6] = {1.0, 6.699398, 21.69274, 39.27121, 38.82363, 16.4955};
-    double nr = c[0], ni = 0, dr = d[0], di = 0;
+    const R c[5] = {0.5642236, 3.778987, 11.96482, 20.20933, 16.4955};
+    const R d[6] = {1.0, 6.699398, 21.69274, 39.27121, 38.82363, 16.4955};
+    R nr = c[0], ni = 0, dr = d[0], di = 0;
     for (int k = 1; k < 5; k++) {
-      double r = nr * tr - ni * ti + c[k];
-      double i = nr * ti + ni * tr;
+      R r = nr * tr - ni * ti + c[k];
+      R i = nr * ti + ni * tr;
       nr = r;
       ni = i;
     }
     for (int k = 1; k < 6; k++) {
-      double r = dr * tr - di * ti + d[k];
-      double i = dr * ti + di * tr;
+      R r = dr * tr - di * ti + d[k];
+      R i = dr * ti + di * tr;
       dr = r;
       di = i;
     }
-    double den = dr * dr + di * di;
+    R den = dr * dr + di * di;
     *H = (nr * dr + ni * di) / den;
     *L = (ni * dr - nr * di) / den;
   } else {
     const double c[7] = {0.5641900381, 1.320521697, 35.7668278,  219.0312964,
                          1540.786893,  3321.990492, 36183.30536};
-    const double d[8] = {1,           1.841438936, 61.57036588, 364.2190727,
+    const R d[8] = {1,           1.841438936, 61.57036588, 364.2190727,
                          2186.181081, 9022.227659, 24322.84021, 32066.59372};
-    const double ur = tr * tr - ti * ti, ui = 2.0 * tr * ti;
-    double eu = exp(ur);
-    double er = eu * cos(ui), ei = eu * sin(ui);
-    double nr = c[0], ni = 0, dr = d[0], di = 0;
+    const R ur = tr * tr - ti * ti, ui = 2.0 * tr * ti;
+    R eu = exp(ur);
+    R er = eu * cos(ui), ei = eu * sin(ui);
+    R nr = c[0], ni = 0, dr = d[0], di = 0;
     for (int k = 1; k < 7; k++) {
-      double r = -(nr * ur - ni * ui) + c[k];
-      double i = -(nr * ui + ni * ur);
+      R r = -(nr * ur - ni * ui) + c[k];
+      R i = -(nr * ui + ni * ur);
       nr = r;
       ni = i;
     }
-    double r = nr * tr - ni * ti;
-    double i = nr * ti + ni * tr;
+    R r = nr * tr - ni * ti;
+    R i = nr * ti + ni * tr;
     nr = r;
     ni = i;
     for (int k = 1; k < 8; k++) {
@@ -176,14 +181,15 @@ void voigt_humlicek_w4(double nu, double y, double *H, double *L) {
       dr = r;
       di = i;
     }
-    double den = dr * dr + di * di;
+    R den = dr * dr + di * di;
     *H = er - (nr * dr + ni * di) / den;
     *L = ei - (ni * dr - nr * di) / den;
   }
 }
 
 // Zaghloul & Ali (2011) ACM Algorithm 916 (Src/FADDEEVA.c:286-402).
-void voigt_alg916(double nu, double y, double *H, double *L, const VoigtTables &f) {
+template <class R>
+void voigt_alg916(R nu, R y, R *H, R *L, const VoigtTables &f) {
   if (nu == 0) {
     *H = erfcx_ref(y);
     *L = 0;
@@ -193,24 +199,24 @@ void voigt_alg916(double nu, double y, double *H, double *L, const VoigtTables &
     *L = 2.0 / kSqrtPi * dawson(nu);
     return;
   }
-  const double x = fabs(nu), ya = fabs(y);
+  const R x = fabs(nu), ya = fabs(y);
   if (x + ya > 1e7) {
     if (x < ya) {
-      double xs = x / ya;
+      R xs = x / ya;
       *H = 1. / kSqrtPi / (xs * xs + 1.);
       *L = xs / kSqrtPi / (xs * xs + 1.);
     } else {
-      double ys = ya / x;
+      R ys = ya / x;
       *H = ys / kSqrtPi / (ys * ys + 1.);
       *L = 1. / kSqrtPi / (ys * ys + 1.);
     }
     return;
   }
-  const double xx = x * x, yy = y * y, xy = x * y;
-  const double xy2 = 2 * xy;
-  const double sin_xy = sin(xy), sin_2xy = sin(xy2), cos_2xy = cos(xy2);
-  const double exp_xx = exp(-xx), exp_2ax = exp(2 * f.a * x);
-  const double k1 = exp_xx * erfcx_ref(y);
+  const R xx = x * x, yy = y * y, xy = x * y;
+  const R xy2 = 2 * xy;
+  const R sin_xy = sin(xy), sin_2xy = sin(xy2), cos_2xy = cos(xy2);
+  const R exp_xx = exp(-xx), exp_2ax = exp(2 * f.a * x);
+  const R k1 = exp_xx * erfcx_ref(y);
 
   const int nmax1 = (int)(sqrt(f.log_rmin0 - x * x) / f.a + 0.5);
   const int nmax2 = (int)((f.sqrt_log_rmin0 - x) / f.a + 0.5);
@@ -219,23 +225,23 @@ void voigt_alg916(double nu, double y, double *H, double *L, const VoigtTables &
 
   int nb = (int)(x / f.a + 0.5);
   int nf = nb + 1;
-  const double dxf = f.a * nf - x;
-  const double dxb = x - f.a * nb;
+  const R dxf = f.a * nf - x;
+  const R dxb = x - f.a * nb;
   int nmaxf = (int)((f.sqrt_log_rmin0 - dxf) / f.a);
   int nmaxb = (int)((f.sqrt_log_rmin0 - dxb) / f.a);
   if (nmaxf >= f.nmax) nmaxf = f.nmax - 1;
   if (nmaxb >= f.nmax) nmaxb = f.nmax - 1;
   const int nlo = (nb - nmaxb) > 1 ? (nb - nmaxb) : 1;
 
-  double re = k1 * cos_2xy + 2 * f.a * x * sin_xy * exp_xx * sin_xy / xy / M_PI;
-  double im = -k1 * sin_2xy + 2 * f.a * x * exp_xx * sin_2xy / xy2 / M_PI;
-  double s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
+  R re = k1 * cos_2xy + 2 * f.a * x * sin_xy * exp_xx * sin_xy / xy / M_PI;
+  R im = -k1 * sin_2xy + 2 * f.a * x * exp_xx * sin_2xy / xy2 / M_PI;
+  R s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
 
-  double e1 = exp(-dxf * dxf);
-  double e2 = exp(-2 * f.a * dxf);
-  double ep = 1.;
+  R e1 = exp(-dxf * dxf);
+  R e2 = exp(-2 * f.a * dxf);
+  R ep = 1.;
   for (int n = nf; n <= nf + nmaxf; n++) {
-    double t = e1 * f.exp_a2n2[n - nf] / (f.aa * n * n + yy);
+    R t = e1 * f.exp_a2n2[n - nf] / (R(f.aa) * n * n + yy);
     s3 += t * ep;
     s5 += t * ep * f.a * n;
     ep *= e2;
@@ -244,7 +250,7 @@ void voigt_alg916(double nu, double y, double *H, double *L, const VoigtTables &
   e2 = exp(-2 * f.a * dxb);
   ep = 1.;
   for (int n = nb; n >= nlo; n--) {
-    double t = e1 * f.exp_a2n2[nb - n] / (f.aa * n * n + yy);
+    R t = e1 * f.exp_a2n2[nb - n] / (R(f.aa) * n * n + yy);
     s3 += t * ep;
     s5 += t * ep * f.a * n;
     ep *= e2;
@@ -254,7 +260,7 @@ void voigt_alg916(double nu, double y, double *H, double *L, const VoigtTables &
   if (x < f.sqrt_log_rmin0 || x < 10) {
     ep = 1.;
     for (int n = 1; n <= nmax; n++) {
-      double t = exp_xx * f.exp_a2n2[n] / (f.aa * n * n + yy);
+      R t = exp_xx * f.exp_a2n2[n] / (R(f.aa) * n * n + yy);
       s1 += t;
       ep /= exp_2ax;
       s2 += t * ep;
@@ -268,7 +274,8 @@ void voigt_alg916(double nu, double y, double *H, double *L, const VoigtTables &
 }
 
 // Accuracy-selected w(z) (Zaghloul 2018 region thresholds), Src/FADDEEVA.c:440-590.
-void voigt(double nu, double y, double *H, double *L, const VoigtTables &f) {
+template <class R>
+void voigt(R nu, R y, R *H, R *L, const VoigtTables &f) {
   if (nu == 0) {
     *H = erfcx_ref(y);
     *L = 0;
@@ -279,31 +286,31 @@ void voigt(double nu, double y, double *H, double *L, const VoigtTables &f) {
     return;
   }
   // |z|^2 region boundaries per accuracy row (Src/FADDEEVA.c:471-477)
-  static const double T[5][5] = {{1.6e4, 160.0, 107.0, 28.5, 3.5},
+  static const R T[5][5] = {{1.6e4, 160.0, 107.0, 28.5, 3.5},
                                  {1.5e5, 510.0, 110.0, 39., -0.1},
                                  {1.451e6, 1.6e3, 180.0, 110.0, -0.1},
                                  {1.5e7, 5.01e3, 380.0, 115.0, 114.0},
                                  {1.3e8, 1.6e4, 810.0, 195.0, 116.0}};
-  const double *t = T[f.row];
-  const double zr = nu, zi = y;
-  const double z2r = zr * zr - zi * zi;
-  const double z2i = 2.0 * zr * zi;
-  const double r2 = zr * zr + zi * zi;
-  const double y2 = y * y;
+  const R *t = T[f.row];
+  const R zr = nu, zi = y;
+  const R z2r = zr * zr - zi * zi;
+  const R z2i = 2.0 * zr * zi;
+  const R r2 = zr * zr + zi * zi;
+  const R y2 = y * y;
   if (r2 >= t[0]) {
-    double den = kSqrtPi * (zr * zr + zi * zi);
+    R den = kSqrtPi * (zr * zr + zi * zi);
     *H = zi / den;
     *L = zr / den;
   } else if (r2 >= t[1]) {
-    double wr = z2r - 0.5;
-    double den = kSqrtPi * (wr * wr + z2i * z2i);
+    R wr = z2r - 0.5;
+    R den = kSqrtPi * (wr * wr + z2i * z2i);
     *H = (-zi * wr + zr * z2i) / den;
     *L = (zr * wr + zi * z2i) / den;
   } else if (r2 >= t[2]) {
-    double wr = z2r - 1.5;
-    double pr = wr * zr - z2i * zi;
-    double pi = wr * zi + z2i * zr;
-    double den = kSqrtPi * (pr * pr + pi * pi);
+    R wr = z2r - 1.5;
+    R pr = wr * zr - z2i * zi;
+    R pi = wr * zi + z2i * zr;
+    R den = kSqrtPi * (pr * pr + pi * pi);
     wr = z2r - 1.0;
     *H = (-z2i * pr + wr * pi) / den;
     *L = (wr * pr + z2i * pi) / den;
@@ -315,13 +322,13 @@ void voigt(double nu, double y, double *H, double *L, const VoigtTables &f) {
       voigt_humlicek_w4(nu, y, H, L);
       return;
     }
-    double wr = z2r - 2.5;
-    double ar = -(wr * zi + z2i * zr);
-    double ai = wr * zr - z2i * zi;
+    R wr = z2r - 2.5;
+    R ar = -(wr * zi + z2i * zr);
+    R ai = wr * zr - z2i * zi;
     wr = z2r - 3.;
-    double br = wr * z2r - z2i * z2i + 0.75;
-    double bi = (wr + z2r) * z2i;
-    double den = kSqrtPi * (br * br + bi * bi);
+    R br = wr * z2r - z2i * z2i + 0.75;
+    R bi = (wr + z2r) * z2i;
+    R den = kSqrtPi * (br * br + bi * bi);
     *H = (ar * br + ai * bi) / den;
     *L = (-ar * bi + ai * br) / den;
   } else if (r2 >= t[4]) {
@@ -346,15 +353,15 @@ void voigt(double nu, double y, double *H, double *L, const VoigtTables &f) {
         voigt_alg916(nu, y, H, L, f);
       return;
     }
-    double wr = z2r - 4.5;
-    double ar = -(wr + z2r) * z2i;
-    double ai = wr * z2r - z2i * z2i + 2.;
+    R wr = z2r - 4.5;
+    R ar = -(wr + z2r) * z2i;
+    R ai = wr * z2r - z2i * z2i + 2.;
     wr = z2r - 5.;
-    double br = wr * z2r - z2i * z2i + 3.75;
-    double bi = (wr + z2r) * z2i;
-    double cr = br * zr - bi * zi;
-    double ci = br * zi + bi * zr;
-    double den = kSqrtPi * (cr * cr + ci * ci);
+    R br = wr * z2r - z2i * z2i + 3.75;
+    R bi = (wr + z2r) * z2i;
+    R cr = br * zr - bi * zi;
+    R ci = br * zi + bi * zr;
+    R den = kSqrtPi * (cr * cr + ci * ci);
     *H = (ar * cr + ai * ci) / den;
     *L = (-ar * ci + ai * cr) / den;
   } else {
@@ -505,45 +512,46 @@ void bounds(double *p, const double lim[9][2]) {
 
 // Milne_Eddington_Single (Src/ME_SOLVER.c:101-366).  syn [4][nw]; jac
 // [4][9][nw] scaled by step[] when deriv.
-void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *step, double *syn,
-                double *jac) {
+template <class R>
+void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *step, R *syn,
+                R *jac) {
   const int nw = P.nw;
-  const double p4 = mp[4], p5 = mp[5], p6 = mp[6], p7 = mp[7], p8 = mp[8];
-  const double eta_half = 0.5 * p6;
-  const double b0 = p7 * p8;
-  const double b1 = p7 - b0;
-  const double bsh_n = P.bshift / p4;
-  const double lam_n = P.lambda0 / p4;
-  const double sth = sin(mp[1]);
-  const double cth = cos(mp[1]);
-  const double sth2 = sth * sth;
-  const double cth2p1 = cth * cth + 1;
-  const double c2p = cos(2. * mp[2]);
-  const double s2p = sin(2. * mp[2]);
-  const double kq = eta_half * sth2 * c2p;   // ScSqCs2
-  const double ku = eta_half * sth2 * s2p;   // ScSqSc2
-  const double kt = eta_half * 2.0 * sth * cth;  // ScCsB2
-  const double kv = eta_half * cth;          // CsB2
-  const double shift_b = mp[0] * bsh_n;
-  const double shift_v = 1e3 * (-1e3 * mp[3] / kLightSpeed * P.lambda0 - P.lambda0) / p4;
-  double *sI = syn, *sQ = syn + nw, *sU = syn + 2 * nw, *sV = syn + 3 * nw;
-  double *jI = jac, *jQ = jac ? jac + 9 * nw : nullptr, *jU = jac ? jac + 18 * nw : nullptr,
-         *jV = jac ? jac + 27 * nw : nullptr;
-  const double s7 = step[7], s8 = step[8];
+  const R p4 = mp[4], p5 = mp[5], p6 = mp[6], p7 = mp[7], p8 = mp[8];
+  const R eta_half = 0.5 * p6;
+  const R b0 = p7 * p8;
+  const R b1 = p7 - b0;
+  const R bsh_n = P.bshift / p4;
+  const R lam_n = P.lambda0 / p4;
+  const R sth = sin(mp[1]);
+  const R cth = cos(mp[1]);
+  const R sth2 = sth * sth;
+  const R cth2p1 = cth * cth + 1;
+  const R c2p = cos(2. * mp[2]);
+  const R s2p = sin(2. * mp[2]);
+  const R kq = eta_half * sth2 * c2p;   // ScSqCs2
+  const R ku = eta_half * sth2 * s2p;   // ScSqSc2
+  const R kt = eta_half * 2.0 * sth * cth;  // ScCsB2
+  const R kv = eta_half * cth;          // CsB2
+  const R shift_b = mp[0] * bsh_n;
+  const R shift_v = 1e3 * (-1e3 * mp[3] / kLightSpeed * P.lambda0 - P.lambda0) / p4;
+  R *sI = syn, *sQ = syn + nw, *sU = syn + 2 * nw, *sV = syn + 3 * nw;
+  R *jI = jac, *jQ = jac ? jac + 9 * nw : nullptr, *jU = jac ? jac + 18 * nw : nullptr,
+    *jV = jac ? jac + 27 * nw : nullptr;
+  const R s7 = step[7], s8 = step[8];
 
   for (int iw = 0; iw < nw; iw++) {
-    double phi[3], psi[3], dphi[3][6], dpsi[3][6];
-    double shift_w = 1e3 * P.lambda[iw] / p4 + shift_v;
+    R phi[3], psi[3], dphi[3][6], dpsi[3][6];
+    R shift_w = 1e3 * P.lambda[iw] / p4 + shift_v;
     for (int q = -1; q <= 1; q++) {
       int k = q + 1;
-      double v = shift_w + q * shift_b;
-      double H = 0, L = 0;
+      R v = shift_w + q * shift_b;
+      R H = 0, L = 0;
       voigt(v, p5, &H, &L, P.vt);
       phi[k] = H / kSqrtPi;
       psi[k] = L / kSqrtPi;
       if (deriv) {
-        double dH = 2. * (-v * H + p5 * L) / kSqrtPi;
-        double dL = -2. * (-1. / kSqrtPi + p5 * H + v * L) / kSqrtPi;
+        R dH = 2. * (-v * H + p5 * L) / kSqrtPi;
+        R dL = -2. * (-1. / kSqrtPi + p5 * H + v * L) / kSqrtPi;
         dphi[k][0] = q * bsh_n * dH;
         dpsi[k][0] = q * bsh_n * dL;
         dphi[k][3] = -1e6 / kLightSpeed * lam_n * dH;
@@ -554,10 +562,10 @@ void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *s
         dpsi[k][5] = dH;
       }
     }
-    double eta[4], rho[4];
-    double phis = 0.5 * (phi[0] + phi[2]);
-    double phit = phi[1] - phis;
-    double psit = psi[1] - 0.5 * (psi[0] + psi[2]);
+    R eta[4], rho[4];
+    R phis = 0.5 * (phi[0] + phi[2]);
+    R phit = phi[1] - phis;
+    R psit = psi[1] - 0.5 * (psi[0] + psi[2]);
     eta[0] = eta_half * (phi[1] * sth2 + phis * cth2p1);
     eta[1] = phit * kq;
     eta[2] = phit * ku;
@@ -566,25 +574,25 @@ void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *s
     rho[2] = psit * ku;
     rho[3] = (psi[0] - psi[2]) * kv;
 
-    double a1 = 1 + eta[0];
-    double a1s = a1 * a1;
-    double e2 = eta[1] * eta[1] + eta[2] * eta[2] + eta[3] * eta[3];
-    double r2 = rho[1] * rho[1] + rho[2] * rho[2] + rho[3] * rho[3];
-    double er = eta[1] * rho[1] + eta[2] * rho[2] + eta[3] * rho[3];
-    double del = (a1s * (a1s - e2 + r2) - er * er);
-    double b1d = b1 / del;
-    double c1 = (eta[3] * rho[2] - eta[2] * rho[3]);
-    double c2 = (eta[1] * rho[3] - eta[3] * rho[1]);
-    double c3 = (eta[2] * rho[1] - eta[1] * rho[2]);
+    R a1 = 1 + eta[0];
+    R a1s = a1 * a1;
+    R e2 = eta[1] * eta[1] + eta[2] * eta[2] + eta[3] * eta[3];
+    R r2 = rho[1] * rho[1] + rho[2] * rho[2] + rho[3] * rho[3];
+    R er = eta[1] * rho[1] + eta[2] * rho[2] + eta[3] * rho[3];
+    R del = (a1s * (a1s - e2 + r2) - er * er);
+    R b1d = b1 / del;
+    R c1 = (eta[3] * rho[2] - eta[2] * rho[3]);
+    R c2 = (eta[1] * rho[3] - eta[3] * rho[1]);
+    R c3 = (eta[2] * rho[1] - eta[1] * rho[2]);
     sI[iw] = b0 + b1d * (a1 * (a1s + r2));
     sQ[iw] = -b1d * (a1s * eta[1] + a1 * c1 + rho[1] * er);
     sU[iw] = -b1d * (a1s * eta[2] + a1 * c2 + rho[2] * er);
     sV[iw] = -b1d * (a1s * eta[3] + a1 * c3 + rho[3] * er);
     if (!deriv) continue;
 
-    double de[4][7], dr[4][7];
+    R de[4][7], dr[4][7];
     // d/dB
-    double ps = 0.5 * (dphi[0][0] + dphi[2][0]);
+    R ps = 0.5 * (dphi[0][0] + dphi[2][0]);
     de[0][0] = eta_half * (dphi[1][0] * sth2 + ps * cth2p1);
     de[1][0] = (dphi[1][0] - ps);
     de[2][0] = de[1][0] * ku;
@@ -630,14 +638,14 @@ void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *s
       dr[s][6] = rho[s] / p6;
     }
     for (int k = 0; k < 7; k++) {
-      double da1 = de[0][k];
-      double de2 = 2.0 * eta[1] * de[1][k] + 2.0 * eta[2] * de[2][k] + 2.0 * eta[3] * de[3][k];
-      double dr2 = 2.0 * rho[1] * dr[1][k] + 2.0 * rho[2] * dr[2][k] + 2.0 * rho[3] * dr[3][k];
-      double der = de[1][k] * rho[1] + eta[1] * dr[1][k] + de[2][k] * rho[2] + eta[2] * dr[2][k] +
+      R da1 = de[0][k];
+      R de2 = 2.0 * eta[1] * de[1][k] + 2.0 * eta[2] * de[2][k] + 2.0 * eta[3] * de[3][k];
+      R dr2 = 2.0 * rho[1] * dr[1][k] + 2.0 * rho[2] * dr[2][k] + 2.0 * rho[3] * dr[3][k];
+      R der = de[1][k] * rho[1] + eta[1] * dr[1][k] + de[2][k] * rho[2] + eta[2] * dr[2][k] +
                    de[3][k] * rho[3] + eta[3] * dr[3][k];
-      double ddel = 2 * a1 * da1 * (a1s - e2 + r2) + a1s * (2 * a1 * da1 - de2 + dr2) -
+      R ddel = 2 * a1 * da1 * (a1s - e2 + r2) + a1s * (2 * a1 * da1 - de2 + dr2) -
                     2.0 * er * der;
-      double b1dd = b1d / del;
+      R b1dd = b1d / del;
       jI[k * nw + iw] =
           (b1dd * (del * (da1 * (a1s + r2) + a1 * (2 * a1 * da1 + dr2)) - ddel * (a1 * (a1s + r2)))) *
           step[k];
@@ -663,7 +671,7 @@ void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *s
                     ddel * (a1s * eta[3] + a1 * (eta[2] * rho[1] - eta[1] * rho[2]) + rho[3] * er))) *
           step[k];
     }
-    double T = (1 - p8) / del;
+    R T = (1 - p8) / del;
     jI[7 * nw + iw] = (p8 + T * (a1 * (a1s + r2))) * s7;
     jQ[7 * nw + iw] = (-T * (a1s * eta[1] + a1 * c1 + rho[1] * er)) * s7;
     jU[7 * nw + iw] = (-T * (a1s * eta[2] + a1 * c2 + rho[2] * er)) * s7;
@@ -822,23 +830,25 @@ int init_guess(const meo_plan &P, const double *prof, PixelState &st) {
 // implicit-shift QR on the bidiagonal), the Numerical Recipes svdcmp form the
 // reference uses: Src/SVD_TEMPLATE.h:49-344.  a[m*n] row-major is replaced by
 // U; w[n]; v[n*n].  Returns 1 if the QR sweep limit (50) was hit.
-double pythag(double a, double b) {  // Src/SVD_TEMPLATE.h:49-80
-  double aa = a > 0 ? a : -a;
-  double ab = b > 0 ? b : -b;
-  double mx = aa > ab ? aa : ab;
+template <class R>
+R pythag(R a, R b) {  // Src/SVD_TEMPLATE.h:49-80
+  R aa = a > 0 ? a : -a;
+  R ab = b > 0 ? b : -b;
+  R mx = aa > ab ? aa : ab;
   if (mx == 0) return 0;
   if (mx < 1e150) return sqrt(a * a + b * b);
-  double mn = aa > ab ? ab : aa;
-  double r = mn / mx;
+  R mn = aa > ab ? ab : aa;
+  R r = mn / mx;
   return mx * sqrt(1.0 + r * r);
 }
 
-int gr_svd(double *a, int m, int n, double *w, double *v) {
+template <class R>
+int gr_svd(R *a, int m, int n, R *w, R *v) {
 #define A(i, j) a[(i) * n + (j)]
 #define V(i, j) v[(i) * n + (j)]
   int l = 0, nm = 0;
-  double anorm = 0., c, f, g = 0., h, s, scale = 0., x, y, z;
-  double rv1[16];
+  R anorm = 0., c, f, g = 0., h, s, scale = 0., x, y, z;
+  R rv1[16];
   int hit_limit = 0;
   // Householder reduction to bidiagonal form
   for (int i = 0; i < n; i++) {
@@ -847,7 +857,7 @@ int gr_svd(double *a, int m, int n, double *w, double *v) {
     g = s = scale = 0.0;
     if (i < m) {
       for (int k = i; k < m; k++) scale += fabs(A(k, i));
-      if (scale) {
+      if (scale != 0.0) {
         for (int k = i; k < m; k++) {
           A(k, i) /= scale;
           s += A(k, i) * A(k, i);
@@ -869,7 +879,7 @@ int gr_svd(double *a, int m, int n, double *w, double *v) {
     g = s = scale = 0.0;
     if (i < m && i != n - 1) {
       for (int k = l; k < n; k++) scale += fabs(A(i, k));
-      if (scale) {
+      if (scale != 0.0) {
         for (int k = l; k < n; k++) {
           A(i, k) /= scale;
           s += A(i, k) * A(i, k);
@@ -887,7 +897,7 @@ int gr_svd(double *a, int m, int n, double *w, double *v) {
         for (int k = l; k < n; k++) A(i, k) *= scale;
       }
     }
-    double t = fabs(w[i]) + fabs(rv1[i]);
+    R t = fabs(w[i]) + fabs(rv1[i]);
     if (anorm < t) anorm = t;
   }
   // accumulate right-hand transformations
@@ -974,8 +984,8 @@ int gr_svd(double *a, int m, int n, double *w, double *v) {
       g = rv1[nm];
       h = rv1[k];
       f = ((y - z) * (y + z) + (g - h) * (g + h)) / (2.0 * h * y);
-      g = pythag(f, 1.0);
-      double sg = f >= 0.0 ? g : -g;
+      g = pythag(f, R(1.0));
+      R sg = f >= 0.0 ? g : -g;
       f = ((x - z) * (x + z) + h * (y / (f + sg) - h)) / x;
       c = s = 1.0;
       for (int j = l; j <= nm; j++) {
@@ -1000,7 +1010,7 @@ int gr_svd(double *a, int m, int n, double *w, double *v) {
         }
         z = pythag(f, h);
         w[j] = z;
-        if (z) {
+        if (z != 0.0) {
           z = 1.0 / z;
           c = f * z;
           s = h * z;
@@ -1025,11 +1035,11 @@ int gr_svd(double *a, int m, int n, double *w, double *v) {
 }
 
 // svbksb (Src/SVD_TEMPLATE.h:348-406): x = V diag(1/w) U^T b, w <= 1e-50 skipped.
-void gr_backsub(const double *u, const double *v, const double *w, const double *b, int n,
-                double *x) {
-  double t[16];
+template <class R>
+void gr_backsub(const R *u, const R *v, const R *w, const R *b, int n, R *x) {
+  R t[16];
   for (int j = 0; j < n; j++) {
-    double s = 0.0;
+    R s = 0.0;
     if (w[j] > 1e-50) {
       for (int i = 0; i < n; i++) s += u[i * n + j] * b[i];
       s /= w[j];
@@ -1037,7 +1047,7 @@ void gr_backsub(const double *u, const double *v, const double *w, const double 
     t[j] = s;
   }
   for (int i = 0; i < n; i++) {
-    double s = 0.0;
+    R s = 0.0;
     for (int j = 0; j < n; j++) s += v[i * n + j] * t[j];
     x[i] = s;
   }
@@ -1274,7 +1284,7 @@ double trial(PixelCtx &C) {
   for (int i = 0; i < 9; i++) L.par_tmp[i] = L.par[i];
   apply_step(C, L.par_tmp);
   bounds(L.par_tmp, C.lim);
-  synthesize(*C.P, L.par_tmp, false, C.st.step, L.syn, nullptr);
+  synthesize<double>(*C.P, L.par_tmp, false, C.st.step, L.syn, nullptr);
   L.c_syn++;
   L.chisq = loss(C, L.syn);
   if (C.P->cfg.regul_any) regularise(C, L.par_tmp, false);
@@ -1497,7 +1507,7 @@ extern "C" int meo_synth(meo_plan *P, const double *par, int deriv, double step7
   memcpy(step, P->step, sizeof(step));
   step[7] = step7;
   std::vector<double> J(deriv ? 36 * P->nw : 0);
-  synthesize(*P, par, deriv != 0, step, syn, deriv ? J.data() : nullptr);
+  synthesize<double>(*P, par, deriv != 0, step, syn, deriv ? J.data() : nullptr);
   if (deriv && jac) memcpy(jac, J.data(), sizeof(double) * J.size());
   return ME_OK;
 }
@@ -1558,5 +1568,60 @@ extern "C" int meo_normal_equations(meo_plan *P, const double *prof, const doubl
   synthesize(*P, par, true, C.st.step, syn.data(), P->jac.data());
   normal_equations(C, syn.data(), H, g);
   *chisq = loss(C, syn.data());
+  return ME_OK;
+}
+
+thread_local FlopTally g_tally;
+
+namespace {
+void tally_out(double *c) {
+  c[0] = (double)g_tally.add;
+  c[1] = (double)g_tally.mul;
+  c[2] = (double)g_tally.div;
+  c[3] = (double)g_tally.sqrt_;
+  c[4] = (double)g_tally.exp_;
+  c[5] = (double)g_tally.trig;
+  c[6] = (double)g_tally.special;
+  c[7] = (double)g_tally.cmp;
+}
+}  // namespace
+
+// Operation counts of one synthesis (all nl wavelengths) of the reference's
+// algorithm at `par`: counts[8] = add/sub, mul, div, sqrt, exp/log,
+// sin/cos, erfc, compares.
+extern "C" int meo_count_synth(meo_plan *P, const double *par, int deriv, double *counts) {
+  if (!P || !par || !counts) return ME_ERR_ARG;
+  std::vector<Cnt> syn(4 * P->nw), jac(deriv ? 36 * P->nw : 0);
+  double step[9];
+  memcpy(step, P->step, sizeof(step));
+  g_tally = FlopTally();
+  synthesize<Cnt>(*P, par, deriv != 0, step, syn.data(), deriv ? jac.data() : nullptr);
+  tally_out(counts);
+  return ME_OK;
+}
+
+// Operation counts of one SVD_solve_mem (Golub-Reinsch SVD + truncation
+// ladder + back-substitutions) on the n x n matrix a with right-hand side g.
+extern "C" int meo_count_svd_solve(const double *a, const double *g, int n, double thr,
+                                   double *counts) {
+  if (!a || !g || !counts || n < 1 || n > 16) return ME_ERR_ARG;
+  std::vector<Cnt> A(a, a + n * n), V(n * n), W(n), G(g, g + n), X(n);
+  g_tally = FlopTally();
+  gr_svd<Cnt>(A.data(), n, n, W.data(), V.data());
+  Cnt wmax = W[0];
+  for (int i = 1; i < n; i++) wmax = wmax > W[i] ? wmax : W[i];
+  Cnt t = thr;
+  while (true) {
+    Cnt wthr = wmax * t;
+    for (int i = 0; i < n; i++)
+      if (W[i] < wthr) W[i] = 0.;
+    gr_backsub<Cnt>(A.data(), V.data(), W.data(), G.data(), n, X.data());
+    bool inside = true;
+    for (int i = 0; i < n; i++)
+      if (X[i] > 0.5 || X[i] < -0.5) inside = false;
+    if (inside || t > 2e-3) break;
+    t *= 5.;
+  }
+  tally_out(counts);
   return ME_OK;
 }

@@ -52,6 +52,12 @@ int meo_init_guess(meo_plan *p, const double *prof, double *guess, double *extra
 int meo_normal_equations(meo_plan *p, const double *prof, const double *par,
                          double step7, double norm0, double *H, double *g,
                          double *chisq);
+/* Algorithmic operation counts (a counting scalar type through the same
+ * templated code): counts[8] = add/sub, mul, div, sqrt, exp/log, sin/cos,
+ * erfc, compares for one synthesis at par (all nl wavelengths) and for one
+ * SVD solve (SVD + truncation ladder) of a with right-hand side g. */
+int meo_count_synth(meo_plan *p, const double *par, int deriv, double *counts);
+int meo_count_svd_solve(const double *a, const double *g, int n, double thr, double *counts);
 /* the project's counter-based standard normal draws: out[8] for (pixel, run) */
 void meo_restart_draws(unsigned long long seed, long long pixel, int run, double *out);
 

@@ -1,0 +1,71 @@
+"""The oracle against the reference's C core run live (oracle/_ref).
+
+Skipped where the reference core was not built.  Besides bit-for-bit parity
+on a fresh seeded map, this documents the property that decides how the CUDA
+path is judged: the reference's LM flips to another trajectory on a one-ulp
+change of its input for a large share of pixels (its trial steps after the
+first decompose the previous SVD's orthogonal factor, whose singular values
+are degenerate).
+"""
+import os
+import subprocess
+import sys
+import textwrap
+
+import numpy as np
+import pytest
+
+import oracle_bind as ob
+
+pytestmark = pytest.mark.skipif(not ob.reference_available(), reason="oracle/_ref not built")
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+SCRIPT = textwrap.dedent("""
+    import sys, json, numpy as np
+    sys.path[:0] = [{tests!r}, {pkg!r}]
+    import oracle_bind as ob, me_b200, me_maps
+    name, npix, extra, seed = {args!r}
+    lam = me_maps.wavelengths(name)
+    ref = ob.Reference(me_maps.reference_control_text(name, extra=extra), lam, npix, seed=seed)
+    cfg = me_b200.parse_config_text(me_maps.control_text(name, extra=extra))
+    orc = ob.Oracle(cfg, lam)
+    par = me_maps.draw_parameters(name, npix, 99)
+    prof = me_maps.add_noise(np.stack([ref.synth(p) for p in par]), 1e-3, 99)
+    r_ref = ref.invert(prof)
+    r_orc = orc.invert(prof, rng_mode=ob.MEO_RNG_NR, nr_seed=seed)
+    out = dict(exact=bool(np.array_equal(r_ref, r_orc)), carry=bool(ref.lm_chisq == orc.carry[0]))
+    if {chaos!r}:
+        ref.lm_chisq = 0.0
+        rng = np.random.default_rng(5)
+        r_pert = ref.invert(prof * (1 + 2.3e-16 * rng.choice([-1, 1], prof.shape)))
+        changed = (np.abs(r_pert - r_ref) > 1e-6 * np.abs(r_ref)).any(1)
+        out["changed_fraction"] = float(changed.mean())
+    print(json.dumps(out))
+""")
+
+
+def run_case(name, npix, extra, seed, chaos=False):
+    code = SCRIPT.format(tests=os.path.join(ROOT, "tests"),
+                         pkg=os.path.join(ROOT, "milne-eddington_b200"),
+                         args=(name, npix, extra, seed), chaos=chaos)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True)
+    import json
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def test_reference_parity_run1_and_ulp_chaos():
+    out = run_case("fe15648_64x64", 192, {}, 11, chaos=True)
+    assert out["exact"] and out["carry"]
+    # a sizeable share of pixels change their result under a 1-ulp input change
+    assert out["changed_fraction"] > 0.05
+
+
+def test_reference_parity_restarts_nr_stream():
+    out = run_case("fe15648_64x64", 96, {"num_run": "2", "chisq_criteria": "0.5"}, 31337)
+    assert out["exact"] and out["carry"]
+
+
+def test_reference_parity_fe6302_weights():
+    out = run_case("fe6302_2048x1024", 96, {"num_run": "1"}, 5)
+    assert out["exact"] and out["carry"]
