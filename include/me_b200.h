@@ -112,6 +112,7 @@ typedef struct me_stats {
   long long wavelengths;   /* wavelength points synthesised (both kinds)   */
   long long redo_pixels;   /* pixels re-run to honour the carried LM chi^2 */
   long long launches;      /* inversion kernel launches made by the call     */
+  long long rounds;        /* LM rounds (one trial step per pixel in flight) */
   double kernel_ms;        /* device time of the inversion kernel(s)       */
   double h2d_ms, d2h_ms;   /* host<->device copy time (host entry point)   */
 } me_stats;
@@ -157,6 +158,11 @@ void me_plan_set_carry_chisq(me_plan *plan, double chisq);
  * occupancy-derived default (used by the autotuner and the benchmarks). */
 int me_plan_grid(const me_plan *plan);
 void me_plan_set_grid(me_plan *plan, int grid);
+
+/* Number of pixels a plan keeps in flight on the device (0 = default,
+ * 131072); each holds ~1.6 KB of LM state in HBM. */
+int me_plan_window(const me_plan *plan);
+void me_plan_set_window(me_plan *plan, int window);
 
 /* Inverts npix pixels.  prof: host [npix][4][nl]; res: host [npix][10];
  * fit: host [npix][4][nl] or NULL (best-fit profiles, zeros when skipped);

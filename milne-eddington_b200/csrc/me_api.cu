@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -98,6 +99,15 @@ struct me_plan {
   DevBuf d_lambda, d_dlambda;
   DevBuf d_prof, d_res, d_fit;  // staging of the host entry point
   DevBuf d_flags, d_pen0, d_lastchi, d_counters, d_totals, d_next, d_stale, d_list;
+  // slots of the pixels in flight (struct me::Slots), sized for `window`
+  int window = 0;          // requested slot count (0 = default)
+  int slots_w = 0;         // allocated slot count
+  DevBuf d_slot_pix, d_slot_i32, d_slot_cnt, d_slot_u8, d_slot_sc, d_slot_vec, d_slot_hess,
+      d_slot_list, d_slot_small;
+  int grid_jac = 0, grid_trial = 0, grid_svd = 0;
+  int poll_rounds = 8;     // rounds launched between checks of the queue
+  unsigned long long *h_poll = nullptr;  // pinned: next, busy
+  long long rounds_last = 0;
   std::vector<unsigned char> h_flags;
   std::vector<double> h_pen0, h_lastchi, h_stale, h_used;
   std::vector<long long> h_list;
@@ -227,7 +237,14 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
   }
   P.lambda = p->d_lambda.as<double>();
   P.dlambda = p->d_dlambda.as<double>();
-  p->grid = me::invert_grid(p->precision, device);
+  p->grid_jac = me::round_grid(p->precision, 0, device);
+  p->grid_trial = me::round_grid(p->precision, 1, device);
+  p->grid_svd = me::round_grid(p->precision, 2, device);
+  p->grid = p->grid_trial;
+  if (cudaMallocHost((void **)&p->h_poll, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    me_plan_destroy(p);
+    return fail(ME_ERR_CUDA, "pinned allocation failed");
+  }
 
   me_plan_facts &f = p->facts;
   f.nl = nl;
@@ -249,8 +266,11 @@ extern "C" void me_plan_destroy(me_plan *p) {
   DevBuf *bufs[] = {&p->d_lambda, &p->d_dlambda, &p->d_prof,     &p->d_res,
                     &p->d_fit,    &p->d_flags,   &p->d_pen0,     &p->d_lastchi,
                     &p->d_counters, &p->d_totals, &p->d_next,    &p->d_stale,
-                    &p->d_list};
+                    &p->d_list,   &p->d_slot_pix, &p->d_slot_i32, &p->d_slot_cnt,
+                    &p->d_slot_u8, &p->d_slot_sc, &p->d_slot_vec, &p->d_slot_hess,
+                    &p->d_slot_list, &p->d_slot_small};
   for (DevBuf *b : bufs) b->release();
+  if (p->h_poll) cudaFreeHost(p->h_poll);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -272,6 +292,88 @@ extern "C" int me_plan_grid(const me_plan *p) { return p ? p->grid : 0; }
 extern "C" void me_plan_set_grid(me_plan *p, int grid) {
   if (p && grid > 0) p->grid = grid;
 }
+
+extern "C" int me_plan_window(const me_plan *p) { return p ? p->window : 0; }
+extern "C" void me_plan_set_window(me_plan *p, int window) {
+  if (p && window >= 0) p->window = window;
+}
+
+namespace {
+
+// Grows the slot buffers to W slots and returns the device view.
+int ensure_slots(me_plan *p, int W, me::Slots &S) {
+  if (W > p->slots_w) {
+    const size_t w = (size_t)W;
+    CK(p->d_slot_pix.ensure(w * sizeof(long long)));
+    CK(p->d_slot_i32.ensure(4 * w * sizeof(int)));
+    CK(p->d_slot_cnt.ensure(4 * w * sizeof(unsigned int)));
+    CK(p->d_slot_u8.ensure(w));
+    CK(p->d_slot_sc.ensure((size_t)me::SC_COUNT * w * sizeof(double)));
+    CK(p->d_slot_vec.ensure(5 * 9 * w * sizeof(double)));
+    CK(p->d_slot_hess.ensure(81 * w * sizeof(double)));
+    CK(p->d_slot_list.ensure(2 * w * sizeof(int)));
+    CK(p->d_slot_small.ensure(4 * sizeof(int)));
+    p->slots_w = W;
+  }
+  const size_t w = (size_t)W;
+  S.W = W;
+  S.pix = p->d_slot_pix.as<long long>();
+  int *i32 = p->d_slot_i32.as<int>();
+  S.state = i32;
+  S.run = i32 + w;
+  S.it = i32 + 2 * w;
+  S.tk = i32 + 3 * w;
+  S.cnt = p->d_slot_cnt.as<unsigned int>();
+  S.had_trial = p->d_slot_u8.as<unsigned char>();
+  S.sc = p->d_slot_sc.as<double>();
+  double *v = p->d_slot_vec.as<double>();
+  S.guess = v;
+  S.par = v + 9 * w;
+  S.pbest = v + 18 * w;
+  S.jvec = v + 27 * w;
+  S.ptmp = v + 36 * w;
+  S.hess = p->d_slot_hess.as<double>();
+  S.jlist = p->d_slot_list.as<int>();
+  int *small = p->d_slot_small.as<int>();
+  S.jcount = small;
+  S.busy = small + 2;
+  return ME_OK;
+}
+
+// Runs one queue (A.count items) to completion: rounds of jac_kernel +
+// trial_kernel on the plan's slots until every pixel is done.
+int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &rounds) {
+  const long long cap = p->window > 0 ? p->window : 131072;
+  const int W = (int)(A.count < cap ? A.count : cap);
+  if (W <= 0) return ME_OK;
+  me::Slots S;
+  int rc = ensure_slots(p, W, S);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(S.state, 0, (size_t)W * sizeof(int), st));  // SL_EMPTY
+  CK(cudaMemsetAsync(S.jcount, 0, 4 * sizeof(int), st));           // jcount[2], busy
+  CK(cudaMemsetAsync(A.next, 0, sizeof(unsigned long long), st));
+  int grids[3];
+  grids[0] = std::min(p->grid_jac, (W + me::kBlock - 1) / me::kBlock);
+  grids[1] = std::min(p->grid_trial, (W + me::kBlock - 1) / me::kBlock);
+  grids[2] = std::min(p->grid_svd, (W + me::kSvdBlock - 1) / me::kSvdBlock);
+  int parity = 0;
+  rounds = 0;
+  while (true) {
+    for (int r = 0; r < p->poll_rounds; r++) {
+      CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st));
+      parity ^= 1;
+      rounds++;
+    }
+    CK(cudaMemcpyAsync(p->h_poll, A.next, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(p->h_poll + 1, S.busy, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int busy = *reinterpret_cast<int *>(p->h_poll + 1);
+    if (p->h_poll[0] >= (unsigned long long)A.count && busy == 0) break;
+  }
+  return ME_OK;
+}
+
+}  // namespace
 
 extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npix, double *d_res,
                                       double *d_fit, void *stream, me_stats *stats) {
@@ -304,14 +406,16 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   A.carry = p->carry;
   A.first_pixel = 0;
 
-  CK(cudaMemsetAsync(A.next, 0, sizeof(unsigned long long), st));
+  long long rounds = 0, rounds_total = 0;
   CK(cudaEventRecord(p->ev0, st));
-  CK(me::launch_invert(p->precision, p->P, A, p->grid, st));
+  int rc = run_queue(p, A, st, rounds);
+  if (rc) return rc;
   CK(cudaEventRecord(p->ev1, st));
+  rounds_total += rounds;
 
   // The reference carries LM->chisq from pixel to pixel; it enters only the
   // first regularisation ratio test of each pixel (Src/LM_FIT.c:555-559).  The
-  // launch above assumed the carried value for pixel 0 and "no ratio change"
+  // batch above assumed the carried value for pixel 0 and "no ratio change"
   // for every later pixel; pixels for which the true carried value (the last
   // trial chi^2 of the previous inverted pixel) flips that test are re-run,
   // until no flip remains.
@@ -328,10 +432,10 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   float ms = 0.f;
   cudaEventElapsedTime(&ms, p->ev0, p->ev1);
   double kernel_ms = ms;
-  long long redo_total = 0, launches = 1;
+  long long redo_total = 0, passes = 1;
   p->h_used.assign(n, INFINITY);
-  if (n) p->h_used[0] = p->carry;
-  for (int pass = 0; pass < 1 << 20; pass++) {
+  p->h_used[0] = p->carry;
+  while (true) {
     double prev = p->carry;
     p->h_list.clear();
     for (size_t i = 0; i < n; i++) {
@@ -351,7 +455,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
       break;
     }
     redo_total += (long long)p->h_list.size();
-    launches++;
+    passes++;
     const size_t m = p->h_list.size();
     CK(p->d_list.ensure(m * sizeof(long long)));
     CK(p->d_stale.ensure(n * sizeof(double)));
@@ -363,11 +467,11 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     B.list = p->d_list.as<long long>();
     B.count = (long long)m;
     B.stale = p->d_stale.as<double>();
-    CK(cudaMemsetAsync(B.next, 0, sizeof(unsigned long long), st));
     CK(cudaEventRecord(p->ev0, st));
-    const int g = (int)((m + me::kInvertBlock - 1) / me::kInvertBlock);
-    CK(me::launch_invert(p->precision, p->P, B, g < p->grid ? g : p->grid, st));
+    rc = run_queue(p, B, st, rounds);
+    if (rc) return rc;
     CK(cudaEventRecord(p->ev1, st));
+    rounds_total += rounds;
     CK(cudaMemcpyAsync(p->h_flags.data(), A.flags, n, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(p->h_lastchi.data(), A.lastchi, n * sizeof(double),
                        cudaMemcpyDeviceToHost, st));
@@ -375,6 +479,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     cudaEventElapsedTime(&ms, p->ev0, p->ev1);
     kernel_ms += ms;
   }
+  p->rounds_last = rounds_total;
   if (stats) {
     unsigned long long tot[8];
     CK(cudaMemcpy(tot, A.totals, sizeof(tot), cudaMemcpyDeviceToHost));
@@ -388,7 +493,8 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     stats->jacobians = (long long)tot[5];
     stats->wavelengths = (long long)(tot[3] + tot[5]) * p->P.nl;
     stats->redo_pixels = redo_total;
-    stats->launches = launches;
+    stats->launches = 3 * rounds_total;
+    stats->rounds = rounds_total;
     stats->kernel_ms = kernel_ms;
   }
   return ME_OK;

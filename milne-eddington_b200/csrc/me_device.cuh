@@ -945,6 +945,183 @@ static __device__ __noinline__ int gr_svd(double *a, int n, double *w, double *v
 #undef V_
 }
 
+// The same Golub-Reinsch decomposition producing U and w only (no V): the
+// Householder reduction, the accumulation of the left transformations and the
+// implicit-shift QR sweeps of gr_svd with every operation on V left out.  The
+// operations on U and w are gr_svd's own (V's loops only overwrite scratch
+// scalars that are reassigned before their next use), so U and w come out
+// identical.  Matrix element (i, j) lives at a[(i * n + j) * STR], w[i] at
+// w[i * STR], so one thread's matrix can sit in a column of shared memory.
+template <int STR>
+__device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
+#define A_(i, j) a[((i) * n + (j)) * STR]
+#define W_(i) w[(i) * STR]
+#define R_(i) rv1[(i) * STR]
+  const int m = n;
+  int l = 0, nm = 0;
+  double anorm = 0., c, f, g = 0., h, s, scale = 0., x, y, z;
+  int hit = 0;
+  for (int i = 0; i < n; i++) {
+    l = i + 1;
+    R_(i) = scale * g;
+    g = s = scale = 0.0;
+    for (int k = i; k < m; k++) scale += fabs(A_(k, i));
+    if (scale) {
+      const double is = 1.0 / scale;
+      for (int k = i; k < m; k++) {
+        const double t = A_(k, i) * is;
+        A_(k, i) = t;
+        s += t * t;
+      }
+      f = A_(i, i);
+      g = f >= 0 ? -sqrt(s) : sqrt(s);
+      h = f * g - s;
+      A_(i, i) = f - g;
+      const double ih = 1.0 / h;
+      for (int j = l; j < n; j++) {
+        s = 0.0;
+        for (int k = i; k < m; k++) s += A_(k, i) * A_(k, j);
+        f = s * ih;
+        for (int k = i; k < m; k++) A_(k, j) += f * A_(k, i);
+      }
+      for (int k = i; k < m; k++) A_(k, i) *= scale;
+    }
+    W_(i) = scale * g;
+    g = s = scale = 0.0;
+    if (i != n - 1) {
+      for (int k = l; k < n; k++) scale += fabs(A_(i, k));
+      if (scale) {
+        const double is = 1.0 / scale;
+        for (int k = l; k < n; k++) {
+          const double t = A_(i, k) * is;
+          A_(i, k) = t;
+          s += t * t;
+        }
+        f = A_(i, l);
+        g = f >= 0 ? -sqrt(s) : sqrt(s);
+        h = f * g - s;
+        A_(i, l) = f - g;
+        const double ih = 1.0 / h;
+        for (int k = l; k < n; k++) R_(k) = A_(i, k) * ih;
+        for (int j = l; j < m; j++) {
+          s = 0.0;
+          for (int k = l; k < n; k++) s += A_(j, k) * A_(i, k);
+          for (int k = l; k < n; k++) A_(j, k) += s * R_(k);
+        }
+        for (int k = l; k < n; k++) A_(i, k) *= scale;
+      }
+    }
+    const double t = fabs(W_(i)) + fabs(R_(i));
+    if (anorm < t) anorm = t;
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    l = i + 1;
+    g = W_(i);
+    for (int j = l; j < n; j++) A_(i, j) = 0.0;
+    if (g != 0.0) {
+      g = 1.0 / g;
+      const double iaii = 1.0 / A_(i, i);
+      for (int j = l; j < n; j++) {
+        s = 0.0;
+        for (int k = l; k < m; k++) s += A_(k, i) * A_(k, j);
+        f = (s * iaii) * g;
+        for (int k = i; k < m; k++) A_(k, j) += f * A_(k, i);
+      }
+      for (int j = i; j < m; j++) A_(j, i) *= g;
+    } else {
+      for (int j = i; j < m; j++) A_(j, i) = 0.0;
+    }
+    A_(i, i) += 1.0;
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    for (int its = 0; its < 50; its++) {
+      int flag = 1;
+      for (l = k; l >= 0; l--) {
+        nm = l - 1;
+        if ((fabs(R_(l)) + anorm) == anorm) {
+          flag = 0;
+          break;
+        }
+        if (nm >= 0 && (fabs(W_(nm)) + anorm) == anorm) break;
+      }
+      if (flag) {
+        c = 0.0;
+        s = 1.0;
+        for (int i = l; i <= k; i++) {
+          f = s * R_(i);
+          R_(i) = c * R_(i);
+          if ((fabs(f) + anorm) == anorm) break;
+          g = W_(i);
+          h = pythag_d(f, g);
+          W_(i) = h;
+          h = 1.0 / h;
+          c = g * h;
+          s = -f * h;
+          for (int j = 0; j < m; j++) {
+            y = A_(j, nm);
+            z = A_(j, i);
+            A_(j, nm) = y * c + z * s;
+            A_(j, i) = z * c - y * s;
+          }
+        }
+      }
+      z = W_(k);
+      if (l == k) {
+        if (z < 0.0) W_(k) = -z;  // (V's column k would change sign here)
+        break;
+      }
+      if (its == 49) hit = 1;
+      x = W_(l);
+      nm = k - 1;
+      y = W_(nm);
+      g = R_(nm);
+      h = R_(k);
+      f = ((y - z) * (y + z) + (g - h) * (g + h)) / (2.0 * h * y);
+      g = pythag_d(f, 1.0);
+      f = ((x - z) * (x + z) + h * (y / (f + (f >= 0.0 ? g : -g)) - h)) / x;
+      c = s = 1.0;
+      for (int j = l; j <= nm; j++) {
+        const int i = j + 1;
+        g = R_(i);
+        y = W_(i);
+        h = s * g;
+        g *= c;
+        z = pythag_d(f, h);
+        R_(j) = z;
+        const double iz = 1.0 / z;
+        c = f * iz;
+        s = h * iz;
+        f = x * c + g * s;
+        g = g * c - x * s;
+        h = y * s;
+        y *= c;
+        z = pythag_d(f, h);
+        W_(j) = z;
+        if (z) {
+          z = 1.0 / z;
+          c = f * z;
+          s = h * z;
+        }
+        f = c * g + s * y;
+        x = c * y - s * g;
+        for (int jj = 0; jj < m; jj++) {
+          y = A_(jj, j);
+          z = A_(jj, i);
+          A_(jj, j) = y * c + z * s;
+          A_(jj, i) = z * c - y * s;
+        }
+      }
+      R_(l) = 0.0;
+      R_(k) = f;
+      W_(k) = x;
+    }
+  }
+  return hit;
+#undef A_
+#undef W_
+#undef R_
+}
+
 // x = V diag(1/w) U^T b, skipping w <= 1e-50 (svbksb, SVD_TEMPLATE.h:348-406).
 __device__ __forceinline__ void gr_backsub(const double *u, const double *v, const double *w,
                                            const double *b, int n, double *x) {

@@ -1,17 +1,25 @@
-// me_invert.cuh -- the inversion kernel (hot path), instantiated per precision
-// by me_invert_f32.cu / me_invert_f64.cu.
+// me_invert.cuh -- the inversion hot path: one LM "round" is two kernels.
 //
-// invert_kernel<T> is the hot path: a persistent kernel, one pixel per thread,
-// each thread running the reference's INVERSION (Src/LM_FIT.c:665-742) as a
-// flat state machine.  Every trip round the thread's loop performs exactly one
-// LM trial step (SVD solve + forward synthesis + chi^2, Src/LM_FIT.c:473-527),
-// preceded, only in lanes that need it, by a synthesis with the analytic
-// Jacobian fused with the normal equations (Milne_Eddington_Single(Deriv) +
-// Hessian_Compute, Src/ME_SOLVER.c:101-366 and Src/LM_FIT.c:240-350).  So the
-// lanes of a warp stay in step on the dominant trial work whatever iteration,
-// trial or restart each pixel is at.  A lane that finishes its pixel takes the
-// next one from a global atomic counter: finished pixels leave the warp and
-// restarts are queued in place, with no host round trip.
+// Every pixel in flight owns a slot whose state lives in HBM (struct Slots).
+// A round advances every slot by exactly one LM trial step:
+//
+//   jac_kernel    over the compacted list of slots that need the synthesis
+//                 with Jacobian (a run start or an accepted step): the
+//                 Milne-Eddington synthesis + analytic Jacobian fused with the
+//                 weighted normal equations (Milne_Eddington_Single(Deriv) +
+//                 Hessian_Compute + Get_Regul, Src/ME_SOLVER.c:101-366,
+//                 Src/LM_FIT.c:240-396, 549-586);
+//   trial_kernel  over all slots: one trial step (Trial_Synthesis,
+//                 Src/LM_FIT.c:473-527: SVD solve, parameter update, forward
+//                 synthesis, chi^2), the accept / reject / convergence logic
+//                 (Src/LM_FIT.c:588-646), the end-of-run restart policy
+//                 (INVERSION, Src/LM_FIT.c:701-733) and, when a pixel is done,
+//                 its result and the refill of the slot from the queue.
+//
+// Slots that accept a step append themselves to the next round's Jacobian
+// list, so that work runs at full SIMD width instead of in a divergent subset
+// of a warp; finished pixels leave and new ones enter without a host round
+// trip.  Instantiated per synthesis precision by me_invert_f32.cu / _f64.cu.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -20,7 +28,6 @@
 #include "me_kernels.h"
 
 namespace me {
-
 namespace detail {
 
 template <class T>
@@ -42,16 +49,16 @@ __device__ __forceinline__ void fill_table(const DevPlan &P, T *s_tab) {
   __syncthreads();
 }
 
-// Synthesis with Jacobian fused with the weighted normal equations
-// (Milne_Eddington_Single(Deriv=1) + Hessian_Compute + Loss_Function).
-// sw[s] = weight_s / sqrt(norm0), so sum (J sw)(J sw) = J^T W J with
-// W = weight^2 / norm0 (Noise_Init, Src/ME_SOLVER.c:410-441).
-// H45 = upper triangle of the full 9x9 (row-major i <= j), g9 = -J^T W r,
-// returns sum (r sw)^2 / (4 nl) accumulated in FP64.
+// Synthesis with Jacobian fused with the weighted normal equations.
+// sw[s] = weight_s / sqrt(norm0): sum (J sw)(J sw) = J^T W J with
+// W = weight^2 / norm0 (Noise_Init, Src/ME_SOLVER.c:410-441).  H45 = upper
+// triangle of the full 9x9 (row-major, i <= j), g9 = -J^T W r; returns
+// sum (r sw)^2 / (4 nl) accumulated in FP64.
 template <class T>
-__device__ __forceinline__ double deriv_pass(const DevPlan &P, const VoigtK<T> &K, const double *par,
-                                             const double *step, const double *prof,
-                                             const double sw[4], double *H45, double *g9) {
+__device__ __forceinline__ double deriv_pass(const DevPlan &P, const VoigtK<T> &K,
+                                             const double *par, const double *step,
+                                             const double *prof, const double sw[4], double *H45,
+                                             double *g9) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
   T h[45], g[9];
@@ -94,13 +101,12 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, const VoigtK<T> &
 }
 
 // Forward synthesis + chi^2 (Trial_Synthesis's synthesis and Loss_Function);
-// residuals and their squares accumulate in FP64.  fit (nullable) receives
-// the synthetic profile.
+// residuals and their squares in FP64.  fit (nullable) receives the profile.
 template <class T>
 __device__ __noinline__ double forward_pass(const DevPlan &P, const VoigtK<T> &K,
-                                               const double *par, const double *step,
-                                               const double *prof, const double sw[4],
-                                               double *fit) {
+                                            const double *par, const double *step,
+                                            const double *prof, const double sw[4],
+                                            double *fit) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
   double chi = 0.0;
@@ -121,7 +127,7 @@ __device__ __noinline__ double forward_pass(const DevPlan &P, const VoigtK<T> &K
   return chi / (4.0 * nl);
 }
 
-// Get_Regul (Src/LM_FIT.c:354-396) penalty part.
+// Get_Regul's penalty (Src/LM_FIT.c:354-396).
 __device__ __forceinline__ double penalty_of(const DevPlan &P, const double *par) {
   double pen = 0.0;
   for (int i = 0; i < 9; i++) {
@@ -132,171 +138,353 @@ __device__ __forceinline__ double penalty_of(const DevPlan &P, const double *par
   return pen;
 }
 
-enum : int { S_FETCH = 0, S_START = 1, S_NEXT = 2, S_TRIAL = 3, S_DONE = 4 };
+__device__ __forceinline__ void append_jac(const Slots &S, int parity_next, int s) {
+  const int k = atomicAdd(S.jcount + parity_next, 1);
+  S.jlist[parity_next * S.W + k] = s;
+}
+
+__device__ __forceinline__ void load9(const double *a, int W, int s, double *v) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) v[i] = a[(size_t)i * W + s];
+}
+__device__ __forceinline__ void store9(double *a, int W, int s, const double *v) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) a[(size_t)i * W + s] = v[i];
+}
+
+// Takes pixels from the queue until one is valid (INVERSION_MULTI's gate and
+// Init_Guess, Src/LM_FIT.c:776-789) and sets the slot up for its first run.
+// Skipped pixels get zeros.  Returns false when the queue is exhausted.
+static __device__ bool refill(const DevPlan &P, const InvertArgs &A, const Slots &S, int s,
+                       unsigned long long &t_valid) {
+  const int nl = P.nl;
+  const int W = S.W;
+  while (true) {
+    const unsigned long long k = atomicAdd(A.next, 1ULL);
+    if (k >= (unsigned long long)A.count) return false;
+    const long long pix = A.list ? A.list[k] : (long long)k;
+    const double *pp = A.prof + (size_t)pix * 4 * nl;
+    PixelInit pin;
+    const int bad = init_guess(pp, P, pin, true);
+    if (bad || P.nruns <= 0) {
+#pragma unroll
+      for (int i = 0; i < 10; i++) A.res[(size_t)pix * 10 + i] = 0.0;
+      if (A.fit)
+        for (int i = 0; i < 4 * nl; i++) A.fit[(size_t)pix * 4 * nl + i] = 0.0;
+      if (A.flags) A.flags[pix] = 0;
+      continue;
+    }
+    t_valid++;
+    S.pix[s] = pix;
+    S.run[s] = 0;
+    S.it[s] = 0;
+    store9(S.guess, W, s, pin.guess);
+    store9(S.par, W, s, pin.guess);
+    double *sc = S.sc;
+    sc[SC_LMCHISQ * W + s] =
+        A.stale ? A.stale[pix] : (pix == A.first_pixel ? A.carry : INFINITY);
+    sc[SC_RATIO * W + s] = 1.0;
+    sc[SC_BEST * W + s] = 0.0;
+    sc[SC_NORMP * W + s] = pin.normp;
+    sc[SC_ISN * W + s] = 1.0 / sqrt(pin.norm0);
+    sc[SC_STEP7 * W + s] = pin.step7;
+    sc[SC_L70 * W + s] = pin.l70;
+    sc[SC_L71 * W + s] = pin.l71;
+#pragma unroll
+    for (int i = 0; i < 4; i++) S.cnt[i * W + s] = 0;
+    S.had_trial[s] = 0;
+    if (A.penalty0) A.penalty0[pix] = P.regul_any ? penalty_of(P, pin.guess) : 0.0;
+    S.state[s] = SL_JAC_START;
+    return true;
+  }
+}
 
 }  // namespace detail
 
 using namespace detail;
 
+// ---------------------------------------------------------------------------
+// Synthesis with Jacobian + normal equations for the slots of jlist[parity].
+// ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(kInvertBlock, ME_INV_MINB) invert_kernel(const DevPlan P, InvertArgs A) {
+__global__ void __launch_bounds__(kBlock) jac_kernel(const DevPlan P, InvertArgs A, Slots S,
+                                                     int parity) {
   __shared__ T s_tab[50];
   fill_table<T>(P, s_tab);
   VoigtK<T> K;
   load_voigt<T>(K, P, s_tab);
-
-  const int nl = P.nl;
+  if (blockIdx.x == 0 && threadIdx.x == 0) S.jcount[parity ^ 1] = 0;
+  const int count = S.jcount[parity];
+  const int W = S.W;
   const int n = P.npar;
-  double hess[81], vm[81];
-  double jvec[9], sol[9];
-  double par[9], ptmp[9], pbest[9], step[9];
-  double sw[4];
-  PixelInit pin;
-  double chisq = 0, lmchisq = 0, ratio = 1, penalty = 0, damp = 0, chisq_best = 0;
-  int run = 0, it = 0, state = S_FETCH;
-  long long pix = -1;
-  const double *pp = nullptr;
-  unsigned int pc_runs = 0, pc_iter = 0, pc_trials = 0, pc_acc = 0;
-  unsigned long long t_runs = 0, t_iter = 0, t_trials = 0, t_acc = 0, t_jac = 0, t_valid = 0,
-                     t_svdlim = 0;
-  bool had_trial = false;
-
-  while (true) {
-    // ---------------- take pixels until one needs inverting ----------------
-    while (state == S_FETCH) {
-      const unsigned long long k = atomicAdd(A.next, 1ULL);
-      if (k >= (unsigned long long)A.count) {
-        state = S_DONE;
-        break;
-      }
-      pix = A.list ? A.list[k] : (long long)k;
-      pp = A.prof + (size_t)pix * 4 * nl;
-      const int bad = init_guess(pp, P, pin, true);  // also the INVERSION_MULTI gate
-      if (bad || P.nruns <= 0) {
+  const int nl = P.nl;
+  unsigned long long t_jac = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const int s = S.jlist[parity * W + i];
+    const long long pix = S.pix[s];
+    const double *pp = A.prof + (size_t)pix * 4 * nl;
+    double par[9], step[9], sw[4];
+    load9(S.par, W, s, par);
 #pragma unroll
-        for (int i = 0; i < 10; i++) A.res[(size_t)pix * 10 + i] = 0.0;
-        if (A.fit)
-          for (int i = 0; i < 4 * nl; i++) A.fit[(size_t)pix * 4 * nl + i] = 0.0;
-        if (A.flags) A.flags[pix] = 0;
+    for (int k = 0; k < 9; k++) step[k] = P.step[k];
+    step[7] = S.sc[SC_STEP7 * W + s];
+    const double isn = S.sc[SC_ISN * W + s];
+#pragma unroll
+    for (int k = 0; k < 4; k++) sw[k] = P.weights[k] * isn;
+    double H45[45], g9[9];
+    const double chi0 = deriv_pass<T>(P, K, par, step, pp, sw, H45, g9);
+    t_jac++;
+    double ratio = S.sc[SC_RATIO * W + s];
+    if (S.state[s] == SL_JAC_START) {  // LM_FIT set-up (Src/LM_FIT.c:549-566)
+      S.sc[SC_CHISQ * W + s] = chi0;
+      ratio = 1.0;
+      if (P.regul_any) {
+        const double pen = penalty_of(P, par);
+        if (pen > 0.1 * S.sc[SC_LMCHISQ * W + s]) ratio = 0.1 * chi0 / pen;
+      }
+      S.sc[SC_RATIO * W + s] = ratio;
+      S.it[s] = 0;
+      if (P.niter <= 0) {
+        S.state[s] = SL_RUN_END;
         continue;
       }
-      t_valid++;
-#pragma unroll
-      for (int i = 0; i < 9; i++) step[i] = P.step[i];
-      step[7] = pin.step7;
-      const double isn = 1.0 / sqrt(pin.norm0);
-#pragma unroll
-      for (int s = 0; s < 4; s++) sw[s] = P.weights[s] * isn;
-#pragma unroll
-      for (int i = 0; i < 9; i++) par[i] = pin.guess[i];
-      run = 0;
-      lmchisq = A.stale ? A.stale[pix] : (pix == A.first_pixel ? A.carry : INFINITY);
-      if (A.penalty0) A.penalty0[pix] = P.regul_any ? penalty_of(P, par) : 0.0;
-      pc_runs = pc_iter = pc_trials = pc_acc = 0;
-      had_trial = false;
-      state = S_START;
     }
-    if (state == S_DONE) break;
-
-    // ------------- synthesis with Jacobian -> normal equations -------------
-    bool end_run = false;
-    if (state == S_START || state == S_NEXT) {
-      double H45[45], g9[9];
-      const double chi0 = deriv_pass<T>(P, K, par, step, pp, sw, H45, g9);
-      t_jac++;
-      if (state == S_START) {  // LM_FIT set-up (Src/LM_FIT.c:549-566)
-        chisq = chi0;
-        ratio = 1.0;
-        if (P.regul_any) {
-          penalty = penalty_of(P, par);
-          if (penalty > 0.1 * lmchisq) ratio = 0.1 * chisq / penalty;
-        }
-        it = 0;
-        end_run = (P.niter <= 0);
+    // Hessian_Compute's free-parameter block + Get_Regul(matrix)
+    double g[9];
+    for (int a = 0; a < n; a++) {
+      const int ia = P.free_idx[a];
+      for (int b = a; b < n; b++) {
+        const int ib = P.free_idx[b];
+        double h = H45[ia * 9 - ia * (ia + 1) / 2 + ib];
+        if (a == b && P.regul_any && P.regul[ia]) h += P.regul_weight[ia] * ratio;
+        S.hess[(size_t)(a * n + b) * W + s] = h;
+        S.hess[(size_t)(b * n + a) * W + s] = h;
       }
-      if (!end_run) {
-        // Hessian_Compute's free-parameter block + Get_Regul(matrix)
-        for (int a = 0; a < n; a++) {
-          const int ia = P.free_idx[a];
-          for (int b = a; b < n; b++) {
-            const int ib = P.free_idx[b];
-            const int idx = ia * 9 - ia * (ia + 1) / 2 + ib;  // (ia <= ib)
-            hess[a * n + b] = H45[idx];
-            hess[b * n + a] = H45[idx];
+      g[a] = g9[ia];
+      if (P.regul_any && P.regul[ia]) g[a] -= (par[ia] - P.regul_value[ia]) * P.regul_weight[ia] * ratio;
+    }
+    for (int a = 0; a < n; a++) S.jvec[(size_t)a * W + s] = g[a];
+    S.cnt[1 * W + s]++;
+    S.sc[SC_DAMP * W + s] = P.damp;
+    S.tk[s] = 1;
+    S.state[s] = SL_TRIAL;
+  }
+  if (A.totals && t_jac) atomicAdd(A.totals + 5, t_jac);
+}
+
+// ---------------------------------------------------------------------------
+// The SVD solve of every slot's trial step (SVD_solve_mem, Src/LM_FIT.c:400-469)
+// and its trial parameters (Par_update + bounds_check, Src/LM_FIT.c:511-516).
+//
+// The reference decomposes, at the first trial of an LM iteration, the
+// normal matrix H, and at every later trial the U factor the previous trial's
+// SVD left in its place.  Two exact identities let this kernel skip V:
+//   * H is symmetric positive semi-definite, so its SVD has V = U and the
+//     truncated solve V W+ U^T g equals U W+ U^T g;
+//   * a U factor is orthogonal: its singular values are all 1 (nothing is
+//     truncated at any rung of the threshold ladder) and V W^-1 U^T g is
+//     U_prev^T g, clamped to +-0.5 as the ladder's last rung does.
+// So trial 1 runs the U-only decomposition of H and the ladder; trial k >= 2
+// uses the stored factor directly, and the decomposition that the reference
+// ran at trial k-1 (whose U only trial k+1 needs) is run here at trial k >= 3,
+// i.e. only when the iteration really goes on.  Each thread keeps its matrix
+// in its own column of shared memory.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const DevPlan P, InvertArgs A, Slots S) {
+  extern __shared__ double sm[];
+  const int t = threadIdx.x;
+  double *a = sm + t;
+  double *w = sm + 81 * kSvdBlock + t;
+  double *rv1 = sm + 90 * kSvdBlock + t;
+  const int W = S.W;
+  const int n = P.npar;
+  unsigned long long t_svdlim = 0;
+  for (int s = blockIdx.x * kSvdBlock + t; s < W; s += gridDim.x * kSvdBlock) {
+    if (S.state[s] != SL_TRIAL) continue;
+    const int tk = S.tk[s];
+    double g[9], x[9];
+    for (int k = 0; k < n; k++) g[k] = S.jvec[(size_t)k * W + s];
+    for (int k = 0; k < n * n; k++) a[k * kSvdBlock] = S.hess[(size_t)k * W + s];
+    if (tk == 1) {
+      t_svdlim += gr_svd_u<kSvdBlock>(a, n, w, rv1);
+      double wmax = w[0];
+      for (int i = 1; i < n; i++) wmax = fmax(wmax, w[i * kSvdBlock]);
+      double thr = P.svd_thr;
+      double ug[9];  // U^T g
+      for (int j = 0; j < n; j++) {
+        double acc = 0.0;
+        for (int i = 0; i < n; i++) acc += a[(i * n + j) * kSvdBlock] * g[i];
+        ug[j] = acc;
+      }
+      while (true) {
+        const double wthr = wmax * thr;
+        double tj[9];
+        for (int j = 0; j < n; j++) {
+          double wj = w[j * kSvdBlock];
+          if (wj < wthr) {
+            wj = 0.0;
+            w[j * kSvdBlock] = 0.0;
           }
-          jvec[a] = g9[ia];
+          tj[j] = wj > 1e-50 ? ug[j] / wj : 0.0;
         }
-        if (P.regul_any) {
-          for (int a = 0; a < n; a++) {
-            const int ia = P.free_idx[a];
-            if (!P.regul[ia]) continue;
-            const double r = par[ia] - P.regul_value[ia];
-            jvec[a] -= r * P.regul_weight[ia] * ratio;
-            hess[a * n + a] += P.regul_weight[ia] * ratio;
-          }
+        bool inside = true;
+        for (int i = 0; i < n; i++) {
+          double acc = 0.0;
+          for (int j = 0; j < n; j++) acc += a[(i * n + j) * kSvdBlock] * tj[j];
+          x[i] = acc;
+          if (acc > 0.5 || acc < -0.5) inside = false;
         }
-        pc_iter++;
-        damp = P.damp;
-        state = S_TRIAL;
+        if (inside) break;
+        if (thr > 2e-3) {
+          for (int i = 0; i < n; i++) x[i] = x[i] > 0.5 ? 0.5 : (x[i] < -0.5 ? -0.5 : x[i]);
+          break;
+        }
+        thr *= 5.;
+      }
+    } else {
+      if (tk >= 3) t_svdlim += gr_svd_u<kSvdBlock>(a, n, w, rv1);
+      for (int j = 0; j < n; j++) {
+        double acc = 0.0;
+        for (int i = 0; i < n; i++) acc += a[(i * n + j) * kSvdBlock] * g[i];
+        x[j] = acc > 0.5 ? 0.5 : (acc < -0.5 ? -0.5 : acc);
       }
     }
+    if (tk != 2)
+      for (int k = 0; k < n * n; k++) S.hess[(size_t)k * W + s] = a[k * kSvdBlock];
+    double ptmp[9], step_ia;
+    load9(S.par, W, s, ptmp);
+    for (int q = 0; q < n; q++) {
+      const int ia = P.free_idx[q];
+      step_ia = ia == 7 ? S.sc[SC_STEP7 * W + s] : P.step[ia];
+      ptmp[ia] += x[q] * step_ia;
+    }
+    bounds_fold(ptmp, P, S.sc[SC_L70 * W + s], S.sc[SC_L71 * W + s]);
+    store9(S.ptmp, W, s, ptmp);
+  }
+  if (A.totals && t_svdlim) atomicAdd(A.totals + 6, t_svdlim);
+}
 
-    if (!end_run && state == S_TRIAL) {
-      // ---------------- one trial step (Trial_Synthesis) ----------------
-      t_svdlim += svd_solve(hess, vm, jvec, n, P.svd_thr, sol);
-#pragma unroll
-      for (int i = 0; i < 9; i++) ptmp[i] = par[i];
-      for (int a = 0; a < n; a++) {
-        const int ia = P.free_idx[a];
-        ptmp[ia] += sol[a] * step[ia];
+// ---------------------------------------------------------------------------
+// One trial step for every slot; run and pixel transitions; refills.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kBlock) trial_kernel(const DevPlan P, InvertArgs A, Slots S,
+                                                       int parity) {
+  __shared__ T s_tab[50];
+  fill_table<T>(P, s_tab);
+  VoigtK<T> K;
+  load_voigt<T>(K, P, s_tab);
+  const int W = S.W;
+  const int n = P.npar;
+  const int nl = P.nl;
+  const int next_parity = parity ^ 1;
+  unsigned long long t_valid = 0, t_runs = 0, t_iter = 0, t_trials = 0, t_acc = 0;
+  int busy_delta = 0;
+
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < W; s += gridDim.x * blockDim.x) {
+    int st = S.state[s];
+    if (st == SL_DONE) continue;
+    if (st == SL_EMPTY) {
+      if (refill(P, A, S, s, t_valid)) {
+        busy_delta++;
+        append_jac(S, next_parity, s);
+      } else {
+        S.state[s] = SL_DONE;
       }
-      bounds_fold(ptmp, P, pin.l70, pin.l71);
+      continue;
+    }
+    bool end_run = (st == SL_RUN_END);
+    double par[9];
+    load9(S.par, W, s, par);
+    double *sc = S.sc;
+    double chisq = sc[SC_CHISQ * W + s];
+    double ratio = sc[SC_RATIO * W + s];
+    double lmchisq = sc[SC_LMCHISQ * W + s];
+    const long long pix = S.pix[s];
+    const double *pp = A.prof + (size_t)pix * 4 * nl;
+    double step[9], sw[4];
+#pragma unroll
+    for (int k = 0; k < 9; k++) step[k] = P.step[k];
+    step[7] = sc[SC_STEP7 * W + s];
+    const double isn = sc[SC_ISN * W + s];
+#pragma unroll
+    for (int k = 0; k < 4; k++) sw[k] = P.weights[k] * isn;
+    const double l70 = sc[SC_L70 * W + s], l71 = sc[SC_L71 * W + s];
+
+    if (!end_run) {
+      // --------- Trial_Synthesis (Src/LM_FIT.c:473-527), after svd_kernel ---------
+      double ptmp[9];
+      load9(S.ptmp, W, s, ptmp);
       const double chi_new = forward_pass<T>(P, K, ptmp, step, pp, sw, nullptr);
       lmchisq = chi_new;
-      had_trial = true;
-      pc_trials++;
-      if (P.regul_any) penalty = penalty_of(P, ptmp);
+      S.had_trial[s] = 1;
+      S.cnt[2 * W + s]++;
+      t_trials++;
+      const double penalty = P.regul_any ? penalty_of(P, ptmp) : 0.0;
       if (chi_new < chisq) {  // accept (Src/LM_FIT.c:591-615)
         if (P.regul_any && penalty > 0.1 * lmchisq) ratio = 0.1 * chisq / penalty;
 #pragma unroll
         for (int i = 0; i < 9; i++) par[i] = ptmp[i];
-        pc_acc++;
+        store9(S.par, W, s, par);
+        S.cnt[3 * W + s]++;
+        t_acc++;
         const bool conv = ((chisq - chi_new) / chisq) < P.convg;
         chisq = chi_new;
-        it++;
-        if (conv || it >= P.niter)
+        const int it = S.it[s] + 1;
+        S.it[s] = it;
+        if (conv || it >= P.niter) {
           end_run = true;
-        else
-          state = S_NEXT;
+        } else {
+          S.state[s] = SL_JAC_NEXT;
+          append_jac(S, next_parity, s);
+        }
       } else {  // reject: grow the damping; past its limit the run ends
-        damp *= P.lam_reject;
-        if (damp > P.lam_lim[1]) end_run = true;
+        const double damp = sc[SC_DAMP * W + s] * P.lam_reject;
+        sc[SC_DAMP * W + s] = damp;
+        if (damp > P.lam_lim[1]) {
+          end_run = true;
+        } else {  // another trial, on the SVD's U factor (svd_kernel)
+          S.tk[s]++;
+        }
       }
+      sc[SC_CHISQ * W + s] = chisq;
+      sc[SC_RATIO * W + s] = ratio;
+      sc[SC_LMCHISQ * W + s] = lmchisq;
     }
 
     if (end_run) {
       // ---------------- end of one LM_FIT run (INVERSION) ----------------
-      const double chisq_run = chisq / pin.normp;
-      pc_runs++;
-      if (chisq_run < P.chisq_crit || run == 0 || chisq_run < chisq_best) {
+      const double chisq_run = chisq / sc[SC_NORMP * W + s];
+      int run = S.run[s];
+      S.cnt[0 * W + s]++;
+      t_runs++;
+      double pbest[9];
+      double best = sc[SC_BEST * W + s];
+      if (chisq_run < P.chisq_crit || run == 0 || chisq_run < best) {
 #pragma unroll
         for (int i = 0; i < 9; i++) pbest[i] = par[i];
-        chisq_best = chisq_run;
+        store9(S.pbest, W, s, pbest);
+        best = chisq_run;
+        sc[SC_BEST * W + s] = best;
+      } else {
+        load9(S.pbest, W, s, pbest);
       }
       bool stop = false;
       if (chisq_run < P.chisq_crit && (run >= 4 || run == P.nruns * 4)) stop = true;
-      if (run >= P.nruns * 2 && chisq_best < P.chisq_crit * 2) stop = true;
+      if (run >= P.nruns * 2 && best < P.chisq_crit * 2) stop = true;
       run++;
+      S.run[s] = run;
       if (!stop && run < P.nruns * 4) {
         // Random_Jump (Src/LM_FIT.c:157-201)
+        double g[9];
+        load9(S.guess, W, s, g);
         if (run < 4) {
 #pragma unroll
           for (int i = 0; i < 9; i++) par[i] = pbest[i];
-          par[2] = pin.guess[2] + kPi / 4. * run;
+          par[2] = g[2] + kPi / 4. * run;
         } else {
           double z[8];
           restart_draws(P.seed, pix, run, z);
-          const double *g = pin.guess;
           par[0] = g[0] * (1 + 0.6 * z[0]);
           par[1] = g[1] + kPi / 8. * z[1];
           par[2] = g[2] + kPi / 4. * (run + 0.3 * z[2]);
@@ -307,10 +495,13 @@ __global__ void __launch_bounds__(kInvertBlock, ME_INV_MINB) invert_kernel(const
           par[7] = pbest[7];
           par[8] = g[8] + 0.1 * z[7];
         }
-        bounds_fold(par, P, pin.l70, pin.l71);
-        state = S_START;
+        bounds_fold(par, P, l70, l71);
+        store9(S.par, W, s, par);
+        S.state[s] = SL_JAC_START;
+        append_jac(S, next_parity, s);
       } else {
-        // pixel done: best-fit profile, theta fold, HMI_REF (Src/LM_FIT.c:727-733, 791-799)
+        // pixel done: best-fit profile, theta fold, HMI_REF, result
+        // (Src/LM_FIT.c:727-733, 791-799)
         if (A.fit) forward_pass<T>(P, K, pbest, step, nullptr, sw, A.fit + (size_t)pix * 4 * nl);
         if (pbest[1] > kPi) pbest[1] -= kPi;
         if (P.hmi_ref) {
@@ -320,29 +511,31 @@ __global__ void __launch_bounds__(kInvertBlock, ME_INV_MINB) invert_kernel(const
         double *r = A.res + (size_t)pix * 10;
 #pragma unroll
         for (int i = 0; i < 9; i++) r[i] = pbest[i];
-        r[9] = chisq_best;
-        if (A.flags) A.flags[pix] = 1 | (had_trial ? 2 : 0);
-        if (A.lastchi) A.lastchi[pix] = lmchisq;
+        r[9] = best;
+        if (A.flags) A.flags[pix] = 1 | (S.had_trial[s] ? 2 : 0);
+        if (A.lastchi) A.lastchi[pix] = sc[SC_LMCHISQ * W + s];
         if (A.counters) {
-          uint4 c4 = make_uint4(pc_runs, pc_iter, pc_trials, pc_acc);
+          uint4 c4 = make_uint4(S.cnt[0 * W + s], S.cnt[1 * W + s], S.cnt[2 * W + s],
+                                S.cnt[3 * W + s]);
           reinterpret_cast<uint4 *>(A.counters)[pix] = c4;
         }
-        t_runs += pc_runs;
-        t_iter += pc_iter;
-        t_trials += pc_trials;
-        t_acc += pc_acc;
-        state = S_FETCH;
+        t_iter += S.cnt[1 * W + s];
+        if (refill(P, A, S, s, t_valid)) {
+          append_jac(S, next_parity, s);
+        } else {
+          S.state[s] = SL_DONE;
+          busy_delta--;
+        }
       }
     }
   }
+  if (busy_delta) atomicAdd(S.busy, busy_delta);
   if (A.totals) {
-    atomicAdd(A.totals + 0, t_valid);
-    atomicAdd(A.totals + 1, t_runs);
-    atomicAdd(A.totals + 2, t_iter);
-    atomicAdd(A.totals + 3, t_trials);
-    atomicAdd(A.totals + 4, t_acc);
-    atomicAdd(A.totals + 5, t_jac);
-    atomicAdd(A.totals + 6, t_svdlim);
+    if (t_valid) atomicAdd(A.totals + 0, t_valid);
+    if (t_runs) atomicAdd(A.totals + 1, t_runs);
+    if (t_iter) atomicAdd(A.totals + 2, t_iter);
+    if (t_trials) atomicAdd(A.totals + 3, t_trials);
+    if (t_acc) atomicAdd(A.totals + 4, t_acc);
   }
 }
 

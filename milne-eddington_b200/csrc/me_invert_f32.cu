@@ -1,20 +1,32 @@
-// me_invert_f32.cu -- float instantiation of the inversion kernel.
+// me_invert_f32.cu -- float instantiation of the inversion round kernels.
 #include "me_invert.cuh"
 
 namespace me {
 
-template __global__ void invert_kernel<float>(const DevPlan P, InvertArgs A);
+template __global__ void jac_kernel<float>(const DevPlan P, InvertArgs A, Slots S, int parity);
+template __global__ void trial_kernel<float>(const DevPlan P, InvertArgs A, Slots S, int parity);
 
-int invert_grid_f32(int device) {
+// which: 0 = jac_kernel, 1 = trial_kernel, 2 = svd_kernel (CTAs for a full device)
+int round_grid_f32(int which, int device) {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, invert_kernel<float>, kInvertBlock, 0);
+  if (which == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jac_kernel<float>, kBlock, 0);
+  } else if (which == 1) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trial_kernel<float>, kBlock, 0);
+  } else {
+    cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSvdSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, svd_kernel, kSvdBlock, kSvdSmem);
+  }
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
 
-cudaError_t launch_invert_f32(const DevPlan &P, const InvertArgs &A, int grid, cudaStream_t st) {
-  invert_kernel<float><<<grid, kInvertBlock, 0, st>>>(P, A);
+cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
+                           const int grids[3], cudaStream_t st) {
+  jac_kernel<float><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
+  svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S);
+  trial_kernel<float><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
   return cudaGetLastError();
 }
 

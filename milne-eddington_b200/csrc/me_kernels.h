@@ -1,5 +1,5 @@
 // me_kernels.h -- launch interface between the host plan (me_api.cu) and the
-// CUDA kernels (me_kernels.cu).
+// CUDA kernels (me_invert.cuh, me_units.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -8,34 +8,73 @@
 
 namespace me {
 
-constexpr int kInvertBlock = 128;
-// minimum resident CTAs per SM the inversion kernel is compiled for (caps
-// its registers at 65536 / (128 * ME_INV_MINB))
-#ifndef ME_INV_MINB
-#define ME_INV_MINB 3
-#endif
+constexpr int kBlock = 128;
+constexpr int kSvdBlock = 64;  // threads of svd_kernel; each holds its matrix in shared memory
+constexpr int kSvdSmem = (81 + 18) * kSvdBlock * 8;
 
-// Buffers of one inversion launch (all device pointers).
+// Life cycle of an inversion slot (one pixel in flight).
+enum SlotStateCode : int {
+  SL_EMPTY = 0,      // waiting for a pixel from the queue
+  SL_JAC_START = 1,  // first synthesis of an LM run (LM_FIT set-up)
+  SL_JAC_NEXT = 2,   // synthesis at newly accepted parameters (next iteration)
+  SL_TRIAL = 3,      // normal equations ready: trial steps
+  SL_RUN_END = 4,    // run ended without a trial step (num_iter <= 0)
+  SL_DONE = 5,       // queue exhausted
+};
+
+// Per-slot scalars, stored [SC_COUNT][W].
+enum SlotScalar : int {
+  SC_CHISQ = 0,    // the LM's current chi^2 (Chisq in LM_FIT)
+  SC_LMCHISQ,      // LM->chisq: chi^2 of the last trial step, carried
+  SC_RATIO,        // LM->ratio (regularisation scaling)
+  SC_DAMP,         // LM->Damp
+  SC_BEST,         // Para->Chisq_Best
+  SC_NORMP,        // Stk->normp
+  SC_ISN,          // 1 / sqrt(Stk->norm0)
+  SC_STEP7,        // Para->step[7] of this pixel
+  SC_L70, SC_L71,  // Para->Limits[7] of this pixel
+  SC_COUNT
+};
+
+// Device state of the in-flight pixels, structure of arrays over W slots so
+// that consecutive threads touch consecutive addresses.
+struct Slots {
+  int W;
+  long long *pix;            // [W]
+  int *state, *run, *it;     // [W]
+  unsigned int *cnt;         // [4][W] runs, iterations, trials, accepted
+  unsigned char *had_trial;  // [W]
+  double *sc;                // [SC_COUNT][W]
+  double *guess, *par, *pbest, *jvec;  // [9][W]
+  double *hess;              // [81][W]: normal matrix, then the SVD's U factor
+  double *ptmp;              // [9][W]: trial parameters of this round
+  int *tk;                   // [W]: index of the trial step within the LM iteration (1 = first)
+  int *jlist;                // [2][W] slots needing a synthesis with Jacobian
+  int *jcount;               // [2]
+  int *busy;                 // slots holding a pixel
+};
+
+// One batch (all device pointers).
 struct InvertArgs {
   const double *prof;          // [npix][4][nl]
   double *res;                 // [npix][10]
   double *fit;                 // [npix][4][nl] or null
-  unsigned char *flags;        // [npix] bit0 inverted, bit1 made a trial step (or null)
-  double *penalty0;            // [npix] regularisation penalty at the first guess (or null)
-  double *lastchi;             // [npix] chi^2 of the pixel's last trial step (or null)
-  unsigned int *counters;      // [npix][4] runs, iterations, trials, accepted (or null)
+  unsigned char *flags;        // [npix] bit0 inverted, bit1 made a trial step
+  double *penalty0;            // [npix] regularisation penalty at the first guess
+  double *lastchi;             // [npix] chi^2 of the pixel's last trial step
+  unsigned int *counters;      // [npix][4] runs, iterations, trials, accepted
   unsigned long long *totals;  // [8] valid, runs, iterations, trials, accepted, jacobians, svd limit hits
-  unsigned long long *next;    // work counter (zeroed before the launch)
+  unsigned long long *next;    // queue position (zeroed before the batch)
   const long long *list;       // pixel indices to process (null = 0..count-1)
-  long long count;             // number of work items
-  const double *stale;         // [npix] carried LM chi^2 per pixel (null = use carry/first_pixel)
+  long long count;             // number of queue items
+  const double *stale;         // [npix] carried LM chi^2 per pixel (null = carry/first_pixel)
   double carry;                // carried LM chi^2 for pixel first_pixel
   long long first_pixel;
 };
 
-int invert_grid(int precision, int device);
-cudaError_t launch_invert(int precision, const DevPlan &P, const InvertArgs &A, int grid,
-                          cudaStream_t st);
+int round_grid(int precision, int which, int device);
+cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                         int parity, const int grids[3], cudaStream_t st);
 cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,
                          double step7, double *d_prof, double *d_jac, cudaStream_t st);
 cudaError_t launch_voigt(int precision, const DevPlan &P, const double *d_nu, const double *d_a,

@@ -117,18 +117,21 @@ __global__ void init_guess_kernel(const DevPlan P, const double *prof, long long
 // launchers
 // ---------------------------------------------------------------------------
 
-int invert_grid_f32(int device);
-int invert_grid_f64(int device);
-cudaError_t launch_invert_f32(const DevPlan &P, const InvertArgs &A, int grid, cudaStream_t st);
-cudaError_t launch_invert_f64(const DevPlan &P, const InvertArgs &A, int grid, cudaStream_t st);
+int round_grid_f32(int which, int device);
+int round_grid_f64(int which, int device);
+cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
+                             const int grids[3], cudaStream_t st);
+cudaError_t launch_round_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
+                             const int grids[3], cudaStream_t st);
 
-int invert_grid(int precision, int device) {
-  return precision == 1 ? invert_grid_f64(device) : invert_grid_f32(device);
+int round_grid(int precision, int which, int device) {
+  return precision == 1 ? round_grid_f64(which, device) : round_grid_f32(which, device);
 }
 
-cudaError_t launch_invert(int precision, const DevPlan &P, const InvertArgs &A, int grid,
-                          cudaStream_t st) {
-  return precision == 1 ? launch_invert_f64(P, A, grid, st) : launch_invert_f32(P, A, grid, st);
+cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                         int parity, const int grids[3], cudaStream_t st) {
+  return precision == 1 ? launch_round_f64(P, A, S, parity, grids, st)
+                        : launch_round_f32(P, A, S, parity, grids, st);
 }
 
 cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,

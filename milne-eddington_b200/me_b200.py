@@ -112,6 +112,7 @@ class MeStats(ctypes.Structure):
         ("wavelengths", ctypes.c_longlong),
         ("redo_pixels", ctypes.c_longlong),
         ("launches", ctypes.c_longlong),
+        ("rounds", ctypes.c_longlong),
         ("kernel_ms", ctypes.c_double),
         ("h2d_ms", ctypes.c_double),
         ("d2h_ms", ctypes.c_double),
@@ -128,7 +129,7 @@ EXPORTED = [
     "me_plan_get_carry_chisq", "me_plan_set_carry_chisq", "me_plan_grid", "me_plan_set_grid",
     "me_invert_batch", "me_invert_batch_device", "me_synthesize", "me_synthesize_device",
     "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
-    "me_synthesize_jacobian_device",
+    "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
 ]
 
 
@@ -168,6 +169,9 @@ def lib() -> ctypes.CDLL:
         L.me_plan_grid.argtypes = [ctypes.c_void_p]
         L.me_plan_set_grid.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_grid.restype = None
+        L.me_plan_window.argtypes = [ctypes.c_void_p]
+        L.me_plan_set_window.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_window.restype = None
         L.me_invert_batch.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                       ctypes.POINTER(MeStats)]
         L.me_invert_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
@@ -286,6 +290,14 @@ class Plan:
     @grid.setter
     def grid(self, g: int):
         lib().me_plan_set_grid(self._h, int(g))
+
+    @property
+    def window(self) -> int:
+        return lib().me_plan_window(self._h)
+
+    @window.setter
+    def window(self, w: int):
+        lib().me_plan_set_window(self._h, int(w))
 
     def invert(self, prof: np.ndarray, want_fit: bool = False):
         """me_invert_batch on host arrays: prof [npix][4][nl] -> res [npix][10] (+fit)."""
