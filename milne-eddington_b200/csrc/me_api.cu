@@ -132,10 +132,12 @@ extern "C" const char *me_strerror(int status) {
   }
 }
 
-extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl, int device,
-                              me_plan **out) {
-  if (!cfg || !lambda || !out) return fail(ME_ERR_ARG, "null argument");
-  *out = nullptr;
+namespace me {
+
+// The plan constants INIT_INV derives (Src/INV_INIT.c:112-201) from a parsed
+// control file and a wavelength grid; P.lambda / P.dlambda are left null.
+int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P) {
+  if (!cfg || !lambda) return fail(ME_ERR_ARG, "null argument");
   if (nl < 4 || nl > ME_MAX_NL) return fail(ME_ERR_ARG, "nl must be in [4, 512]");
   if (cfg->nline < 1) return fail(ME_ERR_CONFIG, "no spectral line (keyword lines)");
   if (cfg->nfigures > 8) return fail(ME_ERR_CONFIG, "Nfigures above 8 has no accuracy row");
@@ -143,16 +145,7 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
   // upper limit (Src/LM_FIT.c:144-150)
   if (!(cfg->damp > 0) || !(cfg->lambda_reject > 1) || !isfinite(cfg->lambda_limits[1]))
     return fail(ME_ERR_CONFIG, "damp must be > 0, lambda_reject > 1, lambda_limits finite");
-  int st = check_device(device);
-  if (st) return st;
-
-  me_plan *p = new me_plan();
-  p->cfg = *cfg;
-  p->device = device;
-  p->precision = cfg->precision == ME_PREC_FP64 ? ME_PREC_FP64 : ME_PREC_FP32;
-  me::DevPlan &P = p->P;
   memset(&P, 0, sizeof(P));
-  // INIT_INV (Src/INV_INIT.c:112-201)
   const double lam0 = cfg->line_lambda0[0];
   P.nl = nl;
   P.lambda0 = lam0;
@@ -168,10 +161,7 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
     P.regul_value[i] = cfg->regul_value[i];
     P.regul_weight[i] = cfg->regul_weight[i];
   }
-  if (P.npar == 0) {
-    delete p;
-    return fail(ME_ERR_CONFIG, "all nine parameters are fixed");
-  }
+  if (P.npar == 0) return fail(ME_ERR_CONFIG, "all nine parameters are fixed");
   P.ncut = nl / 5;
   const double c = 299792458.0;
   double t = (lambda[P.ncut] - lam0) * c / 1e3;  // the reference omits /lambda0 here
@@ -222,7 +212,28 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
   P.regul_any = cfg->regul_any ? 1 : 0;
   P.seed = cfg->rng_seed;
   fill_voigt_consts(P, cfg->nfigures);
+  return ME_OK;
+}
 
+}  // namespace me
+
+extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl, int device,
+                              me_plan **out) {
+  if (!cfg || !lambda || !out) return fail(ME_ERR_ARG, "null argument");
+  *out = nullptr;
+  me::DevPlan P0;
+  int st = me::build_devplan(cfg, lambda, nl, P0);
+  if (st) return st;
+  st = check_device(device);
+  if (st) return st;
+
+  me_plan *p = new me_plan();
+  p->cfg = *cfg;
+  p->device = device;
+  p->precision = cfg->precision == ME_PREC_FP64 ? ME_PREC_FP64 : ME_PREC_FP32;
+  me::DevPlan &P = p->P;
+  P = P0;
+  const double lam0 = P.lambda0;
   std::vector<double> dl(nl);
   for (int i = 0; i < nl; i++) dl[i] = lambda[i] - lam0;
   if (p->d_lambda.ensure(sizeof(double) * nl) || p->d_dlambda.ensure(sizeof(double) * nl) ||

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/me_b200.h"
 #include "me_device.cuh"
 
 namespace me {
@@ -71,6 +72,10 @@ struct InvertArgs {
   double carry;                // carried LM chi^2 for pixel first_pixel
   long long first_pixel;
 };
+
+// Plan constants from a control file and a wavelength grid (me_api.cu);
+// returns an ME_* status, P.lambda / P.dlambda left null.
+int build_devplan(const struct me_config *cfg, const double *lambda, int nl, DevPlan &P);
 
 int round_grid(int precision, int which, int device);
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
