@@ -209,6 +209,37 @@ int me_svd_device(const double *d_a, long nmat, int n, double *d_u, double *d_w,
 int me_synthesize_jacobian_device(me_plan *plan, const double *d_par, long npix, double step7,
                                   double *d_prof, double *d_jac, void *stream);
 
+/* me_invert_batch_device without any device allocation, for callers that
+ * cannot allocate while they invert: code running while a CUDA graph is being
+ * captured, pipelines that give their whole GPU memory to their own pool up
+ * front, real-time loops that must not block in the allocator.  No reference
+ * counterpart: it replaces the same INVERSION_MULTI (Src/LM_FIT.c:746-811) as
+ * me_invert_batch_device, with the control file and the wavelength grid
+ * (host arrays) instead of a plan.
+ *
+ * All of its scratch lives in one static device array of fixed size (about
+ * 12.4 MB, held on every GPU the library is loaded on until the process
+ * exits): at most ME_NOALLOC_MAX_PIXELS pixels per call, ME_NOALLOC_SLOTS of
+ * them in flight; a larger npix is rejected with ME_ERR_ARG -- invert large
+ * maps in chunks, passing *carry_chisq (the LM chi^2 carried from pixel to
+ * pixel, 0 at the start of a map) from one call to the next.  d_prof
+ * [npix][4][nl] and d_res [npix][10] are device buffers of the caller; the
+ * work is ordered on `stream` (a cudaStream_t, NULL = legacy default stream)
+ * and complete when the call returns.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and the kernels' occupancy with that device current;
+ * make that first call before any stream capture.  Every call on a device
+ * shares the one array, which keeps the previous call's contents (the call
+ * clears what must start at zero): calls that overlap on the GPU -- from two
+ * host threads or two streams at once -- race and must be serialised by the
+ * caller. */
+#define ME_NOALLOC_MAX_PIXELS 65536
+#define ME_NOALLOC_SLOTS 8192
+int me_invert_batch_device_noalloc(const me_config *cfg, const double *lambda, int nl,
+                                   const double *d_prof, long npix, double *d_res,
+                                   double *carry_chisq, void *stream);
+
 /* Initial guess for npix profiles: guess [npix][9]; extra [npix][5] =
  * norm0, normp, S lower limit, S upper limit, S step; status [npix] (0 ok,
  * 1 below Icriteria).  Replaces Init_Guess (Src/ME_SOLVER.c:445-676). */

@@ -134,6 +134,8 @@ extern "C" const char *me_strerror(int status) {
 
 namespace me {
 
+int record_error(int code, const char *msg) { return fail(code, msg); }
+
 // The plan constants INIT_INV derives (Src/INV_INIT.c:112-201) from a parsed
 // control file and a wavelength grid; P.lambda / P.dlambda are left null.
 int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P) {

@@ -77,6 +77,9 @@ struct InvertArgs {
 // returns an ME_* status, P.lambda / P.dlambda left null.
 int build_devplan(const struct me_config *cfg, const double *lambda, int nl, DevPlan &P);
 
+// Records `msg` as the calling thread's me_last_error(); returns `code`.
+int record_error(int code, const char *msg);
+
 int round_grid(int precision, int which, int device);
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                          int parity, const int grids[3], cudaStream_t st);

@@ -130,6 +130,7 @@ EXPORTED = [
     "me_invert_batch", "me_invert_batch_device", "me_synthesize", "me_synthesize_device",
     "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
     "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
+    "me_invert_batch_device_noalloc",
 ]
 
 
@@ -191,6 +192,9 @@ def lib() -> ctypes.CDLL:
                                                     ctypes.c_long, ctypes.c_double,
                                                     ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p]
+        L.me_invert_batch_device_noalloc.argtypes = [ctypes.POINTER(MeConfig), _D, ctypes.c_int,
+                                                     ctypes.c_void_p, ctypes.c_long,
+                                                     ctypes.c_void_p, _D, ctypes.c_void_p]
         L.me_init_guess.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                     ctypes.POINTER(ctypes.c_int)]
         _lib = L
@@ -371,6 +375,21 @@ def faddeeva(nfigures: int, nu: np.ndarray, a: np.ndarray, precision: int = ME_P
     _check(lib().me_faddeeva(nfigures, precision, _ptr(nu), _ptr(a), nu.size, _ptr(H), _ptr(L),
                              device), "me_faddeeva")
     return H, L
+
+
+def invert_device_noalloc(cfg: MeConfig, wavelengths: np.ndarray, d_prof: int, npix: int,
+                          d_res: int, carry_chisq: float = 0.0, stream: int = 0) -> float:
+    """me_invert_batch_device_noalloc: the inversion with no device allocation
+    (fixed static scratch, at most ME_NOALLOC_MAX_PIXELS = 65536 pixels per
+    call).  Returns the LM chi^2 to carry into the next call of the same map."""
+    lam = np.ascontiguousarray(wavelengths, dtype=np.float64)
+    carry = np.array([carry_chisq], dtype=np.float64)
+    _check(lib().me_invert_batch_device_noalloc(ctypes.byref(cfg), _ptr(lam), lam.size,
+                                                ctypes.c_void_p(d_prof), npix,
+                                                ctypes.c_void_p(d_res), _ptr(carry),
+                                                ctypes.c_void_p(stream) if stream else None),
+           "me_invert_batch_device_noalloc")
+    return float(carry[0])
 
 
 def svd_device(d_a: int, nmat: int, n: int, d_u: int, d_w: int, d_v: int, stream: int = 0):
