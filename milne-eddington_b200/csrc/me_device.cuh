@@ -20,6 +20,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace me {
 
 constexpr double kPi = 3.14159265358979323846;
@@ -75,13 +77,37 @@ __device__ __forceinline__ void m_sincos(double x, double *s, double *c) { sinco
 // ---------------------------------------------------------------------------
 // Voigt H(nu, a) and Faraday-Voigt L(nu, a) = Re, Im of w(nu + i a)
 // ---------------------------------------------------------------------------
+constexpr int kRden = 32;  // reciprocal table 1 / (a^2 n^2 + y^2), n < kRden
+
 template <class T>
 struct VoigtK {
-  T a, aa, log_rmin0, sqrt_log_rmin0;
+  T a, aa, inv_a, log_rmin0, sqrt_log_rmin0;
+  T ema2, em2a2;  // exp(-a^2), exp(-2 a^2)
   int nmax, nfig;
   T thr[5];
-  const T *ea2n2;  // exp(-a^2 n^2), n = 0..49 (shared memory)
+  const T *ea2n2;  // exp(-a^2 n^2), n = 0..49 (shared memory, per block)
+  const T *e2an;   // exp(-2 a^2 n), n = 0..49 (shared memory, per block)
+  // per synthesis (FP32 path): y = damping and this thread's reciprocal table
+  T yy, inv_y;
+  const T *rden;   // rden[n * rstride] = 1 / (a^2 n^2 + y^2)
+  int rstride;
 };
+
+// Fills the y-dependent part of K for one synthesis at damping y.  On the FP32
+// path every Alg-916 series term 1 / (a^2 n^2 + y^2) then comes from this
+// thread's table instead of a division (the damping is one number per
+// synthesis).  `rden` is this thread's base in shared memory, stride `stride`.
+template <class T>
+__device__ __forceinline__ void voigt_prepare(VoigtK<T> &K, T y, T *rden, int stride) {
+  K.yy = y * y;
+  K.inv_y = T(1) / y;
+  K.rden = rden;
+  K.rstride = stride;
+  if (sizeof(T) == sizeof(float) && rden) {
+#pragma unroll 4
+    for (int n = 0; n < kRden; n++) rden[n * stride] = T(1) / (K.aa * T(n * n) + K.yy);
+  }
+}
 
 // (H, L) pair returned by the Voigt evaluators.
 template <class T>
@@ -223,10 +249,94 @@ __device__ HL<T> voigt_humlicek_w4(T nu, T y) {
   return {H, L};
 }
 
-// Zaghloul & Ali (2011) ACM Algorithm 916 (FADDEEVA.c:286-402).  erfcx_y is
-// erfcx(y), constant over one synthesis, computed once per call by the caller.
+// FP32 form of Alg 916 with the same series, terms and cut-offs, arranged for
+// the GPU: the 1 / (a^2 n^2 + y^2) factors come from the per-synthesis table;
+// with d_b = x - a n_b and d_f = a - d_b (n_f = n_b + 1), exp(-d_f^2) and
+// exp(-2 a d_f) follow from exp(-d_b^2) and exp(-2 a d_b) and the constants
+// exp(-a^2), exp(-2 a^2); exp(-2 a x) = exp(-2 a^2 n_b) exp(-2 a d_b); and
+// 2 a x sin(xy)^2 / (xy pi) = 2 a sin(xy)^2 / (y pi).
+__device__ __forceinline__ HL<float> voigt_alg916_f32(float nu, float y, float erfcx_y,
+                                                      const VoigtK<float> &K) {
+  if (nu == 0.f) return {erfcx_y, 0.f};
+  if (y == 0.f) return {expf(-nu * nu), float(2.0 / kSqrtPi) * dawson_t(nu)};
+  const float x = fabsf(nu), ya = fabsf(y);
+  if (x + ya > 1e7f) {
+    if (x < ya) {
+      const float xs = __fdividef(x, ya), r = __fdividef(float(1.0 / kSqrtPi), xs * xs + 1.f);
+      return {r, xs * r};
+    }
+    const float ys = __fdividef(ya, x), r = __fdividef(float(1.0 / kSqrtPi), ys * ys + 1.f);
+    return {ys * r, r};
+  }
+  const float a = K.a;
+  const float xx = x * x, xy = x * y;
+  float sxy, cxy;
+  sincosf(xy, &sxy, &cxy);
+  const float s2 = 2.f * sxy * cxy;
+  const float c2 = (cxy - sxy) * (cxy + sxy);
+  const float exx = expf(-xx);
+  const float k1 = exx * erfcx_y;
+  const float r2 = K.log_rmin0 - xx;
+  const int nmax1 = r2 >= 0.f ? (int)(sqrtf(r2) * K.inv_a + 0.5f) : -2147483647;
+  const int nmax2 = (int)((K.sqrt_log_rmin0 - x) * K.inv_a + 0.5f);
+  int nmax = nmax1 > nmax2 ? nmax1 : nmax2;
+  if (nmax >= K.nmax) nmax = K.nmax - 1;
+  const int nb = (int)(x * K.inv_a + 0.5f);
+  const int nf = nb + 1;
+  const float dxb = x - a * nb;
+  const float dxf = a - dxb;
+  int nmaxf = (int)((K.sqrt_log_rmin0 - dxf) * K.inv_a);
+  int nmaxb = (int)((K.sqrt_log_rmin0 - dxb) * K.inv_a);
+  if (nmaxf >= K.nmax) nmaxf = K.nmax - 1;
+  if (nmaxb >= K.nmax) nmaxb = K.nmax - 1;
+  const int nlo = (nb - nmaxb) > 1 ? (nb - nmaxb) : 1;
+  const float inv_pi = float(1.0 / kPi);
+  const float ay = a * K.inv_y * inv_pi * exx;
+  float re = k1 * c2 + 2.f * ay * sxy * sxy;
+  float im = -k1 * s2 + ay * s2;
+  const float e1b = expf(-dxb * dxb);
+  const float e2b = expf(-2.f * a * dxb);
+  const float ie2b = __fdividef(1.f, e2b);
+  const float e1f = K.ema2 * e1b * ie2b;
+  const float e2f = K.em2a2 * ie2b;
+  auto rd = [&](int n) {
+    return n < kRden ? K.rden[n * K.rstride] : __fdividef(1.f, K.aa * float(n * n) + K.yy);
+  };
+  float s1 = 0.f, s2s = 0.f, s3 = 0.f, s4 = 0.f, s5 = 0.f, ep = 1.f;
+  for (int n = nf; n <= nf + nmaxf; n++) {
+    const float t = e1f * K.ea2n2[n - nf] * rd(n) * ep;
+    s3 += t;
+    s5 += t * float(n);
+    ep *= e2f;
+  }
+  ep = 1.f;
+  for (int n = nb; n >= nlo; n--) {
+    const float t = e1b * K.ea2n2[nb - n] * rd(n) * ep;
+    s3 += t;
+    s5 += t * float(n);
+    ep *= e2b;
+  }
+  re += a * y * s3 * inv_pi;
+  im += a * a * s5 * inv_pi;
+  if (x < K.sqrt_log_rmin0 || x < 10.f) {
+    const float q = (nb < 50 ? K.e2an[nb] : expf(-2.f * K.aa * nb)) * e2b;  // exp(-2 a x)
+    ep = 1.f;
+    for (int n = 1; n <= nmax; n++) {
+      const float t = exx * K.ea2n2[n] * rd(n);
+      s1 += t;
+      ep *= q;
+      s2s += t * ep;
+      s4 += t * ep * float(n);
+    }
+    re += a * y * (-2.f * c2 * s1 + s2s) * inv_pi;
+    im += a * (2.f * y * s2 * s1 - a * s4) * inv_pi;
+  }
+  return {re, nu > 0.f ? im : -im};
+}
+
 template <class T>
 __device__ __forceinline__ HL<T> voigt_alg916(T nu, T y, T erfcx_y, const VoigtK<T> &K) {
+  if constexpr (sizeof(T) == sizeof(float)) return voigt_alg916_f32(nu, y, erfcx_y, K);
   if (nu == T(0)) {
     return {erfcx_y, T(0)};
   } else if (y == T(0)) {
@@ -305,9 +415,13 @@ __device__ __forceinline__ HL<T> voigt_alg916(T nu, T y, T erfcx_y, const VoigtK
   return {re, nu > T(0) ? im : -im};
 }
 
-// Accuracy-selected w(z) (Zaghloul 2018 regions; FADDEEVA.c:440-590).
+// Reciprocal: the MUFU approximation on the FP32 path (<= 2 ulp), exact
+// division in FP64.
+__device__ __forceinline__ float rcp_t(float x) { return __fdividef(1.f, x); }
+__device__ __forceinline__ double rcp_t(double x) { return 1.0 / x; }
+
 template <class T>
-__device__ __noinline__ HL<T> voigt(T nu, T y, T erfcx_y, const VoigtK<T> K) {
+__device__ __forceinline__ HL<T> voigt(T nu, T y, T erfcx_y, const VoigtK<T> &K) {
   T H, L;
   if (nu == T(0)) {
     return {erfcx_y, T(0)};
@@ -320,21 +434,21 @@ __device__ __noinline__ HL<T> voigt(T nu, T y, T erfcx_y, const VoigtK<T> K) {
   const T r2 = zr * zr + zi * zi;
   const T y2 = y * y;
   if (r2 >= K.thr[0]) {
-    T den = T(kSqrtPi) * r2;
-    H = zi / den;
-    L = zr / den;
+    const T rden = rcp_t(T(kSqrtPi) * r2);
+    H = zi * rden;
+    L = zr * rden;
   } else if (r2 >= K.thr[1]) {
     T wr = z2r - T(0.5);
-    T den = T(kSqrtPi) * (wr * wr + z2i * z2i);
-    H = (-zi * wr + zr * z2i) / den;
-    L = (zr * wr + zi * z2i) / den;
+    const T rden = rcp_t(T(kSqrtPi) * (wr * wr + z2i * z2i));
+    H = (-zi * wr + zr * z2i) * rden;
+    L = (zr * wr + zi * z2i) * rden;
   } else if (r2 >= K.thr[2]) {
     T wr = z2r - T(1.5);
     T pr = wr * zr - z2i * zi, pi = wr * zi + z2i * zr;
-    T den = T(kSqrtPi) * (pr * pr + pi * pi);
+    const T rden = rcp_t(T(kSqrtPi) * (pr * pr + pi * pi));
     wr = z2r - T(1);
-    H = (-z2i * pr + wr * pi) / den;
-    L = (wr * pr + z2i * pi) / den;
+    H = (-z2i * pr + wr * pi) * rden;
+    L = (wr * pr + z2i * pi) * rden;
   } else if (r2 >= K.thr[3]) {
     if ((K.nfig <= 4 && y2 < T(6e-14)) || (K.nfig == 5 && r2 < T(39) && y2 < T(1e-9))) {
       return voigt_humlicek_w4(nu, y);
@@ -343,9 +457,9 @@ __device__ __noinline__ HL<T> voigt(T nu, T y, T erfcx_y, const VoigtK<T> K) {
     T ar = -(wr * zi + z2i * zr), ai = wr * zr - z2i * zi;
     wr = z2r - T(3);
     T br = wr * z2r - z2i * z2i + T(0.75), bi = (wr + z2r) * z2i;
-    T den = T(kSqrtPi) * (br * br + bi * bi);
-    H = (ar * br + ai * bi) / den;
-    L = (-ar * bi + ai * br) / den;
+    const T rden = rcp_t(T(kSqrtPi) * (br * br + bi * bi));
+    H = (ar * br + ai * bi) * rden;
+    L = (-ar * bi + ai * br) * rden;
   } else if (r2 >= K.thr[4]) {
     if (K.nfig <= 4) {
       if (y2 < T(0.026))
@@ -382,12 +496,41 @@ __device__ __noinline__ HL<T> voigt(T nu, T y, T erfcx_y, const VoigtK<T> K) {
   return {H, L};
 }
 
+
+// Block-wide Voigt tables in shared memory (s_tab: [100] = exp(-a^2 n^2), then
+// exp(-2 a^2 n)) and the per-block constants; call once per block (syncs).
+template <class T>
+__device__ __forceinline__ void voigt_block_setup(VoigtK<T> &K, const DevPlan &P, T *s_tab) {
+  for (int i = threadIdx.x; i < 50; i += blockDim.x) {
+    s_tab[i] = T(P.exp_a2n2[i]);
+    s_tab[50 + i] = T(exp(-2.0 * P.faa * i));
+  }
+  __syncthreads();
+  K.a = T(P.fa);
+  K.aa = T(P.faa);
+  K.inv_a = T(1.0 / P.fa);
+  K.log_rmin0 = T(P.flog_rmin0);
+  K.sqrt_log_rmin0 = T(P.fsqrt_log_rmin0);
+  K.ema2 = T(exp(-P.faa));
+  K.em2a2 = T(exp(-2.0 * P.faa));
+  K.nmax = P.fnmax;
+  K.nfig = P.nfigures;
+#pragma unroll
+  for (int i = 0; i < 5; i++) K.thr[i] = T(P.thr[i]);
+  K.ea2n2 = s_tab;
+  K.e2an = s_tab + 50;
+  K.rden = nullptr;
+  K.rstride = 0;
+  K.yy = T(0);
+  K.inv_y = T(0);
+}
+
 // ---------------------------------------------------------------------------
 // Milne-Eddington synthesis at one wavelength (ME_SOLVER.c:189-362)
 // ---------------------------------------------------------------------------
 template <class T>
 struct SynthCall {
-  T p4, p5, p6, p7, p8;
+  T p4, p5, p6, p7, p8, inv_p4, inv_p6;
   T eta_half, b0, b1, bsh_n, lam_n;
   T sth, cth, sth2, cth2p1, c2p, s2p, kq, ku, kt, kv;
   T shift_b, vshift;  // Zeeman and Doppler shifts
@@ -403,6 +546,8 @@ __device__ __forceinline__ void synth_setup(SynthCall<T> &c, const double *mp, c
   c.p6 = T(mp[6]);
   c.p7 = T(mp[7]);
   c.p8 = T(mp[8]);
+  c.inv_p4 = T(1.0 / mp[4]);
+  c.inv_p6 = T(1.0 / mp[6]);
   c.eta_half = T(0.5) * c.p6;
   c.b0 = c.p7 * c.p8;
   c.b1 = c.p7 - c.b0;
@@ -442,7 +587,7 @@ __device__ __forceinline__ T shift_w(const SynthCall<T> &c, const DevPlan &P, in
 template <>
 __device__ __forceinline__ float shift_w<float>(const SynthCall<float> &c, const DevPlan &P,
                                                 int iw) {
-  return (1e3f * float(__ldg(P.dlambda + iw)) - c.vshift) / c.p4;
+  return (1e3f * float(__ldg(P.dlambda + iw)) - c.vshift) * c.inv_p4;
 }
 template <>
 __device__ __forceinline__ double shift_w<double>(const SynthCall<double> &c, const DevPlan &P,
@@ -450,139 +595,196 @@ __device__ __forceinline__ double shift_w<double>(const SynthCall<double> &c, co
   return 1e3 * __ldg(P.lambda + iw) / c.p4 + c.vshift;
 }
 
-// syn[4] = I, Q, U, V; with DERIV also J[4][9] (derivatives scaled by step[]).
+// One wavelength of Milne_Eddington_Single.  syn[4] = I, Q, U, V.  With
+// DERIV also J[s][k] = d syn_s / d p_k * step[k] * sw[s] (sw: per-Stokes
+// weights the caller wants folded in, 1 for the plain Jacobian).
+//
+// The analytic Jacobian is organised by the chain rule: the Stokes vector
+// depends on the parameters only through the seven absorption-matrix
+// elements x = (eta_I, eta_Q, eta_U, eta_V, rho_Q, rho_U, rho_V), so
+// J = G (dx/dp) with G = dS/dx (4 x 7) formed once per wavelength from the
+// Unno-Rachkovsky solution, and dx/dp from the profile derivatives
+// (LL04 9.110; the same derivatives as Src/ME_SOLVER.c:249-361, regrouped).
+// The three Zeeman components are visited in a loop that accumulates their
+// contributions, so the Voigt evaluation appears once in the code.
 template <class T, bool DERIV>
-__device__ __forceinline__ void me_point(const SynthCall<T> &c, T w0, const VoigtK<T> &K, T syn[4],
-                                         T J[4][9]) {
+__device__ __forceinline__ void me_point(const SynthCall<T> &c, T w0, const VoigtK<T> &K,
+                                         const T sw[4], T syn[4], T J[4][9]) {
   const T rsp = T(1.0 / kSqrtPi);
-  T phi[3], psi[3], dphi[3][4], dpsi[3][4];  // derivative slots: B, v, width, a
+  // sums over the components: "1" = pi (q = 0), "s" = half the sigma sum,
+  // "d" = sigma_b - sigma_r; for the profiles and for the derivative slots
+  // j = B, v, Doppler width, damping
+  T f1 = 0, fs = 0, fd = 0, g1 = 0, gs = 0, gd = 0;
+  T df1[4], dfs[4], dfd[4], dg1[4], dgs[4], dgd[4];
+  if (DERIV) {
 #pragma unroll
+    for (int j = 0; j < 4; j++) df1[j] = dfs[j] = dfd[j] = dg1[j] = dgs[j] = dgd[j] = 0;
+  }
+#pragma unroll 1
   for (int k = 0; k < 3; k++) {
     const int q = k - 1;
     const T v = w0 + T(q) * c.shift_b;
     const HL<T> hl = voigt<T>(v, c.p5, c.erfcx_y, K);
-    const T H = hl.h, L = hl.l;
-    phi[k] = H * rsp;
-    psi[k] = L * rsp;
+    const T phi = hl.h * rsp, psi = hl.l * rsp;
+    const T w1 = q == 0 ? T(1) : T(0);
+    const T ws = q == 0 ? T(0) : T(0.5);
+    const T wd = T(-q);  // +1 for sigma_b (q = -1), -1 for sigma_r
+    f1 += w1 * phi;
+    fs += ws * phi;
+    fd += wd * phi;
+    g1 += w1 * psi;
+    gs += ws * psi;
+    gd += wd * psi;
     if (DERIV) {
-      const T dH = T(2) * (-v * H + c.p5 * L) * rsp;
-      const T dL = T(-2) * (-rsp + c.p5 * H + v * L) * rsp;
-      dphi[k][0] = T(q) * c.bsh_n * dH;
-      dpsi[k][0] = T(q) * c.bsh_n * dL;
-      dphi[k][1] = T(-1e6 / kLightSpeed) * c.lam_n * dH;
-      dpsi[k][1] = T(-1e6 / kLightSpeed) * c.lam_n * dL;
-      dphi[k][2] = -v / c.p4 * dH;
-      dpsi[k][2] = -v / c.p4 * dL;
-      dphi[k][3] = -dL;
-      dpsi[k][3] = dH;
+      const T dH = T(2) * (-v * hl.h + c.p5 * hl.l) * rsp;
+      const T dL = T(-2) * (-rsp + c.p5 * hl.h + v * hl.l) * rsp;
+      const T fac[3] = {T(q) * c.bsh_n, T(-1e6 / kLightSpeed) * c.lam_n, -v * c.inv_p4};
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const T dp = fac[j] * dH, dq = fac[j] * dL;
+        df1[j] += w1 * dp;
+        dfs[j] += ws * dp;
+        dfd[j] += wd * dp;
+        dg1[j] += w1 * dq;
+        dgs[j] += ws * dq;
+        dgd[j] += wd * dq;
+      }
+      // d/da: dH/da = -dL/dv, dL/da = dH/dv
+      df1[3] -= w1 * dL;
+      dfs[3] -= ws * dL;
+      dfd[3] -= wd * dL;
+      dg1[3] += w1 * dH;
+      dgs[3] += ws * dH;
+      dgd[3] += wd * dH;
     }
   }
-  const T phis = T(0.5) * (phi[0] + phi[2]);
-  const T phit = phi[1] - phis;
-  const T psit = psi[1] - T(0.5) * (psi[0] + psi[2]);
-  T eta[4], rho[4];
-  eta[0] = c.eta_half * (phi[1] * c.sth2 + phis * c.cth2p1);
-  eta[1] = phit * c.kq;
-  eta[2] = phit * c.ku;
-  eta[3] = (phi[0] - phi[2]) * c.kv;
-  rho[1] = psit * c.kq;
-  rho[2] = psit * c.ku;
-  rho[3] = (psi[0] - psi[2]) * c.kv;
-  const T a1 = T(1) + eta[0];
+  const T phit = f1 - fs, psit = g1 - gs;
+  T x[7];  // eta_I, eta_Q, eta_U, eta_V, rho_Q, rho_U, rho_V
+  x[0] = c.eta_half * (f1 * c.sth2 + fs * c.cth2p1);
+  x[1] = phit * c.kq;
+  x[2] = phit * c.ku;
+  x[3] = fd * c.kv;
+  x[4] = psit * c.kq;
+  x[5] = psit * c.ku;
+  x[6] = gd * c.kv;
+  const T a1 = T(1) + x[0];
   const T a1s = a1 * a1;
-  const T e2 = eta[1] * eta[1] + eta[2] * eta[2] + eta[3] * eta[3];
-  const T r2 = rho[1] * rho[1] + rho[2] * rho[2] + rho[3] * rho[3];
-  const T er = eta[1] * rho[1] + eta[2] * rho[2] + eta[3] * rho[3];
+  const T e2 = x[1] * x[1] + x[2] * x[2] + x[3] * x[3];
+  const T r2 = x[4] * x[4] + x[5] * x[5] + x[6] * x[6];
+  const T er = x[1] * x[4] + x[2] * x[5] + x[3] * x[6];
   const T del = a1s * (a1s - e2 + r2) - er * er;
-  const T idel = T(1) / del;
+  const T idel = rcp_t(del);
   const T b1d = c.b1 * idel;
-  const T cc[4] = {T(0), eta[3] * rho[2] - eta[2] * rho[3], eta[1] * rho[3] - eta[3] * rho[1],
-                   eta[2] * rho[1] - eta[1] * rho[2]};
-  // numerators of the Unno-Rachkovsky solution: I ~ a1 (a1^2 + r2), P_s ~ ...
+  // cc_s: (eta x rho) components of the solution
+  const T cc[3] = {x[3] * x[5] - x[2] * x[6], x[1] * x[6] - x[3] * x[4],
+                   x[2] * x[4] - x[1] * x[5]};
   T num[4];
   num[0] = a1 * (a1s + r2);
 #pragma unroll
-  for (int s = 1; s < 4; s++) num[s] = a1s * eta[s] + a1 * cc[s] + rho[s] * er;
+  for (int s = 0; s < 3; s++) num[s + 1] = a1s * x[1 + s] + a1 * cc[s] + x[4 + s] * er;
   syn[0] = c.b0 + b1d * num[0];
 #pragma unroll
   for (int s = 1; s < 4; s++) syn[s] = -b1d * num[s];
   if (!DERIV) return;
 
-  // d eta_s / d p_k and d rho_s / d p_k for k = B, theta, phi, v, width, a, eta0
-  T de[4][7], dr[4][7];
+  // G = dS/dx: dS_I = b1 (dnum0 - R0 dDel) / Del, dS_P = -b1 (dnum_P - R_P dDel) / Del
+  T dDel[7];
+  dDel[0] = T(2) * a1 * (T(2) * a1s - e2 + r2);
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    dDel[1 + s] = T(-2) * (a1s * x[1 + s] + er * x[4 + s]);
+    dDel[4 + s] = T(2) * (a1s * x[4 + s] - er * x[1 + s]);
+  }
+  T G[4][7];
   {
-    // B, v, width, a share the form of eta/rho in phi'/psi'
+    const T R0 = num[0] * idel;
+    const T cI = b1d * sw[0];
+    G[0][0] = cI * (T(3) * a1s + r2 - R0 * dDel[0]);
+#pragma unroll
+    for (int m = 1; m < 4; m++) G[0][m] = cI * (-R0 * dDel[m]);
+#pragma unroll
+    for (int m = 4; m < 7; m++) G[0][m] = cI * (T(2) * a1 * x[m] - R0 * dDel[m]);
+  }
+  // d cc_s / d eta_t and d cc_s / d rho_t (s, t over Q, U, V); cc_Q = eV rU - eU rV, ...
+#pragma unroll
+  for (int s = 0; s < 3; s++) {
+    const T Rs = num[s + 1] * idel;
+    const T cs = -b1d * sw[s + 1];
+    const T es = x[1 + s], rs = x[4 + s];
+    // d num_s / d a1
+    G[s + 1][0] = cs * (T(2) * a1 * es + cc[s] - Rs * dDel[0]);
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      // d cc_s / d eta_t = eps(s, t, u) rho_u, d cc_s / d rho_t = -eps(s, t, u) eta_u
+      T dce = 0, dcr = 0;
+      const int u = 3 - s - t;
+      if (s != t) {
+        const T sgn = ((t - s + 3) % 3 == 1) ? T(-1) : T(1);
+        dce = sgn * x[4 + u];
+        dcr = -sgn * x[1 + u];
+      }
+      const T dne = (s == t ? a1s : T(0)) + a1 * dce + rs * x[4 + t];
+      const T dnr = a1 * dcr + (s == t ? er : T(0)) + rs * x[1 + t];
+      G[s + 1][1 + t] = cs * (dne - Rs * dDel[1 + t]);
+      G[s + 1][4 + t] = cs * (dnr - Rs * dDel[4 + t]);
+    }
+  }
+
+  // dx/dp for p = B, theta, phi, v, width, a, eta0, each scaled by step[p]
+  T dx[7][7];
+  {
     const int slot_k[4] = {0, 3, 4, 5};
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const int k = slot_k[j];
-      const T ps = T(0.5) * (dphi[0][j] + dphi[2][j]);
-      de[0][k] = c.eta_half * (dphi[1][j] * c.sth2 + ps * c.cth2p1);
-      const T t = dphi[1][j] - ps;
-      de[1][k] = t * c.kq;
-      de[2][k] = t * c.ku;
-      de[3][k] = (dphi[0][j] - dphi[2][j]) * c.kv;
-      const T u = dpsi[1][j] - T(0.5) * (dpsi[0][j] + dpsi[2][j]);
-      dr[1][k] = u * c.kq;
-      dr[2][k] = u * c.ku;
-      dr[3][k] = (dpsi[0][j] - dpsi[2][j]) * c.kv;
+      const T st = c.step[k];
+      const T dpt = (df1[j] - dfs[j]) * st, dgt = (dg1[j] - dgs[j]) * st;
+      dx[k][0] = c.eta_half * (df1[j] * c.sth2 + dfs[j] * c.cth2p1) * st;
+      dx[k][1] = dpt * c.kq;
+      dx[k][2] = dpt * c.ku;
+      dx[k][3] = dfd[j] * c.kv * st;
+      dx[k][4] = dgt * c.kq;
+      dx[k][5] = dgt * c.ku;
+      dx[k][6] = dgd[j] * c.kv * st;
+    }
+    const T s1 = c.step[1], s2 = c.step[2], s6 = c.step[6] * c.inv_p6;
+    const T ptk = phit * c.kt * s1, gtk = psit * c.kt * s1;
+    dx[1][0] = ptk;
+    dx[1][1] = ptk * c.c2p;
+    dx[1][2] = ptk * c.s2p;
+    dx[1][3] = -c.eta_half * fd * c.sth * s1;
+    dx[1][4] = gtk * c.c2p;
+    dx[1][5] = gtk * c.s2p;
+    dx[1][6] = -c.eta_half * gd * c.sth * s1;
+    dx[2][0] = 0;
+    dx[2][1] = T(-2) * x[2] * s2;
+    dx[2][2] = T(2) * x[1] * s2;
+    dx[2][3] = 0;
+    dx[2][4] = T(-2) * x[5] * s2;
+    dx[2][5] = T(2) * x[4] * s2;
+    dx[2][6] = 0;
+#pragma unroll
+    for (int m = 0; m < 7; m++) dx[6][m] = x[m] * s6;
+  }
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+      T acc = G[s][0] * dx[k][0];
+#pragma unroll
+      for (int m = 1; m < 7; m++) acc += G[s][m] * dx[k][m];
+      J[s][k] = acc;
     }
   }
-  de[0][1] = phit * c.kt;
-  de[1][1] = de[0][1] * c.c2p;
-  de[2][1] = de[0][1] * c.s2p;
-  de[3][1] = c.eta_half * (phi[0] - phi[2]) * (-c.sth);
-  dr[1][1] = psit * c.kt * c.c2p;
-  dr[2][1] = psit * c.kt * c.s2p;
-  dr[3][1] = c.eta_half * (psi[0] - psi[2]) * (-c.sth);
-  de[0][2] = 0;
-  de[1][2] = T(-2) * eta[2];
-  de[2][2] = T(2) * eta[1];
-  de[3][2] = 0;
-  dr[1][2] = T(-2) * rho[2];
-  dr[2][2] = T(2) * rho[1];
-  dr[3][2] = 0;
-  const T ip6 = T(1) / c.p6;
-  de[0][6] = eta[0] * ip6;
+  // S = S0 + S1 and beta = S0 / S
+  const T t7 = (T(1) - c.p8) * idel * c.step[7];
+  J[0][7] = (c.p8 * c.step[7] + t7 * num[0]) * sw[0];
 #pragma unroll
-  for (int s = 1; s < 4; s++) {
-    de[s][6] = eta[s] * ip6;
-    dr[s][6] = rho[s] * ip6;
-  }
-  const T b1dd = b1d * idel;
+  for (int s = 1; s < 4; s++) J[s][7] = -t7 * num[s] * sw[s];
+  const T t8 = c.p7 * idel * c.step[8];
+  J[0][8] = (c.p7 * c.step[8] - t8 * num[0]) * sw[0];
 #pragma unroll
-  for (int k = 0; k < 7; k++) {
-    const T da1 = de[0][k];
-    const T de2 = T(2) * (eta[1] * de[1][k] + eta[2] * de[2][k] + eta[3] * de[3][k]);
-    const T dr2 = T(2) * (rho[1] * dr[1][k] + rho[2] * dr[2][k] + rho[3] * dr[3][k]);
-    const T der = de[1][k] * rho[1] + eta[1] * dr[1][k] + de[2][k] * rho[2] + eta[2] * dr[2][k] +
-                  de[3][k] * rho[3] + eta[3] * dr[3][k];
-    const T ddel = T(2) * a1 * da1 * (a1s - e2 + r2) + a1s * (T(2) * a1 * da1 - de2 + dr2) -
-                   T(2) * er * der;
-    J[0][k] = b1dd * (del * (da1 * (a1s + r2) + a1 * (T(2) * a1 * da1 + dr2)) - ddel * num[0]) *
-              c.step[k];
-    // d cc_s: cc1 = e3 r2 - e2 r3, cc2 = e1 r3 - e3 r1, cc3 = e2 r1 - e1 r2
-    const T dc1 = de[3][k] * rho[2] + eta[3] * dr[2][k] - de[2][k] * rho[3] - eta[2] * dr[3][k];
-    const T dc2 = de[1][k] * rho[3] + eta[1] * dr[3][k] - de[3][k] * rho[1] - eta[3] * dr[1][k];
-    const T dc3 = de[2][k] * rho[1] + eta[2] * dr[1][k] - de[1][k] * rho[2] - eta[1] * dr[2][k];
-    const T dcc[4] = {T(0), dc1, dc2, dc3};
-#pragma unroll
-    for (int s = 1; s < 4; s++) {
-      J[s][k] = -b1dd *
-                (del * (T(2) * a1 * da1 * eta[s] + a1s * de[s][k] + da1 * cc[s] + a1 * dcc[s] +
-                        dr[s][k] * er + rho[s] * der) -
-                 ddel * num[s]) *
-                c.step[k];
-    }
-  }
-  T t7 = (T(1) - c.p8) * idel;
-  J[0][7] = (c.p8 + t7 * num[0]) * c.step[7];
-#pragma unroll
-  for (int s = 1; s < 4; s++) J[s][7] = (-t7 * num[s]) * c.step[7];
-  T t8 = c.p7 * idel;
-  J[0][8] = (c.p7 - t8 * num[0]) * c.step[8];
-#pragma unroll
-  for (int s = 1; s < 4; s++) J[s][8] = (t8 * num[s]) * c.step[8];
+  for (int s = 1; s < 4; s++) J[s][8] = t8 * num[s] * sw[s];
 }
 
 // ---------------------------------------------------------------------------

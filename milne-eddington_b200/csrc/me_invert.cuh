@@ -30,37 +30,19 @@
 namespace me {
 namespace detail {
 
-template <class T>
-__device__ __forceinline__ void load_voigt(VoigtK<T> &K, const DevPlan &P, T *s_tab) {
-  K.a = T(P.fa);
-  K.aa = T(P.faa);
-  K.log_rmin0 = T(P.flog_rmin0);
-  K.sqrt_log_rmin0 = T(P.fsqrt_log_rmin0);
-  K.nmax = P.fnmax;
-  K.nfig = P.nfigures;
-#pragma unroll
-  for (int i = 0; i < 5; i++) K.thr[i] = T(P.thr[i]);
-  K.ea2n2 = s_tab;
-}
-
-template <class T>
-__device__ __forceinline__ void fill_table(const DevPlan &P, T *s_tab) {
-  for (int i = threadIdx.x; i < 50; i += blockDim.x) s_tab[i] = T(P.exp_a2n2[i]);
-  __syncthreads();
-}
-
 // Synthesis with Jacobian fused with the weighted normal equations.
 // sw[s] = weight_s / sqrt(norm0): sum (J sw)(J sw) = J^T W J with
 // W = weight^2 / norm0 (Noise_Init, Src/ME_SOLVER.c:410-441).  H45 = upper
 // triangle of the full 9x9 (row-major, i <= j), g9 = -J^T W r; returns
 // sum (r sw)^2 / (4 nl) accumulated in FP64.
 template <class T>
-__device__ __forceinline__ double deriv_pass(const DevPlan &P, const VoigtK<T> &K,
+__device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                              const double *par, const double *step,
                                              const double *prof, const double sw[4], double *H45,
                                              double *g9) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
+  voigt_prepare<T>(K, c.p5, rden, blockDim.x);
   T h[45], g[9];
 #pragma unroll
   for (int i = 0; i < 45; i++) h[i] = T(0);
@@ -72,15 +54,13 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, const VoigtK<T> &
 #pragma unroll 1
   for (int iw = 0; iw < nl; iw++) {
     T syn[4], J[4][9];
-    me_point<T, true>(c, shift_w<T>(c, P, iw), K, syn, J);
+    me_point<T, true>(c, shift_w<T>(c, P, iw), K, tsw, syn, J);
     T r[4];
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
       chi += rd * rd;
       r[s] = T(rd);
-#pragma unroll
-      for (int k = 0; k < 9; k++) J[s][k] *= tsw[s];
     }
     int idx = 0;
 #pragma unroll
@@ -103,18 +83,20 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, const VoigtK<T> &
 // Forward synthesis + chi^2 (Trial_Synthesis's synthesis and Loss_Function);
 // residuals and their squares in FP64.  fit (nullable) receives the profile.
 template <class T>
-__device__ __noinline__ double forward_pass(const DevPlan &P, const VoigtK<T> &K,
+__device__ __noinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                             const double *par, const double *step,
                                             const double *prof, const double sw[4],
                                             double *fit) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
+  voigt_prepare<T>(K, c.p5, rden, blockDim.x);
+  const T ones[4] = {T(1), T(1), T(1), T(1)};
   double chi = 0.0;
   const int nl = P.nl;
 #pragma unroll 1
   for (int iw = 0; iw < nl; iw++) {
     T syn[4];
-    me_point<T, false>(c, shift_w<T>(c, P, iw), K, syn, nullptr);
+    me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       if (prof) {
@@ -207,12 +189,14 @@ using namespace detail;
 // Synthesis with Jacobian + normal equations for the slots of jlist[parity].
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(kBlock) jac_kernel(const DevPlan P, InvertArgs A, Slots S,
-                                                     int parity) {
-  __shared__ T s_tab[50];
-  fill_table<T>(P, s_tab);
+__global__ void __launch_bounds__(kBlock) jac_kernel(const __grid_constant__ DevPlan P,
+                                                     const __grid_constant__ InvertArgs A,
+                                                     const __grid_constant__ Slots S, int parity) {
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * kBlock];
   VoigtK<T> K;
-  load_voigt<T>(K, P, s_tab);
+  voigt_block_setup<T>(K, P, s_tab);
+  T *rden = s_rden + threadIdx.x;
   if (blockIdx.x == 0 && threadIdx.x == 0) S.jcount[parity ^ 1] = 0;
   const int count = S.jcount[parity];
   const int W = S.W;
@@ -232,7 +216,7 @@ __global__ void __launch_bounds__(kBlock) jac_kernel(const DevPlan P, InvertArgs
 #pragma unroll
     for (int k = 0; k < 4; k++) sw[k] = P.weights[k] * isn;
     double H45[45], g9[9];
-    const double chi0 = deriv_pass<T>(P, K, par, step, pp, sw, H45, g9);
+    const double chi0 = deriv_pass<T>(P, K, rden, par, step, pp, sw, H45, g9);
     t_jac++;
     double ratio = S.sc[SC_RATIO * W + s];
     if (S.state[s] == SL_JAC_START) {  // LM_FIT set-up (Src/LM_FIT.c:549-566)
@@ -290,7 +274,9 @@ __global__ void __launch_bounds__(kBlock) jac_kernel(const DevPlan P, InvertArgs
 // i.e. only when the iteration really goes on.  Each thread keeps its matrix
 // in its own column of shared memory.
 // ---------------------------------------------------------------------------
-static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const DevPlan P, InvertArgs A, Slots S) {
+static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_constant__ DevPlan P,
+                                                               const __grid_constant__ InvertArgs A,
+                                                               const __grid_constant__ Slots S) {
   extern __shared__ double sm[];
   const int t = threadIdx.x;
   double *a = sm + t;
@@ -368,12 +354,15 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const DevPlan P, 
 // One trial step for every slot; run and pixel transitions; refills.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(kBlock) trial_kernel(const DevPlan P, InvertArgs A, Slots S,
+__global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ DevPlan P,
+                                                       const __grid_constant__ InvertArgs A,
+                                                       const __grid_constant__ Slots S,
                                                        int parity) {
-  __shared__ T s_tab[50];
-  fill_table<T>(P, s_tab);
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * kBlock];
   VoigtK<T> K;
-  load_voigt<T>(K, P, s_tab);
+  voigt_block_setup<T>(K, P, s_tab);
+  T *rden = s_rden + threadIdx.x;
   const int W = S.W;
   const int n = P.npar;
   const int nl = P.nl;
@@ -415,7 +404,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const DevPlan P, InvertAr
       // --------- Trial_Synthesis (Src/LM_FIT.c:473-527), after svd_kernel ---------
       double ptmp[9];
       load9(S.ptmp, W, s, ptmp);
-      const double chi_new = forward_pass<T>(P, K, ptmp, step, pp, sw, nullptr);
+      const double chi_new = forward_pass<T>(P, K, rden, ptmp, step, pp, sw, nullptr);
       lmchisq = chi_new;
       S.had_trial[s] = 1;
       S.cnt[2 * W + s]++;
@@ -502,7 +491,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const DevPlan P, InvertAr
       } else {
         // pixel done: best-fit profile, theta fold, HMI_REF, result
         // (Src/LM_FIT.c:727-733, 791-799)
-        if (A.fit) forward_pass<T>(P, K, pbest, step, nullptr, sw, A.fit + (size_t)pix * 4 * nl);
+        if (A.fit) forward_pass<T>(P, K, rden, pbest, step, nullptr, sw, A.fit + (size_t)pix * 4 * nl);
         if (pbest[1] > kPi) pbest[1] -= kPi;
         if (P.hmi_ref) {
           pbest[2] += 0.5 * kPi;

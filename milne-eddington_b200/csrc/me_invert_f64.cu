@@ -3,8 +3,12 @@
 
 namespace me {
 
-template __global__ void jac_kernel<double>(const DevPlan P, InvertArgs A, Slots S, int parity);
-template __global__ void trial_kernel<double>(const DevPlan P, InvertArgs A, Slots S, int parity);
+template __global__ void jac_kernel<double>(const __grid_constant__ DevPlan P,
+                                            const __grid_constant__ InvertArgs A,
+                                            const __grid_constant__ Slots S, int parity);
+template __global__ void trial_kernel<double>(const __grid_constant__ DevPlan P,
+                                              const __grid_constant__ InvertArgs A,
+                                              const __grid_constant__ Slots S, int parity);
 
 // which: 0 = jac_kernel, 1 = trial_kernel, 2 = svd_kernel (CTAs for a full device)
 int round_grid_f64(int which, int device) {

@@ -10,25 +10,6 @@ namespace me {
 
 namespace {
 
-template <class T>
-__device__ __forceinline__ void load_voigt(VoigtK<T> &K, const DevPlan &P, T *s_tab) {
-  K.a = T(P.fa);
-  K.aa = T(P.faa);
-  K.log_rmin0 = T(P.flog_rmin0);
-  K.sqrt_log_rmin0 = T(P.fsqrt_log_rmin0);
-  K.nmax = P.fnmax;
-  K.nfig = P.nfigures;
-#pragma unroll
-  for (int i = 0; i < 5; i++) K.thr[i] = T(P.thr[i]);
-  K.ea2n2 = s_tab;
-}
-
-template <class T>
-__device__ __forceinline__ void fill_table(const DevPlan &P, T *s_tab) {
-  for (int i = threadIdx.x; i < 50; i += blockDim.x) s_tab[i] = T(P.exp_a2n2[i]);
-  __syncthreads();
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -38,10 +19,10 @@ __device__ __forceinline__ void fill_table(const DevPlan &P, T *s_tab) {
 template <class T>
 __global__ void synth_kernel(const DevPlan P, const double *par, long long npix, double step7,
                              double *prof, double *jac) {
-  __shared__ T s_tab[50];
-  fill_table<T>(P, s_tab);
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * 128];
   VoigtK<T> K;
-  load_voigt<T>(K, P, s_tab);
+  voigt_block_setup<T>(K, P, s_tab);
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= npix) return;
   const int nl = P.nl;
@@ -54,15 +35,17 @@ __global__ void synth_kernel(const DevPlan P, const double *par, long long npix,
   for (int k = 0; k < 9; k++) mp[k] = par[i * 9 + k];
   SynthCall<T> c;
   synth_setup<T>(c, mp, P, step);
+  voigt_prepare<T>(K, c.p5, s_rden + threadIdx.x, blockDim.x);
+  const T ones[4] = {T(1), T(1), T(1), T(1)};
   for (int iw = 0; iw < nl; iw++) {
     T syn[4], J[4][9];
     const T w0 = shift_w<T>(c, P, iw);
     if (jac) {
-      me_point<T, true>(c, w0, K, syn, J);
+      me_point<T, true>(c, w0, K, ones, syn, J);
       for (int s = 0; s < 4; s++)
         for (int k = 0; k < 9; k++) jac[((size_t)i * 36 + s * 9 + k) * nl + iw] = (double)J[s][k];
     } else {
-      me_point<T, false>(c, w0, K, syn, J);
+      me_point<T, false>(c, w0, K, ones, syn, J);
     }
     for (int s = 0; s < 4; s++) prof[((size_t)i * 4 + s) * nl + iw] = (double)syn[s];
   }
@@ -71,13 +54,14 @@ __global__ void synth_kernel(const DevPlan P, const double *par, long long npix,
 template <class T>
 __global__ void voigt_kernel(const DevPlan P, const double *nu, const double *a, long long n,
                              double *H, double *L) {
-  __shared__ T s_tab[50];
-  fill_table<T>(P, s_tab);
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * 256];
   VoigtK<T> K;
-  load_voigt<T>(K, P, s_tab);
+  voigt_block_setup<T>(K, P, s_tab);
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const T y = T(a[i]);
+  voigt_prepare<T>(K, y, s_rden + threadIdx.x, blockDim.x);
   const HL<T> r = voigt<T>(T(nu[i]), y, erfcx_t<T>(y), K);
   H[i] = (double)r.h;
   L[i] = (double)r.l;
