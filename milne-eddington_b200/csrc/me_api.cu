@@ -98,7 +98,7 @@ struct me_plan {
   double carry = 0.0;  // LM->chisq carried between pixels (STRUCT_LM LM = {0})
   DevBuf d_lambda, d_dlambda;
   DevBuf d_prof, d_res, d_fit;  // staging of the host entry point
-  DevBuf d_flags, d_pen0, d_lastchi, d_counters, d_totals, d_next, d_stale, d_list;
+  DevBuf d_flags, d_pen0, d_lastchi, d_counters, d_totals, d_next, d_stale, d_list, d_fitpar;
   // slots of the pixels in flight (struct me::Slots), sized for `window`
   int window = 0;          // requested slot count (0 = default)
   int slots_w = 0;         // allocated slot count
@@ -281,7 +281,7 @@ extern "C" void me_plan_destroy(me_plan *p) {
                     &p->d_counters, &p->d_totals, &p->d_next,    &p->d_stale,
                     &p->d_list,   &p->d_slot_pix, &p->d_slot_i32, &p->d_slot_cnt,
                     &p->d_slot_u8, &p->d_slot_sc, &p->d_slot_vec, &p->d_slot_hess,
-                    &p->d_slot_list, &p->d_slot_small};
+                    &p->d_slot_list, &p->d_slot_small, &p->d_fitpar};
   for (DevBuf *b : bufs) b->release();
   if (p->h_poll) cudaFreeHost(p->h_poll);
   if (p->ev0) cudaEventDestroy(p->ev0);
@@ -324,8 +324,8 @@ int ensure_slots(me_plan *p, int W, me::Slots &S) {
     CK(p->d_slot_sc.ensure((size_t)me::SC_COUNT * w * sizeof(double)));
     CK(p->d_slot_vec.ensure(5 * 9 * w * sizeof(double)));
     CK(p->d_slot_hess.ensure(81 * w * sizeof(double)));
-    CK(p->d_slot_list.ensure(2 * w * sizeof(int)));
-    CK(p->d_slot_small.ensure(4 * sizeof(int)));
+    CK(p->d_slot_list.ensure(4 * w * sizeof(int)));
+    CK(p->d_slot_small.ensure(8 * sizeof(int)));
     p->slots_w = W;
   }
   const size_t w = (size_t)W;
@@ -347,9 +347,11 @@ int ensure_slots(me_plan *p, int W, me::Slots &S) {
   S.ptmp = v + 36 * w;
   S.hess = p->d_slot_hess.as<double>();
   S.jlist = p->d_slot_list.as<int>();
+  S.rlist = S.jlist + 2 * w;
   int *small = p->d_slot_small.as<int>();
   S.jcount = small;
-  S.busy = small + 2;
+  S.rcount = small + 2;
+  S.busy = small + 4;
   return ME_OK;
 }
 
@@ -363,7 +365,7 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
   int rc = ensure_slots(p, W, S);
   if (rc) return rc;
   CK(cudaMemsetAsync(S.state, 0, (size_t)W * sizeof(int), st));  // SL_EMPTY
-  CK(cudaMemsetAsync(S.jcount, 0, 4 * sizeof(int), st));           // jcount[2], busy
+  CK(cudaMemsetAsync(S.jcount, 0, 5 * sizeof(int), st));           // jcount[2], rcount[2], busy
   CK(cudaMemsetAsync(A.next, 0, sizeof(unsigned long long), st));
   int grids[3];
   grids[0] = std::min(p->grid_jac, (W + me::kBlock - 1) / me::kBlock);
@@ -407,6 +409,10 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   A.prof = d_prof;
   A.res = d_res;
   A.fit = d_fit;
+  if (d_fit) {
+    CK(p->d_fitpar.ensure(n * 9 * sizeof(double)));
+    A.fitpar = p->d_fitpar.as<double>();
+  }
   A.flags = p->d_flags.as<unsigned char>();
   A.penalty0 = p->d_pen0.as<double>();
   A.lastchi = p->d_lastchi.as<double>();
@@ -492,6 +498,8 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     cudaEventElapsedTime(&ms, p->ev0, p->ev1);
     kernel_ms += ms;
   }
+  if (d_fit)
+    CK(me::launch_fit(p->precision, p->P, A.fitpar, A.flags, npix, d_fit, st));
   p->rounds_last = rounds_total;
   if (stats) {
     unsigned long long tot[8];
@@ -506,7 +514,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     stats->jacobians = (long long)tot[5];
     stats->wavelengths = (long long)(tot[3] + tot[5]) * p->P.nl;
     stats->redo_pixels = redo_total;
-    stats->launches = 3 * rounds_total;
+    stats->launches = 4 * rounds_total + (d_fit ? 1 : 0);
     stats->rounds = rounds_total;
     stats->kernel_ms = kernel_ms;
   }

@@ -83,7 +83,7 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *
 // Forward synthesis + chi^2 (Trial_Synthesis's synthesis and Loss_Function);
 // residuals and their squares in FP64.  fit (nullable) receives the profile.
 template <class T>
-__device__ __noinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
+__device__ __forceinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                             const double *par, const double *step,
                                             const double *prof, const double sw[4],
                                             double *fit) {
@@ -124,7 +124,15 @@ __device__ __forceinline__ void append_jac(const Slots &S, int parity_next, int 
   const int k = atomicAdd(S.jcount + parity_next, 1);
   S.jlist[parity_next * S.W + k] = s;
 }
+__device__ __forceinline__ void append_rej(const Slots &S, int parity_next, int s) {
+  const int k = atomicAdd(S.rcount + parity_next, 1);
+  S.rlist[parity_next * S.W + k] = s;
+}
 
+__device__ __forceinline__ void store9_px(double *a, long long pix, const double *v) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) a[(size_t)pix * 9 + i] = v[i];
+}
 __device__ __forceinline__ void load9(const double *a, int W, int s, double *v) {
 #pragma unroll
   for (int i = 0; i < 9; i++) v[i] = a[(size_t)i * W + s];
@@ -189,7 +197,7 @@ using namespace detail;
 // Synthesis with Jacobian + normal equations for the slots of jlist[parity].
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void __launch_bounds__(kBlock) jac_kernel(const __grid_constant__ DevPlan P,
+__global__ void __launch_bounds__(kBlock, ME_JAC_MINB) jac_kernel(const __grid_constant__ DevPlan P,
                                                      const __grid_constant__ InvertArgs A,
                                                      const __grid_constant__ Slots S, int parity) {
   __shared__ T s_tab[100];
@@ -197,7 +205,10 @@ __global__ void __launch_bounds__(kBlock) jac_kernel(const __grid_constant__ Dev
   VoigtK<T> K;
   voigt_block_setup<T>(K, P, s_tab);
   T *rden = s_rden + threadIdx.x;
-  if (blockIdx.x == 0 && threadIdx.x == 0) S.jcount[parity ^ 1] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S.jcount[parity ^ 1] = 0;
+    S.rcount[parity ^ 1] = 0;
+  }
   const int count = S.jcount[parity];
   const int W = S.W;
   const int n = P.npar;
@@ -257,7 +268,7 @@ __global__ void __launch_bounds__(kBlock) jac_kernel(const __grid_constant__ Dev
 }
 
 // ---------------------------------------------------------------------------
-// The SVD solve of every slot's trial step (SVD_solve_mem, Src/LM_FIT.c:400-469)
+// The SVD solve of the slots' trial steps (SVD_solve_mem, Src/LM_FIT.c:400-469)
 // and its trial parameters (Par_update + bounds_check, Src/LM_FIT.c:511-516).
 //
 // The reference decomposes, at the first trial of an LM iteration, the
@@ -276,7 +287,8 @@ __global__ void __launch_bounds__(kBlock) jac_kernel(const __grid_constant__ Dev
 // ---------------------------------------------------------------------------
 static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_constant__ DevPlan P,
                                                                const __grid_constant__ InvertArgs A,
-                                                               const __grid_constant__ Slots S) {
+                                                               const __grid_constant__ Slots S,
+                                                               int parity, int which) {
   extern __shared__ double sm[];
   const int t = threadIdx.x;
   double *a = sm + t;
@@ -285,7 +297,14 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_cons
   const int W = S.W;
   const int n = P.npar;
   unsigned long long t_svdlim = 0;
-  for (int s = blockIdx.x * kSvdBlock + t; s < W; s += gridDim.x * kSvdBlock) {
+  // which = 0: the slots that just built their normal matrix (the Jacobian
+  // list of this round, first trials); which = 1: the slots going on after a
+  // rejected trial.  Two launches keep the costly decompositions of H apart
+  // from the cheap ones of orthogonal factors.
+  const int *list = which == 0 ? S.jlist + parity * W : S.rlist + parity * W;
+  const int count = which == 0 ? S.jcount[parity] : S.rcount[parity];
+  for (int i = blockIdx.x * kSvdBlock + t; i < count; i += gridDim.x * kSvdBlock) {
+    const int s = list[i];
     if (S.state[s] != SL_TRIAL) continue;
     const int tk = S.tk[s];
     double g[9], x[9];
@@ -434,6 +453,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
           end_run = true;
         } else {  // another trial, on the SVD's U factor (svd_kernel)
           S.tk[s]++;
+          append_rej(S, next_parity, s);
         }
       }
       sc[SC_CHISQ * W + s] = chisq;
@@ -491,7 +511,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
       } else {
         // pixel done: best-fit profile, theta fold, HMI_REF, result
         // (Src/LM_FIT.c:727-733, 791-799)
-        if (A.fit) forward_pass<T>(P, K, rden, pbest, step, nullptr, sw, A.fit + (size_t)pix * 4 * nl);
+        if (A.fitpar) store9_px(A.fitpar, pix, pbest);  // profiles: launch_fit after the batch
         if (pbest[1] > kPi) pbest[1] -= kPi;
         if (P.hmi_ref) {
           pbest[2] += 0.5 * kPi;

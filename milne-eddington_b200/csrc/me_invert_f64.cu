@@ -29,7 +29,8 @@ int round_grid_f64(int which, int device) {
 cudaError_t launch_round_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
                            const int grids[3], cudaStream_t st) {
   jac_kernel<double><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
-  svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S);
+  svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, 0);
+  svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, 1);
   trial_kernel<double><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
   return cudaGetLastError();
 }

@@ -10,6 +10,10 @@
 namespace me {
 
 constexpr int kBlock = 128;
+// minimum resident CTAs per SM jac_kernel is compiled for (its register cap)
+#ifndef ME_JAC_MINB
+#define ME_JAC_MINB 2
+#endif
 constexpr int kSvdBlock = 64;  // threads of svd_kernel; each holds its matrix in shared memory
 constexpr int kSvdSmem = (81 + 18) * kSvdBlock * 8;
 
@@ -52,6 +56,8 @@ struct Slots {
   int *tk;                   // [W]: index of the trial step within the LM iteration (1 = first)
   int *jlist;                // [2][W] slots needing a synthesis with Jacobian
   int *jcount;               // [2]
+  int *rlist;                // [2][W] slots going on to another trial after a rejected one
+  int *rcount;               // [2]
   int *busy;                 // slots holding a pixel
 };
 
@@ -60,6 +66,7 @@ struct InvertArgs {
   const double *prof;          // [npix][4][nl]
   double *res;                 // [npix][10]
   double *fit;                 // [npix][4][nl] or null
+  double *fitpar;              // [npix][9] best parameters before the post-folds (with fit)
   unsigned char *flags;        // [npix] bit0 inverted, bit1 made a trial step
   double *penalty0;            // [npix] regularisation penalty at the first guess
   double *lastchi;             // [npix] chi^2 of the pixel's last trial step
@@ -83,6 +90,11 @@ int record_error(int code, const char *msg);
 int round_grid(int precision, int which, int device);
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                          int parity, const int grids[3], cudaStream_t st);
+// Best-fit profiles after a batch: synthesis at fitpar for the inverted
+// pixels (flags bit 0), zeros for the skipped ones.
+cudaError_t launch_fit(int precision, const DevPlan &P, const double *d_fitpar,
+                       const unsigned char *d_flags, long long npix, double *d_fit,
+                       cudaStream_t st);
 cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,
                          double step7, double *d_prof, double *d_jac, cudaStream_t st);
 cudaError_t launch_voigt(int precision, const DevPlan &P, const double *d_nu, const double *d_a,

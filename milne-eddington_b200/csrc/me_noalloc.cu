@@ -42,8 +42,8 @@ constexpr size_t kOffU8 = align256(kOffCnt + 16 * (size_t)kSlots);          // [
 constexpr size_t kOffSc = align256(kOffU8 + (size_t)kSlots);                // [SC][W] double
 constexpr size_t kOffVec = align256(kOffSc + 8 * me::SC_COUNT * (size_t)kSlots);  // [45][W]
 constexpr size_t kOffHess = align256(kOffVec + 8 * 45 * (size_t)kSlots);    // [81][W] double
-constexpr size_t kOffList = align256(kOffHess + 8 * 81 * (size_t)kSlots);   // [2][W] int
-constexpr size_t kOffFlags = align256(kOffList + 8 * (size_t)kSlots);       // [P] uchar
+constexpr size_t kOffList = align256(kOffHess + 8 * 81 * (size_t)kSlots);   // [4][W] int
+constexpr size_t kOffFlags = align256(kOffList + 16 * (size_t)kSlots);      // [P] uchar
 constexpr size_t kOffPen0 = align256(kOffFlags + (size_t)kMaxPix);          // [P] double
 constexpr size_t kOffLast = align256(kOffPen0 + 8 * (size_t)kMaxPix);       // [P] double
 constexpr size_t kOffCount = align256(kOffLast + 8 * (size_t)kMaxPix);      // [P][4] uint
@@ -56,10 +56,11 @@ constexpr size_t kScratchBytes = align256(kOffRedo + 8 * (size_t)kMaxPix);
 // names it directly.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-// Small-counter block (kOffSmall): jcount[2], busy, pad, next, totals[8],
-// redo count, carry out.
+// Small-counter block (kOffSmall): jcount[2], rcount[2], busy, pad, next,
+// totals[8], redo count, carry out.
 struct Small {
   int jcount[2];
+  int rcount[2];
   int busy;
   int pad;
   unsigned long long next;
@@ -145,7 +146,7 @@ int setup(int prec, DeviceSetup **out) {
 int run_rounds(int prec, const me::DevPlan &P, const me::InvertArgs &A, const me::Slots &S,
                const int grids[3], cudaStream_t st, Small *d_small) {
   NA_CK(cudaMemsetAsync(S.state, 0, sizeof(int) * (size_t)S.W, st));  // SL_EMPTY
-  NA_CK(cudaMemsetAsync(d_small, 0, offsetof(Small, totals), st));   // jcount, busy, next
+  NA_CK(cudaMemsetAsync(d_small, 0, offsetof(Small, totals), st));  // lists, busy, next
   int parity = 0;
   while (true) {
     for (int r = 0; r < 8; r++) {
@@ -213,7 +214,9 @@ extern "C" int me_invert_batch_device_noalloc(const me_config *cfg, const double
   S.ptmp = v + 36 * w;
   S.hess = reinterpret_cast<double *>(base + kOffHess);
   S.jlist = reinterpret_cast<int *>(base + kOffList);
+  S.rlist = S.jlist + 2 * w;
   S.jcount = d_small->jcount;
+  S.rcount = d_small->rcount;
   S.busy = &d_small->busy;
   // (the kernels index the [k][W] arrays with the active slot count W as
   // their stride; with W < kSlots each region is used densely from its start)

@@ -52,6 +52,35 @@ __global__ void synth_kernel(const DevPlan P, const double *par, long long npix,
 }
 
 template <class T>
+__global__ void fit_kernel(const DevPlan P, const double *fitpar, const unsigned char *flags,
+                           long long npix, double *fit) {
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * 128];
+  VoigtK<T> K;
+  voigt_block_setup<T>(K, P, s_tab);
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= npix) return;
+  const int nl = P.nl;
+  double *out = fit + (size_t)i * 4 * nl;
+  if (!(flags[i] & 1)) {
+    for (int k = 0; k < 4 * nl; k++) out[k] = 0.0;
+    return;
+  }
+  double mp[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) mp[k] = fitpar[i * 9 + k];
+  SynthCall<T> c;
+  synth_setup<T>(c, mp, P, P.step);
+  voigt_prepare<T>(K, c.p5, s_rden + threadIdx.x, blockDim.x);
+  const T ones[4] = {T(1), T(1), T(1), T(1)};
+  for (int iw = 0; iw < nl; iw++) {
+    T syn[4];
+    me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
+    for (int s = 0; s < 4; s++) out[s * nl + iw] = (double)syn[s];
+  }
+}
+
+template <class T>
 __global__ void voigt_kernel(const DevPlan P, const double *nu, const double *a, long long n,
                              double *H, double *L) {
   __shared__ T s_tab[100];
@@ -127,6 +156,19 @@ cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, l
     synth_kernel<double><<<g, b, 0, st>>>(P, d_par, npix, step7, d_prof, d_jac);
   else
     synth_kernel<float><<<g, b, 0, st>>>(P, d_par, npix, step7, d_prof, d_jac);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fit(int precision, const DevPlan &P, const double *d_fitpar,
+                       const unsigned char *d_flags, long long npix, double *d_fit,
+                       cudaStream_t st) {
+  const int b = 128;
+  const unsigned g = (unsigned)((npix + b - 1) / b);
+  if (g == 0) return cudaSuccess;
+  if (precision == 1)
+    fit_kernel<double><<<g, b, 0, st>>>(P, d_fitpar, d_flags, npix, d_fit);
+  else
+    fit_kernel<float><<<g, b, 0, st>>>(P, d_fitpar, d_flags, npix, d_fit);
   return cudaGetLastError();
 }
 
