@@ -1,18 +1,32 @@
 #!/usr/bin/env python
 """Benchmark of the B200 Milne-Eddington inversion (one JSON line on stdout).
 
-Metric: converged pixels/s on B200 -- pixels inverted per second, counted as
-converged when their chi^2 is <= 1.05 x the chi^2 the reference's FP64 C code
-reaches on the same profile.  The converged share is measured on a seeded
-sample of the map against the reference core (oracle/_ref, the reference's own
-C sources compiled here; the oracle restatement where it was not built).
+Metric: converged pixels/s on one B200 -- pixels inverted per second, counted
+as converged when their chi^2 is <= 1.05 x the chi^2 the reference's FP64 C
+code reaches on the same profile -- with the learned initialiser, beside the
+plain LM with the reference's random restarts on the same map and GPU.  The
+converged share is measured on a seeded sample of the map against the
+reference core (oracle/_ref, the reference's own C sources compiled here; the
+oracle restatement where it was not built).
 
-A step is one inversion of the whole synthetic map (default: the 1024x1024
-Fe I 15648.5 A map, num_run = 5, chisq_criteria = 1.5, FP32 synthesis with FP64
-SVD solve and chi^2 test).  The map (2 GB of FP64 profiles, larger than L2) is
-resident in HBM when the timed region starts; `e2e` times the same step
-through the host entry point me_invert_batch with the profiles in pinned host
-memory (host->device copy, inversion, device->host copy of the results).
+Workload (default): the 1024x1024 Fe I 15648.5 A map (nl = 60, seeded draws of
+B, theta, phi, v, Doppler width, damping, eta0, beta; S = 1; noise 1e-3),
+num_run = 5, chisq_criteria = 1.5, FP32 synthesis with FP64 SVD solve and
+chi^2 test, with Bounds_Dopp = 100, 400 mA and Bounds_Damp = 0.05, 1.0: the
+default Doppler bounds (10-80 mA) cannot reach the drawn widths (150-350 mA),
+so with them no start can fit and chisq_criteria is met by a sixth of the
+pixels at best (`--bounds literal` runs that variant).
+
+The initialiser is trained once per line and grid before the timed region
+(4M profiles synthesised on the GPU from seeded draws of the same
+distributions, other seeds than the map's, 20 epochs of Adam, lr 1e-3, batch
+4096); its training time is reported, its inference is inside every step.
+
+A step is one inversion of the whole map.  The map (2 GB of FP64 profiles,
+larger than L2) is resident in HBM when the timed region starts; `e2e` times
+the same step through the host entry point me_invert_batch with the profiles
+in pinned host memory (host->device copy, inference, inversion, device->host
+copy of the results).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     torchrun --nproc-per-node N bench.py --gpus N ...   (one rank per GPU)
@@ -51,18 +65,18 @@ UNIT = "pixels/s"
 _W = {}
 
 
-def _cpu_worker_init(kind, workload, npix_max, seed, extra):
+def _cpu_worker_init(kind, workload, npix_max, seed, widen):
     sys.path[:0] = [os.path.join(ROOT, "tests"), PKG]
     import oracle_bind as ob
     import me_b200
     lam = me_maps.wavelengths(workload)
     _W["kind"] = kind
     if kind == "reference":
-        _W["eng"] = ob.Reference(me_maps.reference_control_text(workload, extra=extra), lam,
-                                 npix_max, seed=seed)
+        _W["eng"] = ob.Reference(me_maps.reference_control_text(workload, widen_bounds=widen),
+                                 lam, npix_max, seed=seed)
     else:
         cfg = me_b200.parse_config_text(me_maps.control_text(workload, precision="FP64",
-                                                             extra=extra))
+                                                             widen_bounds=widen))
         _W["eng"] = ob.Oracle(cfg, lam)
 
 
@@ -79,16 +93,16 @@ def cpu_kind():
         else "port"
 
 
-def cpu_invert(prof, workload, procs, extra=None):
+def cpu_invert(prof, workload, procs, widen):
     """Inverts prof [n][4][nl] with `procs` processes of the reference core;
-    returns (results, seconds)."""
+    returns (results, seconds, kind)."""
     kind = cpu_kind()
     n = prof.shape[0]
     procs = max(1, min(procs, n))
     chunks = np.array_split(np.arange(n), procs)
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs, initializer=_cpu_worker_init,
-                  initargs=(kind, workload, max(len(c) for c in chunks), 4242, extra or {})) as pool:
+                  initargs=(kind, workload, max(len(c) for c in chunks), 4242, widen)) as pool:
         pool.map(_cpu_worker_invert, [prof[c[:1]] for c in chunks])  # warm every worker
         t0 = time.perf_counter()
         parts = pool.map(_cpu_worker_invert, [prof[c] for c in chunks])
@@ -173,11 +187,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="fe15648_1024x1024", choices=list(me_maps.WORKLOADS))
+    ap.add_argument("--bounds", default="widened", choices=["widened", "literal"])
     ap.add_argument("--npix", type=int, default=0, help="override the map size (testing)")
     ap.add_argument("--precision", default="FP32", choices=["FP32", "FP64"])
-    ap.add_argument("--sample", type=int, default=2048,
+    ap.add_argument("--sample", type=int, default=4096,
                     help="pixels of the CPU sample (reference timing + converged share)")
-    ap.add_argument("--cpu-sample", type=int, default=0, help="override --sample")
+    ap.add_argument("--train-samples", type=int, default=4 << 20)
+    ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--plain-steps", type=int, default=-1, help="timed plain-LM steps (-1: K)")
     ap.add_argument("--e2e-steps", type=int, default=1)
     return ap.parse_args()
 
@@ -188,6 +205,7 @@ def reference_arm(args):
     if rank != 0:
         return 0
     w = me_maps.WORKLOADS[args.workload]
+    widen = args.bounds == "widened"
     cores = host_cores()
     # ~7 ms of one core per pixel at num_run = 5: a step of ~2 s on all cores
     npix = args.npix or max(cores * 48, 256)
@@ -195,7 +213,7 @@ def reference_arm(args):
     times = []
     kind = None
     for i in range(args.warmup + args.steps):
-        _, dt, kind = cpu_invert(prof, args.workload, cores)
+        _, dt, kind = cpu_invert(prof, args.workload, cores, widen)
         if i >= args.warmup:
             times.append(dt)
     step = max(times)
@@ -204,8 +222,10 @@ def reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded draws of the workload's parameter distributions)",
-            "config": {"workload": args.workload, "pixels_per_step": npix,
+            "config": {"workload": args.workload, "bounds": args.bounds,
+                       "pixels_per_step": npix,
                        "num_run": int(w["ctl"].get("num_run", 4)), "nl": w["nl"],
+                       "init": "Init_Guess + random restarts (the reference's algorithm)",
                        "cpu_processes": cores},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": f"{npix} pixels of {args.workload} per step, "
@@ -214,6 +234,67 @@ def reference_arm(args):
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def roofline_flops(stats, fc, nl):
+    """Algorithmic FLOPs of the LM work a batch did (reference algorithm,
+    counted per event with a counting scalar type: tests/golden/flop_counts.json)."""
+    def flops(c):
+        return c.get("add", 0) + c.get("mul", 0) + c.get("div", 0) + c.get("sqrt", 0)
+
+    first = stats["iterations"]
+    later = stats["trials"] - first
+    return (stats["trials"] * nl * (flops(fc["forward_per_lambda"]) + flops(fc["loss_per_lambda"]))
+            + first * flops(fc["svd_solve_normal_matrix"])
+            + later * flops(fc["svd_solve_orthogonal"])
+            + stats["jacobians"] * nl * (flops(fc["jacobian_per_lambda"])
+                                         + flops(fc["normal_equations_per_lambda"])))
+
+
+def param_errors(res, ref):
+    """Median and 99th percentile |res - ref| per parameter in G, deg, deg,
+    m/s, mA, -, -, -, - (S, beta in continuum units)."""
+    names = ["B_G", "theta_deg", "phi_deg", "v_m_s", "doppler_mA", "damping", "eta0", "S",
+             "beta"]
+    scale = [1.0, 180 / np.pi, 180 / np.pi, 1e3, 1.0, 1.0, 1.0, 1.0, 1.0]
+    d = np.abs(res[:, :9] - ref[:, :9])
+    d[:, 2] = np.minimum(d[:, 2], np.pi - d[:, 2])  # azimuth is folded into [0, pi)
+    return {n: [float(np.median(d[:, k]) * sc), float(np.quantile(d[:, k], 0.99) * sc)]
+            for k, (n, sc) in enumerate(zip(names, scale))}
+
+
+def timed_steps(torch, step, n, stream, dist, clk=None):
+    """Runs n steps between a barrier + synchronize on both sides; returns
+    (seconds, per-step stats), max over ranks."""
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stats = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx = clk if clk is not None else _Null()
+    with ctx:
+        ev0.record(stream)
+        for _ in range(n):
+            stats.append(step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    return elapsed, stats
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
 
 
 def main():
@@ -237,6 +318,7 @@ def main():
 
     w = me_maps.WORKLOADS[args.workload]
     name = args.workload
+    widen = args.bounds == "widened"
     npix = args.npix or w["npix"]
     lam = me_maps.wavelengths(name)
     nl = lam.size
@@ -254,130 +336,150 @@ def main():
     torch.cuda.synchronize()
     gen.close()
     res = torch.zeros((npix, 10), dtype=torch.float64, device="cuda")
+    res_plain = torch.zeros((npix, 10), dtype=torch.float64, device="cuda")
 
-    cfg = me_b200.parse_config_text(me_maps.control_text(name, precision=args.precision,
-                                                         seed=seed))
-    plan = me_b200.Plan(cfg, lam, device=local)
+    ctl = me_maps.control_text(name, precision=args.precision, seed=seed, widen_bounds=widen)
+    plan = me_b200.Plan(me_b200.parse_config_text(ctl), lam, device=local)
+    plain = me_b200.Plan(me_b200.parse_config_text(ctl), lam, device=local)
     stream = torch.cuda.current_stream()
+
+    # ---- the learned initialiser: trained on the GPU for this line and grid
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    init = me_b200.Initializer.train(plan, samples=args.train_samples, epochs=args.train_epochs,
+                                     seed=20240607 + 7919 * rank)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    plan.set_initializer(init)
 
     def step():
         return plan.invert_device(prof.data_ptr(), npix, res.data_ptr(), 0, stream.cuda_stream)
 
-    for _ in range(args.warmup):
-        st = step()
+    def step_plain():
+        return plain.invert_device(prof.data_ptr(), npix, res_plain.data_ptr(), 0,
+                                   stream.cuda_stream)
 
-    # ---- timed region: K device-resident steps
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    stats = []
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            stats.append(step())
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    elapsed = ev0.elapsed_time(ev1) / 1e3
-    if dist:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    for _ in range(args.warmup):
+        step()
+    clk = ClockSampler(local)
+    elapsed, stats = timed_steps(torch, step, args.steps, stream, dist, clk)
     step_s = elapsed / args.steps
-    kernel_ms = statistics.mean(s["kernel_ms"] for s in stats)
     last = stats[-1]
+    kernel_ms = statistics.mean(s["kernel_ms"] for s in stats)
+    init_ms = statistics.mean(s["init_ms"] for s in stats)
+
+    # ---- the plain LM with the reference's restarts, same map and GPU
+    plain_steps = args.steps if args.plain_steps < 0 else args.plain_steps
+    plain_s, plain_last = None, None
+    if plain_steps > 0:
+        step_plain()  # warm-up (slot buffers, caches)
+        el, pst = timed_steps(torch, step_plain, plain_steps, stream, dist)
+        plain_s, plain_last = el / plain_steps, pst[-1]
 
     # ---- end to end through the host entry point (pinned host buffers)
     e2e = None
     if args.e2e_steps > 0:
         h_prof = torch.empty((npix, 4, nl), dtype=torch.float64, pin_memory=True)
         h_prof.copy_(prof)
-        h_res = np.zeros((npix, 10))
         h_prof_np = h_prof.numpy()
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            r_host, st_e2e = plan.invert(h_prof_np)
+            _, st_e2e = plan.invert(h_prof_np)
         e2e_s = (time.perf_counter() - t0) / args.e2e_steps
         if dist:
             t = torch.tensor([e2e_s], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
-        e2e = {"npix": npix, "seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"],
-               "d2h_ms": st_e2e["d2h_ms"]}
+        e2e = {"seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"], "d2h_ms": st_e2e["d2h_ms"]}
 
     res_np = res.cpu().numpy()
+    res_plain_np = res_plain.cpu().numpy()
     out = {}
     if rank == 0:
         # ---- CPU leg: the reference core on a seeded sample of this map, timed on
-        # the host cores (cpu_baseline); its chi^2 also decides which of the
-        # GPU's pixels count as converged (chi^2 <= 1.05 x the reference's)
+        # the host cores (cpu_baseline); its chi^2 decides which of the GPU's
+        # pixels count as converged (chi^2 <= 1.05 x the reference's)
         cores = host_cores()
-        nb = min(npix, args.cpu_sample or max(args.sample, cores * 32))
+        nb = min(npix, max(args.sample, cores * 32))
         rng = np.random.default_rng(7)
         idx = np.sort(rng.choice(npix, size=nb, replace=False))
         sample_prof = prof[idx].cpu().numpy()
-        ref_res, base_dt, base_kind = cpu_invert(sample_prof, name, cores)
-        cpu_value = nb / base_dt
+        ref_res, base_dt, base_kind = cpu_invert(sample_prof, name, cores, widen)
         valid = ref_res[:, 9] > 0
-        ratio = res_np[idx, 9][valid] / ref_res[valid, 9]
-        frac = float(np.mean(ratio <= 1.05)) if valid.any() else 0.0
-        ref_kind = base_kind
 
-        # ---- roofline of the inversion kernel: algorithmic FLOPs per launch
+        def conv(r):
+            ratio = r[idx, 9][valid] / ref_res[valid, 9]
+            return (float(np.mean(ratio <= 1.05)) if valid.any() else 0.0,
+                    [float(np.quantile(ratio, q)) for q in (0.01, 0.5, 0.99)])
+
+        frac, ratio_q = conv(res_np)
+        frac_plain, ratio_q_plain = conv(res_plain_np) if plain_s else (None, None)
         fc = json.load(open(os.path.join(ROOT, "tests", "golden", "flop_counts.json")))[name]
-
-        def flops(c):
-            return c.get("add", 0) + c.get("mul", 0) + c.get("div", 0) + c.get("sqrt", 0)
-
-        first = last["iterations"]
-        later = last["trials"] - first
-        alg = (last["trials"] * nl * (flops(fc["forward_per_lambda"]) + flops(fc["loss_per_lambda"]))
-               + first * flops(fc["svd_solve_normal_matrix"])
-               + later * flops(fc["svd_solve_orthogonal"])
-               + last["jacobians"] * nl * (flops(fc["jacobian_per_lambda"])
-                                           + flops(fc["normal_equations_per_lambda"])))
-        achieved = alg / (kernel_ms / 1e3) / 1e12
-        clk = clk.summary()
-        peak = fp32_peak_tflops(torch)
-        out = {"ratio_q": [float(np.quantile(ratio, q)) for q in (0.01, 0.5, 0.99)],
-               "frac": frac, "cpu_value": cpu_value, "nb": nb, "base_kind": base_kind,
-               "cores": cores, "achieved": achieved, "alg": alg, "clk": clk, "peak": peak,
-               "ref_kind": ref_kind}
+        alg = roofline_flops(last, fc, nl)
+        out = {"frac": frac, "ratio_q": ratio_q, "frac_plain": frac_plain,
+               "ratio_q_plain": ratio_q_plain, "cpu_value": nb / base_dt, "nb": nb,
+               "base_kind": base_kind, "cores": cores, "alg": alg,
+               "achieved": alg / (kernel_ms / 1e3) / 1e12, "clk": clk.summary(),
+               "peak": fp32_peak_tflops(torch),
+               "err_vs_ref": param_errors(res_np[idx][valid], ref_res[valid]),
+               "err_vs_truth": param_errors(res_np, par_true),
+               "err_vs_truth_ref": param_errors(ref_res[valid], par_true[idx][valid])}
 
     if dist:
         dist.barrier()
     if rank == 0:
         pix_per_s = npix * world / step_s
         value = pix_per_s * out["frac"]
+        plain_cfg = None
+        if plain_s:
+            plain_raw = npix * world / plain_s
+            plain_cfg = {"converged_pixels_per_s": plain_raw * out["frac_plain"],
+                         "raw_pixels_per_s": plain_raw, "ms_per_step": plain_s * 1e3,
+                         "converged_fraction": out["frac_plain"],
+                         "chi2_ratio_q01_q50_q99": out["ratio_q_plain"],
+                         "runs_per_pixel": plain_last["runs"] / max(1, plain_last["valid"]),
+                         "steps": plain_steps, "warmup": 1}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64" if args.precision == "FP32" else "f64",
+            "dtype": "f32+f64 (MLP bf16)" if args.precision == "FP32" else "f64 (MLP bf16)",
             "data": "synthetic (seeded draws of the workload's parameter distributions, "
                     "GPU FP64 synthesis + Gaussian noise)",
-            "config": {"workload": name, "pixels_per_gpu": npix, "nl": nl,
-                       "num_run": int(w["ctl"].get("num_run", 4)),
-                       "precision": args.precision, "init": "Init_Guess (plain LM)",
+            "config": {"workload": name, "bounds": args.bounds, "pixels_per_gpu": npix,
+                       "nl": nl, "num_run": int(w["ctl"].get("num_run", 4)),
+                       "chisq_criteria": float(w["ctl"].get("chisq_criteria", 1.0)),
+                       "precision": args.precision,
+                       "init": "learned (MLP 240-256-256-256-10 GELU), then the reference's "
+                               "restarts for pixels above chisq_criteria",
+                       "train": {"samples": args.train_samples, "epochs": args.train_epochs,
+                                 "batch": 4096, "lr": 1e-3, "seconds": train_s,
+                                 "final_loss": init.final_loss},
                        "parallelism": f"pixel shards x{world}",
                        "l2": "inputs larger than L2 (2 GB of profiles per GPU)",
                        "raw_pixels_per_s": pix_per_s,
                        "converged_fraction": out["frac"],
                        "converged_sample": f"{out['nb']} seeded pixels vs the "
-                                           f"{out['ref_kind']} FP64 chi^2",
-                       "chi2_ratio_q01_q50_q99": out["ratio_q"]},
+                                           f"{out['base_kind']} FP64 chi^2",
+                       "chi2_ratio_q01_q50_q99": out["ratio_q"],
+                       "runs_per_pixel": last["runs"] / max(1, last["valid"]),
+                       "ended_after_learned_start": last["learned_done"] / max(1, last["valid"]),
+                       "init_ms_per_step": init_ms,
+                       "plain_lm": plain_cfg,
+                       "learned_vs_plain": (value / plain_cfg["converged_pixels_per_s"]
+                                            if plain_cfg else None),
+                       "param_err_vs_fp64_ref_median_p99": out["err_vs_ref"],
+                       "param_err_vs_truth_median_p99": out["err_vs_truth"],
+                       "ref_param_err_vs_truth_median_p99": out["err_vs_truth_ref"]},
             "gpu_launches": int(sum(s["launches"] for s in stats)),
             "e2e": None, "clocks": out["clk"],
             "roofline": {"bound": "fp32", "achieved": out["achieved"], "peak": out["peak"],
                          "unit": "TFLOP/s", "frac": out["achieved"] / out["peak"],
                          "traffic": None,
                          "note": "algorithmic FLOPs of the reference algorithm (counted with a "
-                                 "counting scalar type) / inversion-kernel time; peak = FP32 "
+                                 "counting scalar type) / LM round-kernel time; peak = FP32 "
                                  "FFMA throughput measured with cuBLAS SGEMM (TF32 off)",
                          "algorithmic_flop_per_launch": out["alg"]},
             "cpu_baseline": {"value": out["cpu_value"], "unit": UNIT, "cores": out["cores"],
@@ -385,7 +487,8 @@ def main():
                              "sample": f"{out['nb']} seeded pixels of the map, "
                                        f"{out['cores']} processes of the reference core"},
             "stats": {k: last[k] for k in ("valid", "runs", "iterations", "trials", "accepted",
-                                           "jacobians", "redo_pixels", "launches")},
+                                           "jacobians", "redo_pixels", "launches",
+                                           "learned_done")},
         }
         if e2e:
             line["e2e"] = {"value": npix * world / e2e["seconds"] * out["frac"], "unit": UNIT,
@@ -393,6 +496,9 @@ def main():
                            "d2h_bytes_per_step": npix * 10 * 8,
                            "h2d_ms": e2e["h2d_ms"], "d2h_ms": e2e["d2h_ms"]}
         print(json.dumps(line), flush=True)
+    init.close()
+    plan.close()
+    plain.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

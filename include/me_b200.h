@@ -115,6 +115,8 @@ typedef struct me_stats {
   long long rounds;        /* LM rounds (one trial step per pixel in flight) */
   double kernel_ms;        /* device time of the inversion kernel(s)       */
   double h2d_ms, d2h_ms;   /* host<->device copy time (host entry point)   */
+  double init_ms;          /* device time of the learned initialiser        */
+  long long learned_done;  /* pixels that ended after the learned start     */
 } me_stats;
 
 typedef struct me_plan me_plan;
@@ -245,6 +247,92 @@ int me_invert_batch_device_noalloc(const me_config *cfg, const double *lambda, i
  * 1 below Icriteria).  Replaces Init_Guess (Src/ME_SOLVER.c:445-676). */
 int me_init_guess(me_plan *plan, const double *prof, long npix, double *guess,
                   double *extra, int *status);
+
+/* ---------------------------------------------------------------------------
+ * Learned initialiser (no reference counterpart).
+ *
+ * A multilayer perceptron, 4 nl features (I / I_max - 1, 10 Q / I_max,
+ * 10 U / I_max, 10 V / I_max, standardised) -> 256 -> 256 -> 256 GELU -> 10
+ * outputs (B, cos theta, sin 2 phi, cos 2 phi, v, Doppler width, damping,
+ * eta0, beta, S / I_max), on BF16 tensor-core GEMMs with FP32 accumulation,
+ * trained with Adam on profiles that the plan's FP32 forward model synthesises
+ * on the device from seeded parameter draws plus Gaussian noise.
+ *
+ * With an initialiser attached to a plan, every pixel first gets one LM run
+ * (LM_FIT, Src/LM_FIT.c:531-660) from the network's guess; a pixel whose run
+ * meets chisq_criteria ends there, the others go on with the reference's run
+ * schedule (INVERSION, Src/LM_FIT.c:701-733) from Init_Guess, and the best
+ * run is kept.  Without one (the default) the plan is the reference's
+ * algorithm.
+ * ------------------------------------------------------------------------- */
+typedef struct me_mlp me_mlp;
+
+/* Training set and optimiser.  Parameters are drawn uniformly in each range
+ * (cos theta uniform, v normal with sigma v_sigma, S fixed), synthesised on
+ * the plan's grid and line, and given noise of standard deviation `noise`
+ * (in units of the continuum). */
+typedef struct me_mlp_train_params {
+  long long samples;            /* training profiles (>= batch)           */
+  int epochs;                   /* passes over them                        */
+  int batch;                    /* rows per Adam step (multiple of 256)    */
+  double lr;                    /* Adam step size                          */
+  unsigned long long seed;      /* key of the parameter and noise draws    */
+  double b_range[2];            /* field strength [G]                      */
+  double cos_theta_range[2];    /* cosine of the inclination               */
+  double phi_range[2];          /* azimuth [rad]                           */
+  double v_sigma;               /* line-of-sight velocity sigma [km/s]     */
+  double doppler_range[2];      /* Doppler width [mA]                      */
+  double damping_range[2];      /* damping                                 */
+  double eta_range[2];          /* line-to-continuum absorption eta0       */
+  double s;                     /* source function S0 (continuum units)    */
+  double beta_range[2];         /* source function gradient ratio          */
+  double noise;                 /* Gaussian noise sigma                    */
+} me_mlp_train_params;
+
+/* The defaults: the parameter distributions of the Fe I 15648.5 A maps
+ * (B ~ U(0, 3000) G, cos theta ~ U(-1, 1), phi ~ U(0, pi), v ~ N(0, 1.5) km/s,
+ * Doppler width ~ U(150, 350) mA, a ~ U(0.1, 0.8), eta0 ~ U(2, 30), S0 = 1,
+ * beta ~ U(0.1, 0.6), noise 1e-3); 2^22 samples, 16 epochs, batch 4096,
+ * lr 1e-3. */
+int me_mlp_train_params_default(me_mlp_train_params *tp);
+
+/* Trains a new initialiser for the plan's line and grid on the plan's device.
+ * final_loss (may be NULL) receives the mean squared error of the standardised
+ * outputs over the last epoch. */
+int me_mlp_train(me_plan *plan, const me_mlp_train_params *tp, me_mlp **out,
+                 double *final_loss);
+void me_mlp_destroy(me_mlp *mlp);
+
+/* Binary file of the weights and the standardisation; load places the model
+ * on CUDA device `device`. */
+int me_mlp_save(const me_mlp *mlp, const char *path);
+int me_mlp_load(const char *path, int device, me_mlp **out);
+
+/* Network guess par [npix][9] (the reference's units) for profiles prof
+ * [npix][4][nl]: host buffers, or device buffers ordered on `stream`. */
+int me_mlp_predict(me_mlp *mlp, const double *prof, long npix, double *par);
+int me_mlp_predict_device(me_mlp *mlp, const double *d_prof, long npix, double *d_par,
+                          void *stream);
+
+/* Attaches an initialiser to a plan (NULL detaches).  The plan does not own
+ * it; its grid size must match the plan's. */
+int me_plan_set_initializer(me_plan *plan, me_mlp *mlp);
+
+/* Layer sizes and parameters, for checking the training arithmetic.  nl: the
+ * grid size; nin_pad: input width (4 nl rounded up to 32, zero weights past
+ * 4 nl); the output layer has 32 rows of which the first 10 are used.
+ * Parameters are flattened layer by layer as W [dout][din] then b [dout] (FP32
+ * master copies). */
+int me_mlp_shape(const me_mlp *mlp, int *nl, int *nin_pad, long long *nparams);
+int me_mlp_get_params(const me_mlp *mlp, float *params);
+int me_mlp_set_params(me_mlp *mlp, const float *params);
+
+/* Loss and gradient of one batch: x [rows][nin_pad] standardised features,
+ * t [rows][10] standardised targets (host FP32; rows a multiple of 256).
+ * loss = mean over rows and the 10 outputs of (y - t)^2; grad has the layout
+ * of the parameters.  No optimiser step is taken. */
+int me_mlp_loss_grad(me_mlp *mlp, const float *x, const float *t, int rows, double *loss,
+                     float *grad);
 
 #ifdef __cplusplus
 }

@@ -111,6 +111,8 @@ struct me_plan {
   std::vector<unsigned char> h_flags;
   std::vector<double> h_pen0, h_lastchi, h_stale, h_used;
   std::vector<long long> h_list;
+  me_mlp *init = nullptr;  // learned initialiser (not owned), or null
+  DevBuf d_init;           // [npix][9] its guesses for the current batch
 };
 
 extern "C" const char *me_version(void) { return "me_b200 0.1 (sm_100a)"; }
@@ -311,6 +313,28 @@ extern "C" void me_plan_set_window(me_plan *p, int window) {
   if (p && window >= 0) p->window = window;
 }
 
+extern "C" int me_plan_set_initializer(me_plan *p, me_mlp *mlp) {
+  if (!p) return fail(ME_ERR_ARG, "null plan");
+  if (mlp) {
+    int nl = 0;
+    const int rc = me_mlp_shape(mlp, &nl, nullptr, nullptr);
+    if (rc) return rc;
+    if (nl != p->P.nl)
+      return fail(ME_ERR_ARG, "initialiser trained for a grid of another size");
+  }
+  p->init = mlp;
+  return ME_OK;
+}
+
+namespace me {
+int plan_devplan(const me_plan *p, DevPlan *out, int *device) {
+  if (!p || !out || !device) return fail(ME_ERR_ARG, "null argument");
+  *out = p->P;
+  *device = p->device;
+  return ME_OK;
+}
+}  // namespace me
+
 namespace {
 
 // Grows the slot buffers to W slots and returns the device view.
@@ -424,6 +448,17 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   A.stale = nullptr;
   A.carry = p->carry;
   A.first_pixel = 0;
+  float init_ms = 0.f;
+  if (p->init) {
+    CK(p->d_init.ensure(n * 9 * sizeof(double)));
+    CK(cudaEventRecord(p->ev0, st));
+    const int rc = me_mlp_predict_device(p->init, d_prof, npix, p->d_init.as<double>(), st);
+    if (rc) return rc;
+    CK(cudaEventRecord(p->ev1, st));
+    CK(cudaEventSynchronize(p->ev1));
+    cudaEventElapsedTime(&init_ms, p->ev0, p->ev1);
+    A.init_par = p->d_init.as<double>();
+  }
 
   long long rounds = 0, rounds_total = 0;
   CK(cudaEventRecord(p->ev0, st));
@@ -514,9 +549,14 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     stats->jacobians = (long long)tot[5];
     stats->wavelengths = (long long)(tot[3] + tot[5]) * p->P.nl;
     stats->redo_pixels = redo_total;
-    stats->launches = 4 * rounds_total + (d_fit ? 1 : 0);
+    stats->launches = 4 * rounds_total + (d_fit ? 1 : 0) +
+                      (p->init ? me::kMlpPredLaunches *
+                                     ((npix + me::kMlpPredChunk - 1) / me::kMlpPredChunk)
+                               : 0);
     stats->rounds = rounds_total;
     stats->kernel_ms = kernel_ms;
+    stats->init_ms = init_ms;
+    stats->learned_done = (long long)tot[7];
   }
   return ME_OK;
 }

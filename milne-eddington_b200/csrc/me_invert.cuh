@@ -166,10 +166,26 @@ static __device__ bool refill(const DevPlan &P, const InvertArgs &A, const Slots
     }
     t_valid++;
     S.pix[s] = pix;
-    S.run[s] = 0;
     S.it[s] = 0;
     store9(S.guess, W, s, pin.guess);
-    store9(S.par, W, s, pin.guess);
+    if (A.init_par) {
+      // learned start: the free parameters from the initialiser, folded into
+      // the bounds; the fixed ones keep Init_Guess's values
+      double q[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) {
+        const double v = A.init_par[(size_t)pix * 9 + i];
+        q[i] = (P.fixed[i] || !isfinite(v)) ? pin.guess[i] : v;
+      }
+      bounds_fold(q, P, pin.l70, pin.l71);
+      store9(S.par, W, s, q);
+      S.run[s] = -1;
+      if (A.penalty0) A.penalty0[pix] = P.regul_any ? penalty_of(P, q) : 0.0;
+    } else {
+      store9(S.par, W, s, pin.guess);
+      S.run[s] = 0;
+      if (A.penalty0) A.penalty0[pix] = P.regul_any ? penalty_of(P, pin.guess) : 0.0;
+    }
     double *sc = S.sc;
     sc[SC_LMCHISQ * W + s] =
         A.stale ? A.stale[pix] : (pix == A.first_pixel ? A.carry : INFINITY);
@@ -183,7 +199,6 @@ static __device__ bool refill(const DevPlan &P, const InvertArgs &A, const Slots
 #pragma unroll
     for (int i = 0; i < 4; i++) S.cnt[i * W + s] = 0;
     S.had_trial[s] = 0;
-    if (A.penalty0) A.penalty0[pix] = P.regul_any ? penalty_of(P, pin.guess) : 0.0;
     S.state[s] = SL_JAC_START;
     return true;
   }
@@ -383,10 +398,9 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
   voigt_block_setup<T>(K, P, s_tab);
   T *rden = s_rden + threadIdx.x;
   const int W = S.W;
-  const int n = P.npar;
   const int nl = P.nl;
   const int next_parity = parity ^ 1;
-  unsigned long long t_valid = 0, t_runs = 0, t_iter = 0, t_trials = 0, t_acc = 0;
+  unsigned long long t_valid = 0, t_runs = 0, t_iter = 0, t_trials = 0, t_acc = 0, t_learned = 0;
   int busy_delta = 0;
 
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < W; s += gridDim.x * blockDim.x) {
@@ -469,7 +483,8 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
       t_runs++;
       double pbest[9];
       double best = sc[SC_BEST * W + s];
-      if (chisq_run < P.chisq_crit || run == 0 || chisq_run < best) {
+      const int first_run = A.init_par ? -1 : 0;
+      if (chisq_run < P.chisq_crit || run == first_run || chisq_run < best) {
 #pragma unroll
         for (int i = 0; i < 9; i++) pbest[i] = par[i];
         store9(S.pbest, W, s, pbest);
@@ -479,6 +494,12 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
         load9(S.pbest, W, s, pbest);
       }
       bool stop = false;
+      // a learned start that meets chisq_criteria ends the pixel; otherwise
+      // the reference's schedule follows from run 0, keeping the best
+      if (run < 0 && chisq_run < P.chisq_crit) {
+        stop = true;
+        t_learned++;
+      }
       if (chisq_run < P.chisq_crit && (run >= 4 || run == P.nruns * 4)) stop = true;
       if (run >= P.nruns * 2 && best < P.chisq_crit * 2) stop = true;
       run++;
@@ -487,7 +508,10 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
         // Random_Jump (Src/LM_FIT.c:157-201)
         double g[9];
         load9(S.guess, W, s, g);
-        if (run < 4) {
+        if (run == 0) {  // after a learned start: the reference's first run
+#pragma unroll
+          for (int i = 0; i < 9; i++) par[i] = g[i];
+        } else if (run < 4) {
 #pragma unroll
           for (int i = 0; i < 9; i++) par[i] = pbest[i];
           par[2] = g[2] + kPi / 4. * run;
@@ -504,7 +528,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
           par[7] = pbest[7];
           par[8] = g[8] + 0.1 * z[7];
         }
-        bounds_fold(par, P, l70, l71);
+        if (run > 0) bounds_fold(par, P, l70, l71);
         store9(S.par, W, s, par);
         S.state[s] = SL_JAC_START;
         append_jac(S, next_parity, s);
@@ -545,6 +569,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
     if (t_iter) atomicAdd(A.totals + 2, t_iter);
     if (t_trials) atomicAdd(A.totals + 3, t_trials);
     if (t_acc) atomicAdd(A.totals + 4, t_acc);
+    if (t_learned) atomicAdd(A.totals + 7, t_learned);
   }
 }
 

@@ -16,6 +16,9 @@ constexpr int kBlock = 128;
 #endif
 constexpr int kSvdBlock = 64;  // threads of svd_kernel; each holds its matrix in shared memory
 constexpr int kSvdSmem = (81 + 18) * kSvdBlock * 8;
+// learned initialiser inference: rows per chunk, kernel launches per chunk
+constexpr int kMlpPredChunk = 65536;
+constexpr int kMlpPredLaunches = 6;
 
 // Life cycle of an inversion slot (one pixel in flight).
 enum SlotStateCode : int {
@@ -71,13 +74,16 @@ struct InvertArgs {
   double *penalty0;            // [npix] regularisation penalty at the first guess
   double *lastchi;             // [npix] chi^2 of the pixel's last trial step
   unsigned int *counters;      // [npix][4] runs, iterations, trials, accepted
-  unsigned long long *totals;  // [8] valid, runs, iterations, trials, accepted, jacobians, svd limit hits
+  unsigned long long *totals;  // [8] valid, runs, iterations, trials, accepted, jacobians,
+                               // svd limit hits, pixels done after a learned start
   unsigned long long *next;    // queue position (zeroed before the batch)
   const long long *list;       // pixel indices to process (null = 0..count-1)
   long long count;             // number of queue items
   const double *stale;         // [npix] carried LM chi^2 per pixel (null = carry/first_pixel)
   double carry;                // carried LM chi^2 for pixel first_pixel
   long long first_pixel;
+  const double *init_par;      // [npix][9] learned starting parameters (an extra first
+                               // run, run -1), or null for the reference's schedule
 };
 
 // Plan constants from a control file and a wavelength grid (me_api.cu);

@@ -32,6 +32,7 @@ STATUS = {
     -7: "ME_ERR_NOMEM",
     -8: "ME_ERR_FORMAT",
 }
+globals().update({name: code for code, name in STATUS.items()})
 
 _D = ctypes.POINTER(ctypes.c_double)
 
@@ -116,6 +117,8 @@ class MeStats(ctypes.Structure):
         ("kernel_ms", ctypes.c_double),
         ("h2d_ms", ctypes.c_double),
         ("d2h_ms", ctypes.c_double),
+        ("init_ms", ctypes.c_double),
+        ("learned_done", ctypes.c_longlong),
     ]
 
     def as_dict(self):
@@ -131,7 +134,30 @@ EXPORTED = [
     "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
     "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
     "me_invert_batch_device_noalloc",
+    "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
+    "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
+    "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
 ]
+
+
+class MeMlpTrainParams(ctypes.Structure):
+    _fields_ = [
+        ("samples", ctypes.c_longlong),
+        ("epochs", ctypes.c_int),
+        ("batch", ctypes.c_int),
+        ("lr", ctypes.c_double),
+        ("seed", ctypes.c_ulonglong),
+        ("b_range", ctypes.c_double * 2),
+        ("cos_theta_range", ctypes.c_double * 2),
+        ("phi_range", ctypes.c_double * 2),
+        ("v_sigma", ctypes.c_double),
+        ("doppler_range", ctypes.c_double * 2),
+        ("damping_range", ctypes.c_double * 2),
+        ("eta_range", ctypes.c_double * 2),
+        ("s", ctypes.c_double),
+        ("beta_range", ctypes.c_double * 2),
+        ("noise", ctypes.c_double),
+    ]
 
 
 class MeError(RuntimeError):
@@ -197,6 +223,23 @@ def lib() -> ctypes.CDLL:
                                                      ctypes.c_void_p, _D, ctypes.c_void_p]
         L.me_init_guess.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                     ctypes.POINTER(ctypes.c_int)]
+        _F = ctypes.POINTER(ctypes.c_float)
+        L.me_mlp_train_params_default.argtypes = [ctypes.POINTER(MeMlpTrainParams)]
+        L.me_mlp_train.argtypes = [ctypes.c_void_p, ctypes.POINTER(MeMlpTrainParams),
+                                   ctypes.POINTER(ctypes.c_void_p), _D]
+        L.me_mlp_destroy.argtypes = [ctypes.c_void_p]
+        L.me_mlp_destroy.restype = None
+        L.me_mlp_save.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.me_mlp_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.me_mlp_predict.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D]
+        L.me_mlp_predict_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                            ctypes.c_void_p, ctypes.c_void_p]
+        L.me_plan_set_initializer.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.me_mlp_shape.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]
+        L.me_mlp_get_params.argtypes = [ctypes.c_void_p, _F]
+        L.me_mlp_set_params.argtypes = [ctypes.c_void_p, _F]
+        L.me_mlp_loss_grad.argtypes = [ctypes.c_void_p, _F, _F, ctypes.c_int, _D, _F]
         _lib = L
     return _lib
 
@@ -303,6 +346,12 @@ class Plan:
     def window(self, w: int):
         lib().me_plan_set_window(self._h, int(w))
 
+    def set_initializer(self, init: Optional["Initializer"]):
+        """Attaches a learned initialiser (None detaches); the plan does not own it."""
+        _check(lib().me_plan_set_initializer(self._h, init.handle if init is not None else None),
+               "me_plan_set_initializer")
+        self._init = init
+
     def invert(self, prof: np.ndarray, want_fit: bool = False):
         """me_invert_batch on host arrays: prof [npix][4][nl] -> res [npix][10] (+fit)."""
         prof = np.ascontiguousarray(prof, dtype=np.float64)
@@ -406,3 +455,107 @@ def svd(a: np.ndarray, device: int = 0):
     w = np.zeros((nmat, n))
     _check(lib().me_svd(_ptr(a), nmat, n, _ptr(u), _ptr(w), _ptr(v), device), "me_svd")
     return u, w, v
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def mlp_train_params(**overrides) -> MeMlpTrainParams:
+    """me_mlp_train_params_default with keyword overrides (ranges as 2-tuples)."""
+    tp = MeMlpTrainParams()
+    _check(lib().me_mlp_train_params_default(ctypes.byref(tp)), "me_mlp_train_params_default")
+    for k, v in overrides.items():
+        if not hasattr(tp, k):
+            raise KeyError(k)
+        if isinstance(v, (tuple, list)):
+            arr = getattr(tp, k)
+            arr[0], arr[1] = float(v[0]), float(v[1])
+        else:
+            setattr(tp, k, v)
+    return tp
+
+
+class Initializer:
+    """me_mlp: the learned initialiser (4 nl -> 256 -> 256 -> 256 -> 10 GELU MLP)."""
+
+    def __init__(self, handle: ctypes.c_void_p, final_loss: float = float("nan")):
+        self._h = handle
+        self.final_loss = final_loss
+
+    @classmethod
+    def train(cls, plan: "Plan", params: Optional[MeMlpTrainParams] = None, **overrides):
+        tp = params if params is not None else mlp_train_params(**overrides)
+        h = ctypes.c_void_p()
+        loss = np.zeros(1)
+        _check(lib().me_mlp_train(plan.handle, ctypes.byref(tp), ctypes.byref(h), _ptr(loss)),
+               "me_mlp_train")
+        return cls(h, float(loss[0]))
+
+    @classmethod
+    def load(cls, path: str, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().me_mlp_load(str(path).encode(), device, ctypes.byref(h)), "me_mlp_load")
+        return cls(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().me_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def save(self, path: str):
+        _check(lib().me_mlp_save(self._h, str(path).encode()), "me_mlp_save")
+
+    def shape(self):
+        nl, nip, npar = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        _check(lib().me_mlp_shape(self._h, ctypes.byref(nl), ctypes.byref(nip),
+                                  ctypes.byref(npar)), "me_mlp_shape")
+        return nl.value, nip.value, npar.value
+
+    def predict(self, prof: np.ndarray) -> np.ndarray:
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        par = np.zeros((prof.shape[0], 9))
+        _check(lib().me_mlp_predict(self._h, _ptr(prof), prof.shape[0], _ptr(par)),
+               "me_mlp_predict")
+        return par
+
+    def predict_device(self, d_prof: int, npix: int, d_par: int, stream: int = 0):
+        _check(lib().me_mlp_predict_device(self._h, ctypes.c_void_p(d_prof), npix,
+                                           ctypes.c_void_p(d_par), ctypes.c_void_p(stream)),
+               "me_mlp_predict_device")
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.shape()[2], dtype=np.float32)
+        _check(lib().me_mlp_get_params(self._h, _fptr(out)), "me_mlp_get_params")
+        return out
+
+    def set_params(self, params: np.ndarray):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        assert params.size == self.shape()[2]
+        _check(lib().me_mlp_set_params(self._h, _fptr(params)), "me_mlp_set_params")
+
+    def loss_grad(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = np.zeros(1)
+        grad = np.zeros(self.shape()[2], dtype=np.float32)
+        _check(lib().me_mlp_loss_grad(self._h, _fptr(x), _fptr(t), x.shape[0], _ptr(loss),
+                                      _fptr(grad)), "me_mlp_loss_grad")
+        return float(loss[0]), grad
