@@ -166,6 +166,15 @@ void me_plan_set_grid(me_plan *plan, int grid);
 int me_plan_window(const me_plan *plan);
 void me_plan_set_window(me_plan *plan, int window);
 
+/* Pixels in flight at or below which, once every pixel of a batch has been
+ * taken from the queue, the remaining ones are run to the end one warp per
+ * pixel (their synthesis spread over the lanes) instead of one LM step per
+ * launch round: the same arithmetic up to the compiler's contraction of
+ * multiply-adds, and a much shorter tail.  -1 (default): two waves of the
+ * tail kernel's warps on this device; 0: rounds only. */
+int me_plan_tail_slots(const me_plan *plan);
+void me_plan_set_tail_slots(me_plan *plan, int slots);
+
 /* Inverts npix pixels.  prof: host [npix][4][nl]; res: host [npix][10];
  * fit: host [npix][4][nl] or NULL (best-fit profiles, zeros when skipped);
  * stats may be NULL.  Replaces INVERSION_MULTI (Src/LM_FIT.c:746-811). */

@@ -104,7 +104,11 @@ struct me_plan {
   int slots_w = 0;         // allocated slot count
   DevBuf d_slot_pix, d_slot_i32, d_slot_cnt, d_slot_u8, d_slot_sc, d_slot_vec, d_slot_hess,
       d_slot_list, d_slot_small;
-  int grid_jac = 0, grid_trial = 0, grid_svd = 0;
+  int grid_jac = 0, grid_trial = 0, grid_svd = 0, grid_fin = 0;
+  // pixels in flight at or below which, with the queue empty, the tail kernel
+  // finishes the batch (-1: two waves of its warps; 0: rounds only)
+  int tail_slots = -1;
+  long long finish_launches = 0;  // tail-kernel launches of the current batch
   int poll_rounds = 8;     // rounds launched between checks of the queue
   unsigned long long *h_poll = nullptr;  // pinned: next, busy
   long long rounds_last = 0;
@@ -212,6 +216,14 @@ int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P
   P.lcoeffi = cfg->lcoeffi;
   P.niter = cfg->num_iter;
   P.nruns = cfg->num_run;
+  // the LM's trials end only when the damping outgrows its limit, and every
+  // loop on the device is bounded by these (slot_step_cap)
+  if (!(P.lam_reject >= 1.5 && P.lam_accept >= 1.5 && P.lam_reject < 1e300))
+    return fail(ME_ERR_CONFIG, "lambda_accept and lambda_reject should be larger than 1.5");
+  if (!(P.damp > 0 && P.damp < 1e300 && P.lam_lim[1] > 0 && P.lam_lim[1] < 1e300))
+    return fail(ME_ERR_CONFIG, "damp and lambda_limits must be positive and finite");
+  if (P.niter < 0 || P.niter > 100000 || P.nruns < 0 || P.nruns > 100000)
+    return fail(ME_ERR_CONFIG, "num_iter and num_run must lie in [0, 100000]");
   P.hmi_ref = cfg->hmi_ref ? 1 : 0;
   P.regul_any = cfg->regul_any ? 1 : 0;
   P.seed = cfg->rng_seed;
@@ -255,6 +267,7 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
   p->grid_jac = me::round_grid(p->precision, 0, device);
   p->grid_trial = me::round_grid(p->precision, 1, device);
   p->grid_svd = me::round_grid(p->precision, 2, device);
+  p->grid_fin = me::round_grid(p->precision, 3, device);
   p->grid = p->grid_trial;
   if (cudaMallocHost((void **)&p->h_poll, 2 * sizeof(unsigned long long)) != cudaSuccess) {
     me_plan_destroy(p);
@@ -311,6 +324,11 @@ extern "C" void me_plan_set_grid(me_plan *p, int grid) {
 extern "C" int me_plan_window(const me_plan *p) { return p ? p->window : 0; }
 extern "C" void me_plan_set_window(me_plan *p, int window) {
   if (p && window >= 0) p->window = window;
+}
+
+extern "C" int me_plan_tail_slots(const me_plan *p) { return p ? p->tail_slots : 0; }
+extern "C" void me_plan_set_tail_slots(me_plan *p, int slots) {
+  if (p) p->tail_slots = slots < 0 ? -1 : slots;
 }
 
 extern "C" int me_plan_set_initializer(me_plan *p, me_mlp *mlp) {
@@ -379,8 +397,10 @@ int ensure_slots(me_plan *p, int W, me::Slots &S) {
   return ME_OK;
 }
 
-// Runs one queue (A.count items) to completion: rounds of jac_kernel +
-// trial_kernel on the plan's slots until every pixel is done.
+// Runs one queue (A.count items) to completion: rounds of jac_kernel,
+// svd_kernel and trial_kernel on the plan's slots while the queue feeds them,
+// then, once it is empty and at most tail_slots pixels remain, finish_kernel
+// (one warp per pixel, no per-round launches) for the rest.
 int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &rounds) {
   const long long cap = p->window > 0 ? p->window : 131072;
   const int W = (int)(A.count < cap ? A.count : cap);
@@ -397,7 +417,11 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
   grids[2] = std::min(p->grid_svd, (W + me::kSvdBlock - 1) / me::kSvdBlock);
   int parity = 0;
   rounds = 0;
+  // every slot step is one round: a bound no valid batch reaches
+  const double round_cap = (double)me::slot_step_cap(p->P) * (double)((A.count + W - 1) / W + 1);
   while (true) {
+    if ((double)rounds > round_cap)
+      return fail(ME_ERR_TIMEOUT, "inversion rounds exceeded their bound");
     for (int r = 0; r < p->poll_rounds; r++) {
       CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st));
       parity ^= 1;
@@ -407,7 +431,18 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     CK(cudaMemcpyAsync(p->h_poll + 1, S.busy, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     const int busy = *reinterpret_cast<int *>(p->h_poll + 1);
-    if (p->h_poll[0] >= (unsigned long long)A.count && busy == 0) break;
+    const bool drained = p->h_poll[0] >= (unsigned long long)A.count;
+    if (drained && busy == 0) break;
+    const int tail = p->tail_slots < 0 ? 2 * p->grid_fin * (me::kBlock / 32) : p->tail_slots;
+    if (drained && busy <= tail) {
+      // the queue is empty and few pixels remain: one warp per pixel to the end
+      int *cursor = S.busy + 1;
+      CK(cudaMemsetAsync(cursor, 0, sizeof(int), st));
+      const int g = std::min(p->grid_fin, (busy + me::kBlock / 32 - 1) / (me::kBlock / 32));
+      CK(me::launch_finish(p->precision, p->P, A, S, cursor, std::max(g, 1), st));
+      p->finish_launches++;
+      break;
+    }
   }
   return ME_OK;
 }
@@ -461,6 +496,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   }
 
   long long rounds = 0, rounds_total = 0;
+  p->finish_launches = 0;
   CK(cudaEventRecord(p->ev0, st));
   int rc = run_queue(p, A, st, rounds);
   if (rc) return rc;
@@ -490,6 +526,8 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   p->h_used.assign(n, INFINITY);
   p->h_used[0] = p->carry;
   while (true) {
+    for (size_t i = 0; i < n; i++)
+      if (p->h_flags[i] & 8) return fail(ME_ERR_TIMEOUT, "a pixel exceeded its LM step bound");
     double prev = p->carry;
     p->h_list.clear();
     for (size_t i = 0; i < n; i++) {
@@ -549,7 +587,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     stats->jacobians = (long long)tot[5];
     stats->wavelengths = (long long)(tot[3] + tot[5]) * p->P.nl;
     stats->redo_pixels = redo_total;
-    stats->launches = 4 * rounds_total + (d_fit ? 1 : 0) +
+    stats->launches = 4 * rounds_total + p->finish_launches + (d_fit ? 1 : 0) +
                       (p->init ? me::kMlpPredLaunches *
                                      ((npix + me::kMlpPredChunk - 1) / me::kMlpPredChunk)
                                : 0);

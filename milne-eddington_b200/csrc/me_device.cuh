@@ -1324,6 +1324,191 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
 #undef R_
 }
 
+// gr_svd_u with the matrix in the shared memory of one warp (row-major,
+// stride 1) and its vector loops spread over the lanes: lane j owns column j
+// (or row j) of each update, every sum is formed by one lane in gr_svd_u's
+// order, and the scalar recurrences (w, rv1, the QR chase) run redundantly in
+// every lane on private copies.  The arithmetic is gr_svd_u's operation for
+// operation, so the results are the same bits; only the latency changes.
+// w [n] is private to the lane.  All 32 lanes call it.
+static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, int lane) {
+#define A_(i, j) a[(i) * n + (j)]
+  const int m = n;
+  int l = 0, nm = 0;
+  double anorm = 0., c, f, g = 0., h, s, scale = 0., x, y, z;
+  double rv1[9];
+  int hit = 0;
+  for (int i = 0; i < n; i++) {
+    l = i + 1;
+    rv1[i] = scale * g;
+    g = s = scale = 0.0;
+    for (int k = i; k < m; k++) scale += fabs(A_(k, i));
+    if (scale) {
+      const double is = 1.0 / scale;
+      for (int k = i; k < m; k++) {
+        const double t = A_(k, i) * is;
+        s += t * t;
+      }
+      f = A_(i, i) * is;
+      g = f >= 0 ? -sqrt(s) : sqrt(s);
+      h = f * g - s;
+      __syncwarp();
+      if (lane >= i && lane < m) A_(lane, i) = lane == i ? f - g : A_(lane, i) * is;
+      __syncwarp();
+      const double ih = 1.0 / h;
+      if (lane >= l && lane < n) {
+        double sj = 0.0;
+        for (int k = i; k < m; k++) sj += A_(k, i) * A_(k, lane);
+        const double fj = sj * ih;
+        for (int k = i; k < m; k++) A_(k, lane) += fj * A_(k, i);
+      }
+      __syncwarp();
+      if (lane >= i && lane < m) A_(lane, i) *= scale;
+      __syncwarp();
+    }
+    w[i] = scale * g;
+    g = s = scale = 0.0;
+    if (i != n - 1) {
+      for (int k = l; k < n; k++) scale += fabs(A_(i, k));
+      if (scale) {
+        const double is = 1.0 / scale;
+        for (int k = l; k < n; k++) {
+          const double t = A_(i, k) * is;
+          s += t * t;
+        }
+        f = A_(i, l) * is;
+        g = f >= 0 ? -sqrt(s) : sqrt(s);
+        h = f * g - s;
+        const double ih = 1.0 / h;
+        // the scaled row i (with f - g at l) and rv1 = row / h, in every lane
+        for (int k = l; k < n; k++) rv1[k] = (k == l ? f - g : A_(i, k) * is) * ih;
+        __syncwarp();
+        if (lane >= l && lane < n) A_(i, lane) = lane == l ? f - g : A_(i, lane) * is;
+        __syncwarp();
+        if (lane >= l && lane < m) {
+          double sj = 0.0;
+          for (int k = l; k < n; k++) sj += A_(lane, k) * A_(i, k);
+          for (int k = l; k < n; k++) A_(lane, k) += sj * rv1[k];
+        }
+        __syncwarp();
+        if (lane >= l && lane < n) A_(i, lane) *= scale;
+        __syncwarp();
+      }
+    }
+    const double t = fabs(w[i]) + fabs(rv1[i]);
+    if (anorm < t) anorm = t;
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    l = i + 1;
+    g = w[i];
+    if (lane >= l && lane < n) A_(i, lane) = 0.0;
+    __syncwarp();
+    if (g != 0.0) {
+      g = 1.0 / g;
+      const double iaii = 1.0 / A_(i, i);
+      if (lane >= l && lane < n) {
+        double sj = 0.0;
+        for (int k = l; k < m; k++) sj += A_(k, i) * A_(k, lane);
+        const double fj = (sj * iaii) * g;
+        for (int k = i; k < m; k++) A_(k, lane) += fj * A_(k, i);
+      }
+      __syncwarp();
+      if (lane >= i && lane < m) A_(lane, i) *= g;
+    } else {
+      if (lane >= i && lane < m) A_(lane, i) = 0.0;
+    }
+    __syncwarp();
+    if (lane == i) A_(i, i) += 1.0;
+    __syncwarp();
+  }
+  // QR sweeps: each rotation touches row `lane` only, so the lanes need no
+  // synchronisation until the end
+  for (int k = n - 1; k >= 0; k--) {
+    for (int its = 0; its < 50; its++) {
+      int flag = 1;
+      for (l = k; l >= 0; l--) {
+        nm = l - 1;
+        if ((fabs(rv1[l]) + anorm) == anorm) {
+          flag = 0;
+          break;
+        }
+        if (nm >= 0 && (fabs(w[nm]) + anorm) == anorm) break;
+      }
+      if (flag) {
+        c = 0.0;
+        s = 1.0;
+        for (int i = l; i <= k; i++) {
+          f = s * rv1[i];
+          rv1[i] = c * rv1[i];
+          if ((fabs(f) + anorm) == anorm) break;
+          g = w[i];
+          h = pythag_d(f, g);
+          w[i] = h;
+          h = 1.0 / h;
+          c = g * h;
+          s = -f * h;
+          if (lane < m) {
+            const double yy = A_(lane, nm), zz = A_(lane, i);
+            A_(lane, nm) = yy * c + zz * s;
+            A_(lane, i) = zz * c - yy * s;
+          }
+        }
+      }
+      z = w[k];
+      if (l == k) {
+        if (z < 0.0) w[k] = -z;
+        break;
+      }
+      if (its == 49) hit = 1;
+      x = w[l];
+      nm = k - 1;
+      y = w[nm];
+      g = rv1[nm];
+      h = rv1[k];
+      f = ((y - z) * (y + z) + (g - h) * (g + h)) / (2.0 * h * y);
+      g = pythag_d(f, 1.0);
+      f = ((x - z) * (x + z) + h * (y / (f + (f >= 0.0 ? g : -g)) - h)) / x;
+      c = s = 1.0;
+      for (int j = l; j <= nm; j++) {
+        const int i = j + 1;
+        g = rv1[i];
+        y = w[i];
+        h = s * g;
+        g *= c;
+        z = pythag_d(f, h);
+        rv1[j] = z;
+        const double iz = 1.0 / z;
+        c = f * iz;
+        s = h * iz;
+        f = x * c + g * s;
+        g = g * c - x * s;
+        h = y * s;
+        y *= c;
+        z = pythag_d(f, h);
+        w[j] = z;
+        if (z) {
+          z = 1.0 / z;
+          c = f * z;
+          s = h * z;
+        }
+        f = c * g + s * y;
+        x = c * y - s * g;
+        if (lane < m) {
+          const double yy = A_(lane, j), zz = A_(lane, i);
+          A_(lane, j) = yy * c + zz * s;
+          A_(lane, i) = zz * c - yy * s;
+        }
+      }
+      rv1[l] = 0.0;
+      rv1[k] = f;
+      w[k] = x;
+    }
+  }
+  __syncwarp();
+  return hit;
+#undef A_
+}
+
 // x = V diag(1/w) U^T b, skipping w <= 1e-50 (svbksb, SVD_TEMPLATE.h:348-406).
 __device__ __forceinline__ void gr_backsub(const double *u, const double *v, const double *w,
                                            const double *b, int n, double *x) {

@@ -204,6 +204,337 @@ static __device__ bool refill(const DevPlan &P, const InvertArgs &A, const Slots
   }
 }
 
+// Counts a kernel accumulates per thread and adds to the batch totals once.
+struct Tally {
+  unsigned long long valid = 0, runs = 0, iter = 0, trials = 0, acc = 0, learned = 0, jac = 0,
+                     svdlim = 0;
+  int busy_delta = 0;
+  __device__ void flush(const InvertArgs &A, const Slots &S) const {
+    if (busy_delta) atomicAdd(S.busy, busy_delta);
+    if (!A.totals) return;
+    if (valid) atomicAdd(A.totals + 0, valid);
+    if (runs) atomicAdd(A.totals + 1, runs);
+    if (iter) atomicAdd(A.totals + 2, iter);
+    if (trials) atomicAdd(A.totals + 3, trials);
+    if (acc) atomicAdd(A.totals + 4, acc);
+    if (jac) atomicAdd(A.totals + 5, jac);
+    if (svdlim) atomicAdd(A.totals + 6, svdlim);
+    if (learned) atomicAdd(A.totals + 7, learned);
+  }
+};
+
+// The slot's per-pixel constants of a synthesis: step (with the pixel's S
+// step) and the Stokes weights / sqrt(norm0).
+__device__ __forceinline__ void slot_weights(const DevPlan &P, const Slots &S, int s,
+                                             double step[9], double sw[4]) {
+  const int W = S.W;
+#pragma unroll
+  for (int k = 0; k < 9; k++) step[k] = P.step[k];
+  step[7] = S.sc[SC_STEP7 * W + s];
+  const double isn = S.sc[SC_ISN * W + s];
+#pragma unroll
+  for (int k = 0; k < 4; k++) sw[k] = P.weights[k] * isn;
+}
+
+// After the synthesis with Jacobian at the slot's parameters: the LM_FIT
+// set-up on a run start (Src/LM_FIT.c:549-566), the free-parameter block of the
+// normal matrix with Get_Regul's diagonal and gradient terms
+// (Hessian_Compute + Get_Regul, Src/LM_FIT.c:240-396), and the move to the
+// first trial (or the run's end when num_iter <= 0).  One thread per slot.
+__device__ __forceinline__ void jac_store(const DevPlan &P, const Slots &S, int s,
+                                          const double *par, double chi0, const double *H45,
+                                          const double *g9) {
+  const int W = S.W;
+  const int n = P.npar;
+  double ratio = S.sc[SC_RATIO * W + s];
+  if (S.state[s] == SL_JAC_START) {
+    S.sc[SC_CHISQ * W + s] = chi0;
+    ratio = 1.0;
+    if (P.regul_any) {
+      const double pen = penalty_of(P, par);
+      if (pen > 0.1 * S.sc[SC_LMCHISQ * W + s]) ratio = 0.1 * chi0 / pen;
+    }
+    S.sc[SC_RATIO * W + s] = ratio;
+    S.it[s] = 0;
+    if (P.niter <= 0) {
+      S.state[s] = SL_RUN_END;
+      return;
+    }
+  }
+  double g[9];
+  for (int a = 0; a < n; a++) {
+    const int ia = P.free_idx[a];
+    for (int b = a; b < n; b++) {
+      const int ib = P.free_idx[b];
+      double h = H45[ia * 9 - ia * (ia + 1) / 2 + ib];
+      if (a == b && P.regul_any && P.regul[ia]) h += P.regul_weight[ia] * ratio;
+      S.hess[(size_t)(a * n + b) * W + s] = h;
+      S.hess[(size_t)(b * n + a) * W + s] = h;
+    }
+    g[a] = g9[ia];
+    if (P.regul_any && P.regul[ia]) g[a] -= (par[ia] - P.regul_value[ia]) * P.regul_weight[ia] * ratio;
+  }
+  for (int a = 0; a < n; a++) S.jvec[(size_t)a * W + s] = g[a];
+  S.cnt[1 * W + s]++;
+  S.sc[SC_DAMP * W + s] = P.damp;
+  S.tk[s] = 1;
+  S.state[s] = SL_TRIAL;
+}
+
+// The SVD solve of one trial step (SVD_solve_mem, Src/LM_FIT.c:400-469) and
+// its trial parameters (Par_update + bounds_check, Src/LM_FIT.c:511-516).
+//
+// The reference decomposes, at the first trial of an LM iteration, the
+// normal matrix H, and at every later trial the U factor the previous trial's
+// SVD left in its place.  Two exact identities let this skip V:
+//   * H is symmetric positive semi-definite, so its SVD has V = U and the
+//     truncated solve V W+ U^T g equals U W+ U^T g;
+//   * a U factor is orthogonal: its singular values are all 1 (nothing is
+//     truncated at any rung of the threshold ladder) and V W^-1 U^T g is
+//     U_prev^T g, clamped to +-0.5 as the ladder's last rung does.
+// So trial 1 runs the U-only decomposition of H and the ladder; trial k >= 2
+// uses the stored factor directly, and the decomposition that the reference
+// ran at trial k-1 (whose U only trial k+1 needs) is run here at trial k >= 3,
+// i.e. only when the iteration really goes on.
+//
+// WARP = false: one thread, its matrix a column of shared memory (stride
+// STR), w and rv1 likewise.  WARP = true: all 32 lanes of a warp, the matrix
+// row-major in the warp's shared memory, w and rv1 private to each lane (the
+// decomposition is gr_svd_u_warp, the rest runs redundantly in every lane and
+// lane 0 stores).  Returns the number of decompositions that hit the
+// 50-sweep limit.
+template <int STR, bool WARP>
+__device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int s, double *a,
+                                          double *w, double *rv1, int lane) {
+  const int W = S.W;
+  const int n = P.npar;
+  const int nthr = WARP ? 32 : 1;
+  int hits = 0;
+  int tk = S.tk[s];
+  if (WARP) tk = __shfl_sync(0xffffffffu, tk, 0);
+  double g[9], x[9];
+  for (int k = 0; k < n; k++) g[k] = S.jvec[(size_t)k * W + s];
+  for (int k = WARP ? lane : 0; k < n * n; k += nthr) a[k * STR] = S.hess[(size_t)k * W + s];
+  if (WARP) __syncwarp();
+  auto decompose = [&]() {
+    if constexpr (WARP)
+      return gr_svd_u_warp(a, n, w, lane);
+    else
+      return gr_svd_u<STR>(a, n, w, rv1);
+  };
+  if (tk == 1) {
+    hits += decompose();
+    double wmax = w[0];
+    for (int i = 1; i < n; i++) wmax = fmax(wmax, w[i * (WARP ? 1 : STR)]);
+    double thr = P.svd_thr;
+    double ug[9];  // U^T g
+    for (int j = 0; j < n; j++) {
+      double acc = 0.0;
+      for (int i = 0; i < n; i++) acc += a[(i * n + j) * STR] * g[i];
+      ug[j] = acc;
+    }
+    while (true) {
+      const double wthr = wmax * thr;
+      double tj[9];
+      for (int j = 0; j < n; j++) {
+        double &wr = w[j * (WARP ? 1 : STR)];
+        double wj = wr;
+        if (wj < wthr) {
+          wj = 0.0;
+          wr = 0.0;
+        }
+        tj[j] = wj > 1e-50 ? ug[j] / wj : 0.0;
+      }
+      bool inside = true;
+      for (int i = 0; i < n; i++) {
+        double acc = 0.0;
+        for (int j = 0; j < n; j++) acc += a[(i * n + j) * STR] * tj[j];
+        x[i] = acc;
+        if (acc > 0.5 || acc < -0.5) inside = false;
+      }
+      if (inside) break;
+      if (thr > 2e-3) {
+        for (int i = 0; i < n; i++) x[i] = x[i] > 0.5 ? 0.5 : (x[i] < -0.5 ? -0.5 : x[i]);
+        break;
+      }
+      thr *= 5.;
+    }
+  } else {
+    if (tk >= 3) hits += decompose();
+    for (int j = 0; j < n; j++) {
+      double acc = 0.0;
+      for (int i = 0; i < n; i++) acc += a[(i * n + j) * STR] * g[i];
+      x[j] = acc > 0.5 ? 0.5 : (acc < -0.5 ? -0.5 : acc);
+    }
+  }
+  if (tk != 2)
+    for (int k = WARP ? lane : 0; k < n * n; k += nthr) S.hess[(size_t)k * W + s] = a[k * STR];
+  if (!WARP || lane == 0) {
+    double ptmp[9], step_ia;
+    load9(S.par, W, s, ptmp);
+    for (int q = 0; q < n; q++) {
+      const int ia = P.free_idx[q];
+      step_ia = ia == 7 ? S.sc[SC_STEP7 * W + s] : P.step[ia];
+      ptmp[ia] += x[q] * step_ia;
+    }
+    bounds_fold(ptmp, P, S.sc[SC_L70 * W + s], S.sc[SC_L71 * W + s]);
+    store9(S.ptmp, W, s, ptmp);
+  }
+  if (WARP) __syncwarp();
+  return hits;
+}
+
+// After a trial synthesis (chi_new, when the slot is in SL_TRIAL) or at a run
+// that ended without one (SL_RUN_END): the accept / reject / convergence logic
+// (Src/LM_FIT.c:588-646), the end-of-run restart policy (INVERSION,
+// Src/LM_FIT.c:701-733) and, when the pixel is done, its result.  ROUNDS: the
+// slot goes on the next round's lists and a finished slot takes the next
+// pixel from the queue; otherwise (the tail kernel) it only changes state.
+// One thread per slot.
+template <bool ROUNDS>
+__device__ __forceinline__ void trial_transition(const DevPlan &P, const InvertArgs &A,
+                                                 const Slots &S, int s, int st, double chi_new,
+                                                 int next_parity, Tally &t) {
+  const int W = S.W;
+  bool end_run = (st == SL_RUN_END);
+  double par[9];
+  load9(S.par, W, s, par);
+  double *sc = S.sc;
+  double chisq = sc[SC_CHISQ * W + s];
+  double ratio = sc[SC_RATIO * W + s];
+  double lmchisq = sc[SC_LMCHISQ * W + s];
+  const long long pix = S.pix[s];
+  const double l70 = sc[SC_L70 * W + s], l71 = sc[SC_L71 * W + s];
+
+  if (!end_run) {
+    // --------- Trial_Synthesis (Src/LM_FIT.c:473-527) ---------
+    double ptmp[9];
+    load9(S.ptmp, W, s, ptmp);
+    lmchisq = chi_new;
+    S.had_trial[s] = 1;
+    S.cnt[2 * W + s]++;
+    t.trials++;
+    const double penalty = P.regul_any ? penalty_of(P, ptmp) : 0.0;
+    if (chi_new < chisq) {  // accept (Src/LM_FIT.c:591-615)
+      if (P.regul_any && penalty > 0.1 * lmchisq) ratio = 0.1 * chisq / penalty;
+#pragma unroll
+      for (int i = 0; i < 9; i++) par[i] = ptmp[i];
+      store9(S.par, W, s, par);
+      S.cnt[3 * W + s]++;
+      t.acc++;
+      const bool conv = ((chisq - chi_new) / chisq) < P.convg;
+      chisq = chi_new;
+      const int it = S.it[s] + 1;
+      S.it[s] = it;
+      if (conv || it >= P.niter) {
+        end_run = true;
+      } else {
+        S.state[s] = SL_JAC_NEXT;
+        if (ROUNDS) append_jac(S, next_parity, s);
+      }
+    } else {  // reject: grow the damping; past its limit the run ends
+      const double damp = sc[SC_DAMP * W + s] * P.lam_reject;
+      sc[SC_DAMP * W + s] = damp;
+      if (damp > P.lam_lim[1]) {
+        end_run = true;
+      } else {  // another trial, on the SVD's U factor (solve_slot)
+        S.tk[s]++;
+        if (ROUNDS) append_rej(S, next_parity, s);
+      }
+    }
+    sc[SC_CHISQ * W + s] = chisq;
+    sc[SC_RATIO * W + s] = ratio;
+    sc[SC_LMCHISQ * W + s] = lmchisq;
+  }
+
+  if (end_run) {
+    // ---------------- end of one LM_FIT run (INVERSION) ----------------
+    const double chisq_run = chisq / sc[SC_NORMP * W + s];
+    int run = S.run[s];
+    S.cnt[0 * W + s]++;
+    t.runs++;
+    double pbest[9];
+    double best = sc[SC_BEST * W + s];
+    const int first_run = A.init_par ? -1 : 0;
+    if (chisq_run < P.chisq_crit || run == first_run || chisq_run < best) {
+#pragma unroll
+      for (int i = 0; i < 9; i++) pbest[i] = par[i];
+      store9(S.pbest, W, s, pbest);
+      best = chisq_run;
+      sc[SC_BEST * W + s] = best;
+    } else {
+      load9(S.pbest, W, s, pbest);
+    }
+    bool stop = false;
+    // a learned start that meets chisq_criteria ends the pixel; otherwise
+    // the reference's schedule follows from run 0, keeping the best
+    if (run < 0 && chisq_run < P.chisq_crit) {
+      stop = true;
+      t.learned++;
+    }
+    if (chisq_run < P.chisq_crit && (run >= 4 || run == P.nruns * 4)) stop = true;
+    if (run >= P.nruns * 2 && best < P.chisq_crit * 2) stop = true;
+    run++;
+    S.run[s] = run;
+    if (!stop && run < P.nruns * 4) {
+      // Random_Jump (Src/LM_FIT.c:157-201)
+      double g[9];
+      load9(S.guess, W, s, g);
+      if (run == 0) {  // after a learned start: the reference's first run
+#pragma unroll
+        for (int i = 0; i < 9; i++) par[i] = g[i];
+      } else if (run < 4) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) par[i] = pbest[i];
+        par[2] = g[2] + kPi / 4. * run;
+      } else {
+        double z[8];
+        restart_draws(P.seed, pix, run, z);
+        par[0] = g[0] * (1 + 0.6 * z[0]);
+        par[1] = g[1] + kPi / 8. * z[1];
+        par[2] = g[2] + kPi / 4. * (run + 0.3 * z[2]);
+        par[3] = g[3] + 5. * z[3];
+        par[4] = pbest[4] * (1 + 0.2 * z[4]);
+        par[5] = g[5] + 0.1 * z[5];
+        par[6] = g[6] + 5 * z[6];
+        par[7] = pbest[7];
+        par[8] = g[8] + 0.1 * z[7];
+      }
+      if (run > 0) bounds_fold(par, P, l70, l71);
+      store9(S.par, W, s, par);
+      S.state[s] = SL_JAC_START;
+      if (ROUNDS) append_jac(S, next_parity, s);
+    } else {
+      // pixel done: best-fit profile, theta fold, HMI_REF, result
+      // (Src/LM_FIT.c:727-733, 791-799)
+      if (A.fitpar) store9_px(A.fitpar, pix, pbest);  // profiles: launch_fit after the batch
+      if (pbest[1] > kPi) pbest[1] -= kPi;
+      if (P.hmi_ref) {
+        pbest[2] += 0.5 * kPi;
+        if (pbest[2] > kPi) pbest[2] -= kPi;
+      }
+      double *r = A.res + (size_t)pix * 10;
+#pragma unroll
+      for (int i = 0; i < 9; i++) r[i] = pbest[i];
+      r[9] = best;
+      if (A.flags) A.flags[pix] = 1 | (S.had_trial[s] ? 2 : 0);
+      if (A.lastchi) A.lastchi[pix] = sc[SC_LMCHISQ * W + s];
+      if (A.counters) {
+        uint4 c4 = make_uint4(S.cnt[0 * W + s], S.cnt[1 * W + s], S.cnt[2 * W + s],
+                              S.cnt[3 * W + s]);
+        reinterpret_cast<uint4 *>(A.counters)[pix] = c4;
+      }
+      t.iter += S.cnt[1 * W + s];
+      if (ROUNDS && refill(P, A, S, s, t.valid)) {
+        append_jac(S, next_parity, s);
+      } else {
+        S.state[s] = SL_DONE;
+        t.busy_delta--;
+      }
+    }
+  }
+}
+
 }  // namespace detail
 
 using namespace detail;
@@ -226,79 +557,29 @@ __global__ void __launch_bounds__(kBlock, ME_JAC_MINB) jac_kernel(const __grid_c
   }
   const int count = S.jcount[parity];
   const int W = S.W;
-  const int n = P.npar;
   const int nl = P.nl;
-  unsigned long long t_jac = 0;
+  Tally t;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const int s = S.jlist[parity * W + i];
-    const long long pix = S.pix[s];
-    const double *pp = A.prof + (size_t)pix * 4 * nl;
+    const double *pp = A.prof + (size_t)S.pix[s] * 4 * nl;
     double par[9], step[9], sw[4];
     load9(S.par, W, s, par);
-#pragma unroll
-    for (int k = 0; k < 9; k++) step[k] = P.step[k];
-    step[7] = S.sc[SC_STEP7 * W + s];
-    const double isn = S.sc[SC_ISN * W + s];
-#pragma unroll
-    for (int k = 0; k < 4; k++) sw[k] = P.weights[k] * isn;
+    slot_weights(P, S, s, step, sw);
     double H45[45], g9[9];
     const double chi0 = deriv_pass<T>(P, K, rden, par, step, pp, sw, H45, g9);
-    t_jac++;
-    double ratio = S.sc[SC_RATIO * W + s];
-    if (S.state[s] == SL_JAC_START) {  // LM_FIT set-up (Src/LM_FIT.c:549-566)
-      S.sc[SC_CHISQ * W + s] = chi0;
-      ratio = 1.0;
-      if (P.regul_any) {
-        const double pen = penalty_of(P, par);
-        if (pen > 0.1 * S.sc[SC_LMCHISQ * W + s]) ratio = 0.1 * chi0 / pen;
-      }
-      S.sc[SC_RATIO * W + s] = ratio;
-      S.it[s] = 0;
-      if (P.niter <= 0) {
-        S.state[s] = SL_RUN_END;
-        continue;
-      }
-    }
-    // Hessian_Compute's free-parameter block + Get_Regul(matrix)
-    double g[9];
-    for (int a = 0; a < n; a++) {
-      const int ia = P.free_idx[a];
-      for (int b = a; b < n; b++) {
-        const int ib = P.free_idx[b];
-        double h = H45[ia * 9 - ia * (ia + 1) / 2 + ib];
-        if (a == b && P.regul_any && P.regul[ia]) h += P.regul_weight[ia] * ratio;
-        S.hess[(size_t)(a * n + b) * W + s] = h;
-        S.hess[(size_t)(b * n + a) * W + s] = h;
-      }
-      g[a] = g9[ia];
-      if (P.regul_any && P.regul[ia]) g[a] -= (par[ia] - P.regul_value[ia]) * P.regul_weight[ia] * ratio;
-    }
-    for (int a = 0; a < n; a++) S.jvec[(size_t)a * W + s] = g[a];
-    S.cnt[1 * W + s]++;
-    S.sc[SC_DAMP * W + s] = P.damp;
-    S.tk[s] = 1;
-    S.state[s] = SL_TRIAL;
+    t.jac++;
+    jac_store(P, S, s, par, chi0, H45, g9);
   }
-  if (A.totals && t_jac) atomicAdd(A.totals + 5, t_jac);
+  t.flush(A, S);
 }
 
 // ---------------------------------------------------------------------------
-// The SVD solve of the slots' trial steps (SVD_solve_mem, Src/LM_FIT.c:400-469)
-// and its trial parameters (Par_update + bounds_check, Src/LM_FIT.c:511-516).
-//
-// The reference decomposes, at the first trial of an LM iteration, the
-// normal matrix H, and at every later trial the U factor the previous trial's
-// SVD left in its place.  Two exact identities let this kernel skip V:
-//   * H is symmetric positive semi-definite, so its SVD has V = U and the
-//     truncated solve V W+ U^T g equals U W+ U^T g;
-//   * a U factor is orthogonal: its singular values are all 1 (nothing is
-//     truncated at any rung of the threshold ladder) and V W^-1 U^T g is
-//     U_prev^T g, clamped to +-0.5 as the ladder's last rung does.
-// So trial 1 runs the U-only decomposition of H and the ladder; trial k >= 2
-// uses the stored factor directly, and the decomposition that the reference
-// ran at trial k-1 (whose U only trial k+1 needs) is run here at trial k >= 3,
-// i.e. only when the iteration really goes on.  Each thread keeps its matrix
-// in its own column of shared memory.
+// The SVD solves of the slots' trial steps (solve_slot), one thread per slot,
+// its matrix in its own column of shared memory.  which = 0: the slots that
+// just built their normal matrix (the Jacobian list of this round, first
+// trials); which = 1: the slots going on after a rejected trial.  Two launches
+// keep the costly decompositions of H apart from the cheap ones of orthogonal
+// factors.
 // ---------------------------------------------------------------------------
 static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_constant__ DevPlan P,
                                                                const __grid_constant__ InvertArgs A,
@@ -310,78 +591,15 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_cons
   double *w = sm + 81 * kSvdBlock + t;
   double *rv1 = sm + 90 * kSvdBlock + t;
   const int W = S.W;
-  const int n = P.npar;
-  unsigned long long t_svdlim = 0;
-  // which = 0: the slots that just built their normal matrix (the Jacobian
-  // list of this round, first trials); which = 1: the slots going on after a
-  // rejected trial.  Two launches keep the costly decompositions of H apart
-  // from the cheap ones of orthogonal factors.
+  Tally tl;
   const int *list = which == 0 ? S.jlist + parity * W : S.rlist + parity * W;
   const int count = which == 0 ? S.jcount[parity] : S.rcount[parity];
   for (int i = blockIdx.x * kSvdBlock + t; i < count; i += gridDim.x * kSvdBlock) {
     const int s = list[i];
     if (S.state[s] != SL_TRIAL) continue;
-    const int tk = S.tk[s];
-    double g[9], x[9];
-    for (int k = 0; k < n; k++) g[k] = S.jvec[(size_t)k * W + s];
-    for (int k = 0; k < n * n; k++) a[k * kSvdBlock] = S.hess[(size_t)k * W + s];
-    if (tk == 1) {
-      t_svdlim += gr_svd_u<kSvdBlock>(a, n, w, rv1);
-      double wmax = w[0];
-      for (int i = 1; i < n; i++) wmax = fmax(wmax, w[i * kSvdBlock]);
-      double thr = P.svd_thr;
-      double ug[9];  // U^T g
-      for (int j = 0; j < n; j++) {
-        double acc = 0.0;
-        for (int i = 0; i < n; i++) acc += a[(i * n + j) * kSvdBlock] * g[i];
-        ug[j] = acc;
-      }
-      while (true) {
-        const double wthr = wmax * thr;
-        double tj[9];
-        for (int j = 0; j < n; j++) {
-          double wj = w[j * kSvdBlock];
-          if (wj < wthr) {
-            wj = 0.0;
-            w[j * kSvdBlock] = 0.0;
-          }
-          tj[j] = wj > 1e-50 ? ug[j] / wj : 0.0;
-        }
-        bool inside = true;
-        for (int i = 0; i < n; i++) {
-          double acc = 0.0;
-          for (int j = 0; j < n; j++) acc += a[(i * n + j) * kSvdBlock] * tj[j];
-          x[i] = acc;
-          if (acc > 0.5 || acc < -0.5) inside = false;
-        }
-        if (inside) break;
-        if (thr > 2e-3) {
-          for (int i = 0; i < n; i++) x[i] = x[i] > 0.5 ? 0.5 : (x[i] < -0.5 ? -0.5 : x[i]);
-          break;
-        }
-        thr *= 5.;
-      }
-    } else {
-      if (tk >= 3) t_svdlim += gr_svd_u<kSvdBlock>(a, n, w, rv1);
-      for (int j = 0; j < n; j++) {
-        double acc = 0.0;
-        for (int i = 0; i < n; i++) acc += a[(i * n + j) * kSvdBlock] * g[i];
-        x[j] = acc > 0.5 ? 0.5 : (acc < -0.5 ? -0.5 : acc);
-      }
-    }
-    if (tk != 2)
-      for (int k = 0; k < n * n; k++) S.hess[(size_t)k * W + s] = a[k * kSvdBlock];
-    double ptmp[9], step_ia;
-    load9(S.par, W, s, ptmp);
-    for (int q = 0; q < n; q++) {
-      const int ia = P.free_idx[q];
-      step_ia = ia == 7 ? S.sc[SC_STEP7 * W + s] : P.step[ia];
-      ptmp[ia] += x[q] * step_ia;
-    }
-    bounds_fold(ptmp, P, S.sc[SC_L70 * W + s], S.sc[SC_L71 * W + s]);
-    store9(S.ptmp, W, s, ptmp);
+    tl.svdlim += solve_slot<kSvdBlock, false>(P, S, s, a, w, rv1, 0);
   }
-  if (A.totals && t_svdlim) atomicAdd(A.totals + 6, t_svdlim);
+  tl.flush(A, S);
 }
 
 // ---------------------------------------------------------------------------
@@ -400,177 +618,235 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
   const int W = S.W;
   const int nl = P.nl;
   const int next_parity = parity ^ 1;
-  unsigned long long t_valid = 0, t_runs = 0, t_iter = 0, t_trials = 0, t_acc = 0, t_learned = 0;
-  int busy_delta = 0;
-
+  Tally t;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < W; s += gridDim.x * blockDim.x) {
-    int st = S.state[s];
+    const int st = S.state[s];
     if (st == SL_DONE) continue;
     if (st == SL_EMPTY) {
-      if (refill(P, A, S, s, t_valid)) {
-        busy_delta++;
+      if (refill(P, A, S, s, t.valid)) {
+        t.busy_delta++;
         append_jac(S, next_parity, s);
       } else {
         S.state[s] = SL_DONE;
       }
       continue;
     }
-    bool end_run = (st == SL_RUN_END);
-    double par[9];
-    load9(S.par, W, s, par);
-    double *sc = S.sc;
-    double chisq = sc[SC_CHISQ * W + s];
-    double ratio = sc[SC_RATIO * W + s];
-    double lmchisq = sc[SC_LMCHISQ * W + s];
-    const long long pix = S.pix[s];
-    const double *pp = A.prof + (size_t)pix * 4 * nl;
-    double step[9], sw[4];
-#pragma unroll
-    for (int k = 0; k < 9; k++) step[k] = P.step[k];
-    step[7] = sc[SC_STEP7 * W + s];
-    const double isn = sc[SC_ISN * W + s];
-#pragma unroll
-    for (int k = 0; k < 4; k++) sw[k] = P.weights[k] * isn;
-    const double l70 = sc[SC_L70 * W + s], l71 = sc[SC_L71 * W + s];
-
-    if (!end_run) {
-      // --------- Trial_Synthesis (Src/LM_FIT.c:473-527), after svd_kernel ---------
-      double ptmp[9];
+    double chi_new = 0.0;
+    if (st != SL_RUN_END) {  // Trial_Synthesis's synthesis, after svd_kernel
+      double ptmp[9], step[9], sw[4];
       load9(S.ptmp, W, s, ptmp);
-      const double chi_new = forward_pass<T>(P, K, rden, ptmp, step, pp, sw, nullptr);
-      lmchisq = chi_new;
-      S.had_trial[s] = 1;
-      S.cnt[2 * W + s]++;
-      t_trials++;
-      const double penalty = P.regul_any ? penalty_of(P, ptmp) : 0.0;
-      if (chi_new < chisq) {  // accept (Src/LM_FIT.c:591-615)
-        if (P.regul_any && penalty > 0.1 * lmchisq) ratio = 0.1 * chisq / penalty;
-#pragma unroll
-        for (int i = 0; i < 9; i++) par[i] = ptmp[i];
-        store9(S.par, W, s, par);
-        S.cnt[3 * W + s]++;
-        t_acc++;
-        const bool conv = ((chisq - chi_new) / chisq) < P.convg;
-        chisq = chi_new;
-        const int it = S.it[s] + 1;
-        S.it[s] = it;
-        if (conv || it >= P.niter) {
-          end_run = true;
-        } else {
-          S.state[s] = SL_JAC_NEXT;
-          append_jac(S, next_parity, s);
-        }
-      } else {  // reject: grow the damping; past its limit the run ends
-        const double damp = sc[SC_DAMP * W + s] * P.lam_reject;
-        sc[SC_DAMP * W + s] = damp;
-        if (damp > P.lam_lim[1]) {
-          end_run = true;
-        } else {  // another trial, on the SVD's U factor (svd_kernel)
-          S.tk[s]++;
-          append_rej(S, next_parity, s);
-        }
-      }
-      sc[SC_CHISQ * W + s] = chisq;
-      sc[SC_RATIO * W + s] = ratio;
-      sc[SC_LMCHISQ * W + s] = lmchisq;
+      slot_weights(P, S, s, step, sw);
+      chi_new = forward_pass<T>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl, sw,
+                                nullptr);
     }
+    trial_transition<true>(P, A, S, s, st, chi_new, next_parity, t);
+  }
+  t.flush(A, S);
+}
 
-    if (end_run) {
-      // ---------------- end of one LM_FIT run (INVERSION) ----------------
-      const double chisq_run = chisq / sc[SC_NORMP * W + s];
-      int run = S.run[s];
-      S.cnt[0 * W + s]++;
-      t_runs++;
-      double pbest[9];
-      double best = sc[SC_BEST * W + s];
-      const int first_run = A.init_par ? -1 : 0;
-      if (chisq_run < P.chisq_crit || run == first_run || chisq_run < best) {
-#pragma unroll
-        for (int i = 0; i < 9; i++) pbest[i] = par[i];
-        store9(S.pbest, W, s, pbest);
-        best = chisq_run;
-        sc[SC_BEST * W + s] = best;
-      } else {
-        load9(S.pbest, W, s, pbest);
+// ---------------------------------------------------------------------------
+// The tail: once the queue is empty and few pixels remain, rounds are bound by
+// the latency of one thread's synthesis and SVD.  finish_kernel takes the
+// remaining slots one per warp (an atomic cursor over the W slots) and runs
+// each to completion with the same per-slot steps: the synthesis's
+// wavelengths spread over the lanes (deriv_warp / forward_warp: per-point
+// terms staged in shared memory, every sum formed by one lane in the
+// thread-serial order), the SVD on gr_svd_u_warp, and the scalar transitions
+// in lane 0.  No lists, no refills.  The operations and their order are the
+// rounds'; only the compiler's contraction of multiply-adds may differ in
+// this kernel, so results agree to rounding (and, the LM being sensitive to
+// the last bit, some pixels then take another path, as under a one-ulp
+// change of their input).
+// ---------------------------------------------------------------------------
+template <class T>
+struct FinishSmem {
+  T tab[100];
+  T J[kBlock / 32][32 * 36];       // per warp: Jacobian rows of 32 points
+  double R[kBlock / 32][32 * 4];   // per warp: weighted residuals of 32 points
+  double a[kBlock / 32][81];       // per warp: the SVD's matrix
+  T rden[kBlock / 32][kRden];      // per warp: the Voigt reciprocal table
+};
+
+namespace detail {
+
+// voigt_prepare for a warp: one shared reciprocal table, entry n by lane n.
+template <class T>
+__device__ __forceinline__ void voigt_prepare_warp(VoigtK<T> &K, T y, T *rden, int lane) {
+  __syncwarp();
+  voigt_prepare<T>(K, y, nullptr, 1);
+  K.rden = rden;
+  K.rstride = 1;
+  if (sizeof(T) == sizeof(float) && lane < kRden)
+    rden[lane] = T(1) / (K.aa * T(lane * lane) + K.yy);
+  __syncwarp();
+}
+
+// deriv_pass across a warp.  H45 / g9 land in hg[0..53] (shared, all lanes
+// may read after the call); returns chi^2 / (4 nl) in every lane.
+template <class T>
+__device__ double deriv_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const double *par,
+                             const double *step, const double *prof, const double sw[4],
+                             int lane, T *stJ, double *stR, double *hg) {
+  SynthCall<T> c;
+  synth_setup<T>(c, par, P, step);
+  voigt_prepare_warp<T>(K, c.p5, rden, lane);
+  const int nl = P.nl;
+  const T tsw[4] = {T(sw[0]), T(sw[1]), T(sw[2]), T(sw[3])};
+  // this lane's sums: h entries lane and lane + 32 (upper triangle, row-major)
+  // and g entry lane
+  int i0 = 0, j0 = 0, i1 = 0, j1 = 0;
+  {
+    int idx = 0;
+    for (int i = 0; i < 9; i++)
+      for (int j = i; j < 9; j++, idx++) {
+        if (idx == lane) i0 = i, j0 = j;
+        if (idx == lane + 32) i1 = i, j1 = j;
       }
-      bool stop = false;
-      // a learned start that meets chisq_criteria ends the pixel; otherwise
-      // the reference's schedule follows from run 0, keeping the best
-      if (run < 0 && chisq_run < P.chisq_crit) {
-        stop = true;
-        t_learned++;
+  }
+  const bool has1 = lane + 32 < 45, hasg = lane < 9;
+  T h0 = T(0), h1 = T(0), gl = T(0);
+  double chi = 0.0;
+  for (int base = 0; base < nl; base += 32) {
+    const int iw = base + lane;
+    if (iw < nl) {
+      T syn[4], J[4][9];
+      me_point<T, true>(c, shift_w<T>(c, P, iw), K, tsw, syn, J);
+#pragma unroll
+      for (int s = 0; s < 4; s++) stR[lane * 4 + s] = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+#pragma unroll
+        for (int k = 0; k < 9; k++) stJ[lane * 36 + s * 9 + k] = J[s][k];
+    }
+    __syncwarp();
+    const int cnt = nl - base < 32 ? nl - base : 32;
+    for (int q = 0; q < cnt; q++) {
+      const double *rq = stR + q * 4;
+      const T *Jq = stJ + q * 36;
+      T r[4];
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        const double rd = rq[s];
+        chi += rd * rd;
+        r[s] = T(rd);
       }
-      if (chisq_run < P.chisq_crit && (run >= 4 || run == P.nruns * 4)) stop = true;
-      if (run >= P.nruns * 2 && best < P.chisq_crit * 2) stop = true;
-      run++;
-      S.run[s] = run;
-      if (!stop && run < P.nruns * 4) {
-        // Random_Jump (Src/LM_FIT.c:157-201)
-        double g[9];
-        load9(S.guess, W, s, g);
-        if (run == 0) {  // after a learned start: the reference's first run
+      h0 += Jq[i0] * Jq[j0] + Jq[9 + i0] * Jq[9 + j0] + Jq[18 + i0] * Jq[18 + j0] +
+            Jq[27 + i0] * Jq[27 + j0];
+      if (has1)
+        h1 += Jq[i1] * Jq[j1] + Jq[9 + i1] * Jq[9 + j1] + Jq[18 + i1] * Jq[18 + j1] +
+              Jq[27 + i1] * Jq[27 + j1];
+      if (hasg) gl -= Jq[lane] * r[0] + Jq[9 + lane] * r[1] + Jq[18 + lane] * r[2] + Jq[27 + lane] * r[3];
+    }
+    __syncwarp();
+  }
+  hg[lane] = (double)h0;
+  if (has1) hg[lane + 32] = (double)h1;
+  if (hasg) hg[45 + lane] = (double)gl;
+  __syncwarp();
+  return chi / (4.0 * nl);
+}
+
+// forward_pass across a warp (chi^2 only); every lane gets the result.
+template <class T>
+__device__ double forward_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const double *par,
+                               const double *step, const double *prof, const double sw[4],
+                               int lane, double *stR) {
+  SynthCall<T> c;
+  synth_setup<T>(c, par, P, step);
+  voigt_prepare_warp<T>(K, c.p5, rden, lane);
+  const T ones[4] = {T(1), T(1), T(1), T(1)};
+  const int nl = P.nl;
+  double chi = 0.0;
+  for (int base = 0; base < nl; base += 32) {
+    const int iw = base + lane;
+    if (iw < nl) {
+      T syn[4];
+      me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
 #pragma unroll
-          for (int i = 0; i < 9; i++) par[i] = g[i];
-        } else if (run < 4) {
+      for (int s = 0; s < 4; s++) stR[lane * 4 + s] = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+    }
+    __syncwarp();
+    const int cnt = nl - base < 32 ? nl - base : 32;
+    for (int q = 0; q < cnt; q++)
 #pragma unroll
-          for (int i = 0; i < 9; i++) par[i] = pbest[i];
-          par[2] = g[2] + kPi / 4. * run;
-        } else {
-          double z[8];
-          restart_draws(P.seed, pix, run, z);
-          par[0] = g[0] * (1 + 0.6 * z[0]);
-          par[1] = g[1] + kPi / 8. * z[1];
-          par[2] = g[2] + kPi / 4. * (run + 0.3 * z[2]);
-          par[3] = g[3] + 5. * z[3];
-          par[4] = pbest[4] * (1 + 0.2 * z[4]);
-          par[5] = g[5] + 0.1 * z[5];
-          par[6] = g[6] + 5 * z[6];
-          par[7] = pbest[7];
-          par[8] = g[8] + 0.1 * z[7];
-        }
-        if (run > 0) bounds_fold(par, P, l70, l71);
-        store9(S.par, W, s, par);
-        S.state[s] = SL_JAC_START;
-        append_jac(S, next_parity, s);
-      } else {
-        // pixel done: best-fit profile, theta fold, HMI_REF, result
-        // (Src/LM_FIT.c:727-733, 791-799)
-        if (A.fitpar) store9_px(A.fitpar, pix, pbest);  // profiles: launch_fit after the batch
-        if (pbest[1] > kPi) pbest[1] -= kPi;
-        if (P.hmi_ref) {
-          pbest[2] += 0.5 * kPi;
-          if (pbest[2] > kPi) pbest[2] -= kPi;
-        }
-        double *r = A.res + (size_t)pix * 10;
-#pragma unroll
-        for (int i = 0; i < 9; i++) r[i] = pbest[i];
-        r[9] = best;
-        if (A.flags) A.flags[pix] = 1 | (S.had_trial[s] ? 2 : 0);
-        if (A.lastchi) A.lastchi[pix] = sc[SC_LMCHISQ * W + s];
-        if (A.counters) {
-          uint4 c4 = make_uint4(S.cnt[0 * W + s], S.cnt[1 * W + s], S.cnt[2 * W + s],
-                                S.cnt[3 * W + s]);
-          reinterpret_cast<uint4 *>(A.counters)[pix] = c4;
-        }
-        t_iter += S.cnt[1 * W + s];
-        if (refill(P, A, S, s, t_valid)) {
-          append_jac(S, next_parity, s);
-        } else {
+      for (int s = 0; s < 4; s++) {
+        const double rd = stR[q * 4 + s];
+        chi += rd * rd;
+      }
+    __syncwarp();
+  }
+  return chi / (4.0 * nl);
+}
+
+}  // namespace detail
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) finish_kernel(const __grid_constant__ DevPlan P,
+                                                        const __grid_constant__ InvertArgs A,
+                                                        const __grid_constant__ Slots S,
+                                                        int *cursor) {
+  __shared__ FinishSmem<T> sm;
+  VoigtK<T> K;
+  voigt_block_setup<T>(K, P, sm.tab);
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  T *stJ = sm.J[wp];
+  double *stR = sm.R[wp];
+  double *a = sm.a[wp];
+  T *rden = sm.rden[wp];
+  const int W = S.W;
+  const int nl = P.nl;
+  const long long cap = slot_step_cap(P);
+  Tally t;
+  while (true) {
+    int s = 0;
+    if (lane == 0) s = atomicAdd(cursor, 1);
+    s = __shfl_sync(0xffffffffu, s, 0);
+    if (s >= W) break;
+    long long steps = 0;
+    while (true) {
+      __syncwarp();
+      // lane 0 made the last transition: its view of the state decides
+      const int st = __shfl_sync(0xffffffffu, S.state[s], 0);
+      if (st == SL_DONE || st == SL_EMPTY) break;
+      const long long pix = S.pix[s];
+      const double *pp = A.prof + (size_t)pix * 4 * nl;
+      if (++steps > cap) {  // cannot happen for a valid plan; ends the pixel with a flag
+        if (lane == 0) {
+          if (A.flags) A.flags[pix] = 8;
           S.state[s] = SL_DONE;
-          busy_delta--;
+          t.busy_delta--;
         }
+        __syncwarp();
+        break;
       }
+      double step[9], sw[4];
+      slot_weights(P, S, s, step, sw);
+      if (st == SL_JAC_START || st == SL_JAC_NEXT) {
+        double par[9];
+        load9(S.par, W, s, par);
+        const double chi0 = deriv_warp<T>(P, K, rden, par, step, pp, sw, lane, stJ, stR, stR);
+        if (lane == 0) {
+          double H45[45], g9[9];
+          for (int k = 0; k < 45; k++) H45[k] = stR[k];
+          for (int k = 0; k < 9; k++) g9[k] = stR[45 + k];
+          t.jac++;
+          jac_store(P, S, s, par, chi0, H45, g9);
+        }
+        continue;
+      }
+      double chi_new = 0.0;
+      if (st == SL_TRIAL) {
+        double w[9];
+        const int hits = solve_slot<1, true>(P, S, s, a, w, nullptr, lane);
+        if (lane == 0) t.svdlim += hits;
+        double ptmp[9];
+        load9(S.ptmp, W, s, ptmp);
+        chi_new = forward_warp<T>(P, K, rden, ptmp, step, pp, sw, lane, stR);
+      }
+      if (lane == 0) trial_transition<false>(P, A, S, s, st, chi_new, 0, t);
     }
   }
-  if (busy_delta) atomicAdd(S.busy, busy_delta);
-  if (A.totals) {
-    if (t_valid) atomicAdd(A.totals + 0, t_valid);
-    if (t_runs) atomicAdd(A.totals + 1, t_runs);
-    if (t_iter) atomicAdd(A.totals + 2, t_iter);
-    if (t_trials) atomicAdd(A.totals + 3, t_trials);
-    if (t_acc) atomicAdd(A.totals + 4, t_acc);
-    if (t_learned) atomicAdd(A.totals + 7, t_learned);
-  }
+  if (lane == 0) t.flush(A, S);
 }
 
 }  // namespace me

@@ -9,8 +9,12 @@ template __global__ void jac_kernel<float>(const __grid_constant__ DevPlan P,
 template __global__ void trial_kernel<float>(const __grid_constant__ DevPlan P,
                                               const __grid_constant__ InvertArgs A,
                                               const __grid_constant__ Slots S, int parity);
+template __global__ void finish_kernel<float>(const __grid_constant__ DevPlan P,
+                                              const __grid_constant__ InvertArgs A,
+                                              const __grid_constant__ Slots S, int *cursor);
 
-// which: 0 = jac_kernel, 1 = trial_kernel, 2 = svd_kernel (CTAs for a full device)
+// which: 0 = jac_kernel, 1 = trial_kernel, 2 = svd_kernel, 3 = finish_kernel
+// (CTAs for a full device)
 int round_grid_f32(int which, int device) {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -18,6 +22,8 @@ int round_grid_f32(int which, int device) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jac_kernel<float>, kBlock, 0);
   } else if (which == 1) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trial_kernel<float>, kBlock, 0);
+  } else if (which == 3) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finish_kernel<float>, kBlock, 0);
   } else {
     cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSvdSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, svd_kernel, kSvdBlock, kSvdSmem);
@@ -32,6 +38,12 @@ cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots 
   svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, 0);
   svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, 1);
   trial_kernel<float><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finish_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
+                              int grid, cudaStream_t st) {
+  finish_kernel<float><<<grid, kBlock, 0, st>>>(P, A, S, cursor);
   return cudaGetLastError();
 }
 

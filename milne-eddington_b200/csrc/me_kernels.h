@@ -64,6 +64,18 @@ struct Slots {
   int *busy;                 // slots holding a pixel
 };
 
+// An upper bound on the LM steps (syntheses with Jacobian + trial steps) of
+// one pixel: every run ends after num_iter accepted steps, each preceded by
+// at most the trials that take the damping from damp past lambda_limits[1]
+// (lambda_reject >= 1.5 and finite limits are checked on the host).
+__host__ __device__ inline long long slot_step_cap(const DevPlan &P) {
+  double tpi = ceil(log(P.lam_lim[1] / P.damp) / log(P.lam_reject)) + 2.0;
+  if (!(tpi >= 2.0)) tpi = 2.0;
+  if (tpi > 1e4) tpi = 1e4;
+  const double runs = 4.0 * P.nruns + 1.0;
+  return (long long)(runs * (P.niter * (tpi + 1.0) + 2.0) + 16.0);
+}
+
 // One batch (all device pointers).
 struct InvertArgs {
   const double *prof;          // [npix][4][nl]
@@ -93,7 +105,14 @@ int build_devplan(const struct me_config *cfg, const double *lambda, int nl, Dev
 // Records `msg` as the calling thread's me_last_error(); returns `code`.
 int record_error(int code, const char *msg);
 
+// CTAs for a full device: which = 0 jac_kernel, 1 trial_kernel, 2 svd_kernel,
+// 3 finish_kernel
 int round_grid(int precision, int which, int device);
+// The tail kernel: runs every slot still in flight to completion, one warp
+// per slot (slots taken through *cursor, zeroed by the caller).  Only when the
+// queue is exhausted (it does not refill).
+cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                          int *cursor, int grid, cudaStream_t st);
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                          int parity, const int grids[3], cudaStream_t st);
 // Best-fit profiles after a batch: synthesis at fitpar for the inverted

@@ -137,6 +137,16 @@ cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots 
 cudaError_t launch_round_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
                              const int grids[3], cudaStream_t st);
 
+cudaError_t launch_finish_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
+                              int grid, cudaStream_t st);
+cudaError_t launch_finish_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
+                              int grid, cudaStream_t st);
+cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                          int *cursor, int grid, cudaStream_t st) {
+  return precision == 1 ? launch_finish_f64(P, A, S, cursor, grid, st)
+                        : launch_finish_f32(P, A, S, cursor, grid, st);
+}
+
 int round_grid(int precision, int which, int device) {
   return precision == 1 ? round_grid_f64(which, device) : round_grid_f32(which, device);
 }

@@ -133,7 +133,7 @@ EXPORTED = [
     "me_invert_batch", "me_invert_batch_device", "me_synthesize", "me_synthesize_device",
     "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
     "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
-    "me_invert_batch_device_noalloc",
+    "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
@@ -199,6 +199,9 @@ def lib() -> ctypes.CDLL:
         L.me_plan_window.argtypes = [ctypes.c_void_p]
         L.me_plan_set_window.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_window.restype = None
+        L.me_plan_tail_slots.argtypes = [ctypes.c_void_p]
+        L.me_plan_set_tail_slots.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_tail_slots.restype = None
         L.me_invert_batch.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                       ctypes.POINTER(MeStats)]
         L.me_invert_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
@@ -345,6 +348,14 @@ class Plan:
     @window.setter
     def window(self, w: int):
         lib().me_plan_set_window(self._h, int(w))
+
+    @property
+    def tail_slots(self) -> int:
+        return lib().me_plan_tail_slots(self._h)
+
+    @tail_slots.setter
+    def tail_slots(self, n: int):
+        lib().me_plan_set_tail_slots(self._h, int(n))
 
     def set_initializer(self, init: Optional["Initializer"]):
         """Attaches a learned initialiser (None detaches); the plan does not own it."""
