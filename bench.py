@@ -236,19 +236,43 @@ def reference_arm(args):
     return 0
 
 
-def roofline_flops(stats, fc, nl):
-    """Algorithmic FLOPs of the LM work a batch did (reference algorithm,
-    counted per event with a counting scalar type: tests/golden/flop_counts.json)."""
-    def flops(c):
-        return c.get("add", 0) + c.get("mul", 0) + c.get("div", 0) + c.get("sqrt", 0)
+def _flops(c):
+    return c.get("add", 0) + c.get("mul", 0) + c.get("div", 0) + c.get("sqrt", 0)
 
-    first = stats["iterations"]
-    later = stats["trials"] - first
-    return (stats["trials"] * nl * (flops(fc["forward_per_lambda"]) + flops(fc["loss_per_lambda"]))
-            + first * flops(fc["svd_solve_normal_matrix"])
-            + later * flops(fc["svd_solve_orthogonal"])
-            + stats["jacobians"] * nl * (flops(fc["jacobian_per_lambda"])
-                                         + flops(fc["normal_equations_per_lambda"])))
+
+def event_flops(fc, nl, jacobians, trials):
+    """Algorithmic FLOPs of LM work (the reference algorithm, counted per event
+    with a counting scalar type: tests/golden/flop_counts.json) split by the
+    kernel that does it: synthesis with Jacobian + normal equations per
+    Jacobian; an SVD solve of H for the first trial after each Jacobian and of
+    an orthogonal U factor for every later trial; a forward synthesis + chi^2
+    per trial."""
+    first = jacobians
+    later = max(trials - first, 0)
+    return {"jac": jacobians * nl * (_flops(fc["jacobian_per_lambda"])
+                                     + _flops(fc["normal_equations_per_lambda"])),
+            "svd": first * _flops(fc["svd_solve_normal_matrix"])
+            + later * _flops(fc["svd_solve_orthogonal"]),
+            "trial": trials * nl * (_flops(fc["forward_per_lambda"])
+                                    + _flops(fc["loss_per_lambda"]))}
+
+
+def kernel_rooflines(st, fc, nl, peak):
+    """Per-kernel algorithmic FLOP/s from a profiled batch (me_plan_set_profiling):
+    the round kernels over the events the rounds did, the tail kernel over
+    the rest."""
+    tj, tt = st["tail_jacobians"], st["tail_trials"]
+    rounds = event_flops(fc, nl, st["jacobians"] - tj, st["trials"] - tt)
+    tail = event_flops(fc, nl, tj, tt)
+    out = {}
+    for name, ms, fl in (("jac_kernel", st["jac_ms"], rounds["jac"]),
+                         ("svd_kernel", st["svd_ms"], rounds["svd"]),
+                         ("trial_kernel", st["trial_ms"], rounds["trial"]),
+                         ("finish_kernel", st["tail_ms"], sum(tail.values()))):
+        if ms > 0:
+            tf = fl / (ms / 1e3) / 1e12
+            out[name] = {"ms": ms, "algorithmic_flop": fl, "tflops": tf, "frac": tf / peak}
+    return out
 
 
 def param_errors(res, ref):
@@ -346,8 +370,10 @@ def main():
     # ---- the learned initialiser: trained on the GPU for this line and grid
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    torch.cuda.nvtx.range_push("train")
     init = me_b200.Initializer.train(plan, samples=args.train_samples, epochs=args.train_epochs,
                                      seed=20240607 + 7919 * rank)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     plan.set_initializer(init)
@@ -359,21 +385,35 @@ def main():
         return plain.invert_device(prof.data_ptr(), npix, res_plain.data_ptr(), 0,
                                    stream.cuda_stream)
 
+    nvtx = torch.cuda.nvtx  # ranges name the phases for ncu --nvtx-include
+    nvtx.range_push("warmup")
     for _ in range(args.warmup):
         step()
+    nvtx.range_pop()
     clk = ClockSampler(local)
+    nvtx.range_push("timed")
     elapsed, stats = timed_steps(torch, step, args.steps, stream, dist, clk)
+    nvtx.range_pop()
     step_s = elapsed / args.steps
     last = stats[-1]
     kernel_ms = statistics.mean(s["kernel_ms"] for s in stats)
     init_ms = statistics.mean(s["init_ms"] for s in stats)
+
+    # ---- one more step with per-kernel CUDA events (outside the timed region)
+    nvtx.range_push("profiled")
+    plan.set_profiling(True)
+    prof_stats = step()
+    plan.set_profiling(False)
+    nvtx.range_pop()
 
     # ---- the plain LM with the reference's restarts, same map and GPU
     plain_steps = args.steps if args.plain_steps < 0 else args.plain_steps
     plain_s, plain_last = None, None
     if plain_steps > 0:
         step_plain()  # warm-up (slot buffers, caches)
+        nvtx.range_push("plain")
         el, pst = timed_steps(torch, step_plain, plain_steps, stream, dist)
+        nvtx.range_pop()
         plain_s, plain_last = el / plain_steps, pst[-1]
 
     # ---- end to end through the host entry point (pinned host buffers)
@@ -417,12 +457,15 @@ def main():
         frac, ratio_q = conv(res_np)
         frac_plain, ratio_q_plain = conv(res_plain_np) if plain_s else (None, None)
         fc = json.load(open(os.path.join(ROOT, "tests", "golden", "flop_counts.json")))[name]
-        alg = roofline_flops(last, fc, nl)
+        peak = fp32_peak_tflops(torch)
+        kr = kernel_rooflines(prof_stats, fc, nl, peak)
+        top = max(kr, key=lambda k: kr[k]["ms"])
+        alg_step = sum(event_flops(fc, nl, last["jacobians"], last["trials"]).values())
         out = {"frac": frac, "ratio_q": ratio_q, "frac_plain": frac_plain,
                "ratio_q_plain": ratio_q_plain, "cpu_value": nb / base_dt, "nb": nb,
-               "base_kind": base_kind, "cores": cores, "alg": alg,
-               "achieved": alg / (kernel_ms / 1e3) / 1e12, "clk": clk.summary(),
-               "peak": fp32_peak_tflops(torch),
+               "base_kind": base_kind, "cores": cores, "kernels": kr, "top": top,
+               "alg_step": alg_step, "step_tflops": alg_step / (kernel_ms / 1e3) / 1e12,
+               "clk": clk.summary(), "peak": peak,
                "err_vs_ref": param_errors(res_np[idx][valid], ref_res[valid]),
                "err_vs_truth": param_errors(res_np, par_true),
                "err_vs_truth_ref": param_errors(ref_res[valid], par_true[idx][valid])}
@@ -475,13 +518,20 @@ def main():
                        "ref_param_err_vs_truth_median_p99": out["err_vs_truth_ref"]},
             "gpu_launches": int(sum(s["launches"] for s in stats)),
             "e2e": None, "clocks": out["clk"],
-            "roofline": {"bound": "fp32", "achieved": out["achieved"], "peak": out["peak"],
-                         "unit": "TFLOP/s", "frac": out["achieved"] / out["peak"],
+            "roofline": {"bound": "fp32", "kernel": out["top"],
+                         "achieved": out["kernels"][out["top"]]["tflops"],
+                         "peak": out["peak"], "unit": "TFLOP/s",
+                         "frac": out["kernels"][out["top"]]["frac"],
                          "traffic": None,
-                         "note": "algorithmic FLOPs of the reference algorithm (counted with a "
-                                 "counting scalar type) / LM round-kernel time; peak = FP32 "
-                                 "FFMA throughput measured with cuBLAS SGEMM (TF32 off)",
-                         "algorithmic_flop_per_launch": out["alg"]},
+                         "note": "dominant kernel by device time in a profiled step (CUDA "
+                                 "events around every launch): algorithmic FLOPs of the "
+                                 "reference algorithm for the events it ran (counted with a "
+                                 "counting scalar type) / its time; peak = FP32 FFMA rate "
+                                 "measured in this run with cuBLAS SGEMM, TF32 off "
+                                 "(MEASURED_PEAKS.json has no FP32 figure)",
+                         "kernels": out["kernels"],
+                         "step_algorithmic_tflops": out["step_tflops"],
+                         "algorithmic_flop_per_step": out["alg_step"]},
             "cpu_baseline": {"value": out["cpu_value"], "unit": UNIT, "cores": out["cores"],
                              "kind": out["base_kind"],
                              "sample": f"{out['nb']} seeded pixels of the map, "

@@ -117,6 +117,11 @@ typedef struct me_stats {
   double h2d_ms, d2h_ms;   /* host<->device copy time (host entry point)   */
   double init_ms;          /* device time of the learned initialiser        */
   long long learned_done;  /* pixels that ended after the learned start     */
+  /* with me_plan_set_profiling(plan, 1): device time per kernel (CUDA events
+   * around every launch) and the trial steps / syntheses with Jacobian that
+   * the tail kernel did; zeros otherwise */
+  double jac_ms, svd_ms, trial_ms, tail_ms;
+  long long tail_trials, tail_jacobians;
 } me_stats;
 
 typedef struct me_plan me_plan;
@@ -173,6 +178,9 @@ void me_plan_set_window(me_plan *plan, int window);
  * multiply-adds, and a much shorter tail.  -1 (default): two waves of the
  * tail kernel's warps on this device; 0: rounds only. */
 int me_plan_tail_slots(const me_plan *plan);
+/* Records CUDA events around every inversion launch and reports per-kernel
+ * device time in me_stats (off by default; costs a little host time). */
+void me_plan_set_profiling(me_plan *plan, int on);
 void me_plan_set_tail_slots(me_plan *plan, int slots);
 
 /* Inverts npix pixels.  prof: host [npix][4][nl]; res: host [npix][10];

@@ -109,6 +109,14 @@ struct me_plan {
   // finishes the batch (-1: two waves of its warps; 0: rounds only)
   int tail_slots = -1;
   long long finish_launches = 0;  // tail-kernel launches of the current batch
+  // per-kernel device time (me_plan_set_profiling): events recorded around
+  // every launch of a batch, read when it ends
+  bool profile = false;
+  std::vector<cudaEvent_t> evpool;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, size_t>> ev_marks;  // (kind, first event): 0 = round, 1 = tail
+  unsigned long long tail_start_totals[8] = {};
+  bool tail_seen = false;
   int poll_rounds = 8;     // rounds launched between checks of the queue
   unsigned long long *h_poll = nullptr;  // pinned: next, busy
   long long rounds_last = 0;
@@ -301,6 +309,7 @@ extern "C" void me_plan_destroy(me_plan *p) {
   if (p->h_poll) cudaFreeHost(p->h_poll);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
+  for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
 }
@@ -324,6 +333,10 @@ extern "C" void me_plan_set_grid(me_plan *p, int grid) {
 extern "C" int me_plan_window(const me_plan *p) { return p ? p->window : 0; }
 extern "C" void me_plan_set_window(me_plan *p, int window) {
   if (p && window >= 0) p->window = window;
+}
+
+extern "C" void me_plan_set_profiling(me_plan *p, int on) {
+  if (p) p->profile = on != 0;
 }
 
 extern "C" int me_plan_tail_slots(const me_plan *p) { return p ? p->tail_slots : 0; }
@@ -397,6 +410,18 @@ int ensure_slots(me_plan *p, int W, me::Slots &S) {
   return ME_OK;
 }
 
+// n consecutive events from the plan's pool (profiling only).
+cudaEvent_t *take_events(me_plan *p, size_t n) {
+  while (p->evpool.size() < p->ev_used + n) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    p->evpool.push_back(e);
+  }
+  cudaEvent_t *ev = p->evpool.data() + p->ev_used;
+  p->ev_used += n;
+  return ev;
+}
+
 // Runs one queue (A.count items) to completion: rounds of jac_kernel,
 // svd_kernel and trial_kernel on the plan's slots while the queue feeds them,
 // then, once it is empty and at most tail_slots pixels remain, finish_kernel
@@ -423,7 +448,13 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     if ((double)rounds > round_cap)
       return fail(ME_ERR_TIMEOUT, "inversion rounds exceeded their bound");
     for (int r = 0; r < p->poll_rounds; r++) {
-      CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st));
+      cudaEvent_t *ev = nullptr;
+      if (p->profile) {
+        const size_t first = p->ev_used;
+        ev = take_events(p, 5);
+        if (ev) p->ev_marks.push_back({0, first});
+      }
+      CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st, ev));
       parity ^= 1;
       rounds++;
     }
@@ -439,7 +470,22 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
       int *cursor = S.busy + 1;
       CK(cudaMemsetAsync(cursor, 0, sizeof(int), st));
       const int g = std::min(p->grid_fin, (busy + me::kBlock / 32 - 1) / (me::kBlock / 32));
+      cudaEvent_t *ev = nullptr;
+      if (p->profile) {
+        // event counts the rounds did, to attribute the rest to the tail
+        CK(cudaMemcpyAsync(p->tail_start_totals, A.totals, sizeof(p->tail_start_totals),
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        p->tail_seen = true;
+        const size_t first = p->ev_used;
+        ev = take_events(p, 2);
+        if (ev) {
+          p->ev_marks.push_back({1, first});
+          CK(cudaEventRecord(ev[0], st));
+        }
+      }
       CK(me::launch_finish(p->precision, p->P, A, S, cursor, std::max(g, 1), st));
+      if (ev) CK(cudaEventRecord(ev[1], st));
       p->finish_launches++;
       break;
     }
@@ -497,6 +543,9 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
 
   long long rounds = 0, rounds_total = 0;
   p->finish_launches = 0;
+  p->ev_used = 0;
+  p->ev_marks.clear();
+  p->tail_seen = false;
   CK(cudaEventRecord(p->ev0, st));
   int rc = run_queue(p, A, st, rounds);
   if (rc) return rc;
@@ -595,6 +644,28 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     stats->kernel_ms = kernel_ms;
     stats->init_ms = init_ms;
     stats->learned_done = (long long)tot[7];
+    if (p->profile) {
+      // per-kernel device time from the events of every launch of the batch
+      for (const auto &m : p->ev_marks) {
+        cudaEvent_t *e = p->evpool.data() + m.second;
+        float t = 0.f;
+        if (m.first == 0) {
+          cudaEventElapsedTime(&t, e[0], e[1]);
+          stats->jac_ms += t;
+          cudaEventElapsedTime(&t, e[1], e[3]);
+          stats->svd_ms += t;
+          cudaEventElapsedTime(&t, e[3], e[4]);
+          stats->trial_ms += t;
+        } else {
+          cudaEventElapsedTime(&t, e[0], e[1]);
+          stats->tail_ms += t;
+        }
+      }
+      if (p->tail_seen) {
+        stats->tail_trials = (long long)(tot[3] - p->tail_start_totals[3]);
+        stats->tail_jacobians = (long long)(tot[5] - p->tail_start_totals[5]);
+      }
+    }
   }
   return ME_OK;
 }

@@ -33,11 +33,16 @@ int round_grid_f32(int which, int device) {
 }
 
 cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                           const int grids[3], cudaStream_t st) {
+                           const int grids[3], cudaStream_t st, cudaEvent_t *ev) {
+  if (ev) cudaEventRecord(ev[0], st);
   jac_kernel<float><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
+  if (ev) cudaEventRecord(ev[1], st);
   svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, 0);
+  if (ev) cudaEventRecord(ev[2], st);
   svd_kernel<<<grids[2], kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, 1);
+  if (ev) cudaEventRecord(ev[3], st);
   trial_kernel<float><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
+  if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }
 

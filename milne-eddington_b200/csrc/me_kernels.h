@@ -113,8 +113,12 @@ int round_grid(int precision, int which, int device);
 // queue is exhausted (it does not refill).
 cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                           int *cursor, int grid, cudaStream_t st);
+// One round: jac_kernel, svd_kernel (first trials), svd_kernel (later
+// trials), trial_kernel.  ev (nullable): 5 events recorded before, between
+// and after the four launches (per-kernel device time when profiling).
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
-                         int parity, const int grids[3], cudaStream_t st);
+                         int parity, const int grids[3], cudaStream_t st,
+                         cudaEvent_t *ev = nullptr);
 // Best-fit profiles after a batch: synthesis at fitpar for the inverted
 // pixels (flags bit 0), zeros for the skipped ones.
 cudaError_t launch_fit(int precision, const DevPlan &P, const double *d_fitpar,

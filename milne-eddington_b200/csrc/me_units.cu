@@ -133,9 +133,9 @@ __global__ void init_guess_kernel(const DevPlan P, const double *prof, long long
 int round_grid_f32(int which, int device);
 int round_grid_f64(int which, int device);
 cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                             const int grids[3], cudaStream_t st);
+                             const int grids[3], cudaStream_t st, cudaEvent_t *ev);
 cudaError_t launch_round_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                             const int grids[3], cudaStream_t st);
+                             const int grids[3], cudaStream_t st, cudaEvent_t *ev);
 
 cudaError_t launch_finish_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
                               int grid, cudaStream_t st);
@@ -152,9 +152,9 @@ int round_grid(int precision, int which, int device) {
 }
 
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
-                         int parity, const int grids[3], cudaStream_t st) {
-  return precision == 1 ? launch_round_f64(P, A, S, parity, grids, st)
-                        : launch_round_f32(P, A, S, parity, grids, st);
+                         int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev) {
+  return precision == 1 ? launch_round_f64(P, A, S, parity, grids, st, ev)
+                        : launch_round_f32(P, A, S, parity, grids, st, ev);
 }
 
 cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,

@@ -119,6 +119,12 @@ class MeStats(ctypes.Structure):
         ("d2h_ms", ctypes.c_double),
         ("init_ms", ctypes.c_double),
         ("learned_done", ctypes.c_longlong),
+        ("jac_ms", ctypes.c_double),
+        ("svd_ms", ctypes.c_double),
+        ("trial_ms", ctypes.c_double),
+        ("tail_ms", ctypes.c_double),
+        ("tail_trials", ctypes.c_longlong),
+        ("tail_jacobians", ctypes.c_longlong),
     ]
 
     def as_dict(self):
@@ -134,6 +140,7 @@ EXPORTED = [
     "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
     "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
+    "me_plan_set_profiling",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
@@ -202,6 +209,8 @@ def lib() -> ctypes.CDLL:
         L.me_plan_tail_slots.argtypes = [ctypes.c_void_p]
         L.me_plan_set_tail_slots.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_tail_slots.restype = None
+        L.me_plan_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_profiling.restype = None
         L.me_invert_batch.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                       ctypes.POINTER(MeStats)]
         L.me_invert_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
@@ -356,6 +365,10 @@ class Plan:
     @tail_slots.setter
     def tail_slots(self, n: int):
         lib().me_plan_set_tail_slots(self._h, int(n))
+
+    def set_profiling(self, on: bool = True):
+        """Per-kernel device time in the stats (CUDA events around every launch)."""
+        lib().me_plan_set_profiling(self._h, int(bool(on)))
 
     def set_initializer(self, init: Optional["Initializer"]):
         """Attaches a learned initialiser (None detaches); the plan does not own it."""
