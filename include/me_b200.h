@@ -175,9 +175,21 @@ void me_plan_set_window(me_plan *plan, int window);
  * taken from the queue, the remaining ones are run to the end one warp per
  * pixel (their synthesis spread over the lanes) instead of one LM step per
  * launch round: the same arithmetic up to the compiler's contraction of
- * multiply-adds, and a much shorter tail.  -1 (default): two waves of the
- * tail kernel's warps on this device; 0: rounds only. */
+ * multiply-adds, and a much shorter tail.  -1 (default): half a wave of the
+ * tail kernel's warps on this device (~900 on a B200); 0: rounds only. */
 int me_plan_tail_slots(const me_plan *plan);
+/* Once every pixel of a batch has been taken from the queue, the LM rounds
+ * give each pixel still in flight a group of lanes (2, 4, ... up to this
+ * power of two, enough to fill about one wave of the Jacobian kernel) that
+ * splits its synthesis and SVD; 1 keeps one thread per pixel.  Default 32.
+ * Results agree with one thread per pixel to rounding. */
+int me_plan_max_group(const me_plan *plan);
+void me_plan_set_max_group(me_plan *plan, int lanes);
+/* Lanes per 9x9 SVD in the LM rounds that still feed from the queue (1, 2, 4
+ * or 8); more lanes cut the decomposition's latency, fewer keep more of them
+ * in flight.  Default 1. */
+int me_plan_svd_lanes(const me_plan *plan);
+void me_plan_set_svd_lanes(me_plan *plan, int lanes);
 /* Records CUDA events around every inversion launch and reports per-kernel
  * device time in me_stats (off by default; costs a little host time). */
 void me_plan_set_profiling(me_plan *plan, int on);

@@ -106,8 +106,12 @@ struct me_plan {
       d_slot_list, d_slot_small;
   int grid_jac = 0, grid_trial = 0, grid_svd = 0, grid_fin = 0;
   // pixels in flight at or below which, with the queue empty, the tail kernel
-  // finishes the batch (-1: two waves of its warps; 0: rounds only)
+  // finishes the batch (-1: half a wave of its warps; 0: rounds only)
   int tail_slots = -1;
+  // largest lane group per slot in the rounds once the queue is empty (1: one
+  // thread per slot throughout)
+  int max_group = 32;
+  int svd_lanes = 1;  // lanes per matrix of the SVD launches in the full rounds
   long long finish_launches = 0;  // tail-kernel launches of the current batch
   // per-kernel device time (me_plan_set_profiling): events recorded around
   // every launch of a batch, read when it ends
@@ -339,6 +343,19 @@ extern "C" void me_plan_set_profiling(me_plan *p, int on) {
   if (p) p->profile = on != 0;
 }
 
+extern "C" int me_plan_svd_lanes(const me_plan *p) { return p ? p->svd_lanes : 0; }
+extern "C" void me_plan_set_svd_lanes(me_plan *p, int lanes) {
+  if (p) p->svd_lanes = lanes >= 8 ? 8 : lanes >= 4 ? 4 : lanes >= 2 ? 2 : 1;
+}
+
+extern "C" int me_plan_max_group(const me_plan *p) { return p ? p->max_group : 0; }
+extern "C" void me_plan_set_max_group(me_plan *p, int lanes) {
+  if (!p) return;
+  int g = 1;
+  while (g * 2 <= lanes && g < 32) g *= 2;
+  p->max_group = g;
+}
+
 extern "C" int me_plan_tail_slots(const me_plan *p) { return p ? p->tail_slots : 0; }
 extern "C" void me_plan_set_tail_slots(me_plan *p, int slots) {
   if (p) p->tail_slots = slots < 0 ? -1 : slots;
@@ -439,8 +456,13 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
   int grids[3];
   grids[0] = std::min(p->grid_jac, (W + me::kBlock - 1) / me::kBlock);
   grids[1] = std::min(p->grid_trial, (W + me::kBlock - 1) / me::kBlock);
-  grids[2] = std::min(p->grid_svd, (W + me::kSvdBlock - 1) / me::kSvdBlock);
+  grids[2] = p->svd_lanes > 1
+                 ? (int)std::min<long long>(p->grid_trial,
+                                            ((long long)W * p->svd_lanes + me::kBlock - 1) / me::kBlock)
+                 : std::min(p->grid_svd, (W + me::kSvdBlock - 1) / me::kSvdBlock);
   int parity = 0;
+  int group = 1;              // lanes per slot of the next rounds
+  int ggrids[3] = {1, 1, 1};  // their grids
   rounds = 0;
   // every slot step is one round: a bound no valid batch reaches
   const double round_cap = (double)me::slot_step_cap(p->P) * (double)((A.count + W - 1) / W + 1);
@@ -454,7 +476,10 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
         ev = take_events(p, 5);
         if (ev) p->ev_marks.push_back({0, first});
       }
-      CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st, ev));
+      if (group > 1)
+        CK(me::launch_round_grp(p->precision, group, p->P, A, S, parity, ggrids, st, ev));
+      else
+        CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st, ev, p->svd_lanes));
       parity ^= 1;
       rounds++;
     }
@@ -464,7 +489,20 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     const int busy = *reinterpret_cast<int *>(p->h_poll + 1);
     const bool drained = p->h_poll[0] >= (unsigned long long)A.count;
     if (drained && busy == 0) break;
-    const int tail = p->tail_slots < 0 ? 2 * p->grid_fin * (me::kBlock / 32) : p->tail_slots;
+    if (drained && p->max_group > 1) {
+      // the queue is empty: give each slot in flight as many lanes as fill
+      // about one wave of the Jacobian kernel on the whole device
+      const long long wave = (long long)p->grid_jac * me::kBlock;
+      int g = 1;
+      while (g < p->max_group && (long long)busy * g * 2 <= wave) g *= 2;
+      group = g;
+      const long long need = ((long long)W * g + me::kBlock - 1) / me::kBlock;
+      ggrids[0] = (int)std::min<long long>(p->grid_jac, need);
+      ggrids[1] = (int)std::min<long long>(p->grid_trial, need);
+      ggrids[2] = (int)std::min<long long>(p->grid_trial, need);
+    }
+    // default: half a wave of the tail kernel's warps
+    const int tail = p->tail_slots < 0 ? p->grid_fin * (me::kBlock / 32) / 2 : p->tail_slots;
     if (drained && busy <= tail) {
       // the queue is empty and few pixels remain: one warp per pixel to the end
       int *cursor = S.busy + 1;

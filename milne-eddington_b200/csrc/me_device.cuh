@@ -1324,15 +1324,21 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
 #undef R_
 }
 
-// gr_svd_u with the matrix in the shared memory of one warp (row-major,
-// stride 1) and its vector loops spread over the lanes: lane j owns column j
-// (or row j) of each update, every sum is formed by one lane in gr_svd_u's
-// order, and the scalar recurrences (w, rv1, the QR chase) run redundantly in
-// every lane on private copies.  The arithmetic is gr_svd_u's operation for
-// operation, so the results are the same bits; only the latency changes.
-// w [n] is private to the lane.  All 32 lanes call it.
-static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, int lane) {
+// gr_svd_u for a group of G consecutive lanes of a warp (G a power of two,
+// `mask` the group's lanes), the matrix row-major in the group's shared
+// memory (stride 1): the vector loops of each update are spread over the
+// lanes (lane t takes rows or columns t, t + G, ... of it), every sum is
+// formed by one lane in gr_svd_u's order, and the scalar recurrences (w, rv1,
+// the QR chase) run redundantly in every lane on private copies.  The
+// arithmetic is gr_svd_u's operation for operation; only the latency
+// changes.  w [n] is private to the lane.  All lanes of the group call it.
+template <int G>
+__device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, unsigned mask) {
 #define A_(i, j) a[(i) * n + (j)]
+#define GSYNC()                  \
+  do {                           \
+    if (G > 1) __syncwarp(mask); \
+  } while (0)
   const int m = n;
   int l = 0, nm = 0;
   double anorm = 0., c, f, g = 0., h, s, scale = 0., x, y, z;
@@ -1352,19 +1358,19 @@ static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, in
       f = A_(i, i) * is;
       g = f >= 0 ? -sqrt(s) : sqrt(s);
       h = f * g - s;
-      __syncwarp();
-      if (lane >= i && lane < m) A_(lane, i) = lane == i ? f - g : A_(lane, i) * is;
-      __syncwarp();
+      GSYNC();
+      for (int k = i + lane; k < m; k += G) A_(k, i) = k == i ? f - g : A_(k, i) * is;
+      GSYNC();
       const double ih = 1.0 / h;
-      if (lane >= l && lane < n) {
+      for (int j = l + lane; j < n; j += G) {
         double sj = 0.0;
-        for (int k = i; k < m; k++) sj += A_(k, i) * A_(k, lane);
+        for (int k = i; k < m; k++) sj += A_(k, i) * A_(k, j);
         const double fj = sj * ih;
-        for (int k = i; k < m; k++) A_(k, lane) += fj * A_(k, i);
+        for (int k = i; k < m; k++) A_(k, j) += fj * A_(k, i);
       }
-      __syncwarp();
-      if (lane >= i && lane < m) A_(lane, i) *= scale;
-      __syncwarp();
+      GSYNC();
+      for (int k = i + lane; k < m; k += G) A_(k, i) *= scale;
+      GSYNC();
     }
     w[i] = scale * g;
     g = s = scale = 0.0;
@@ -1382,17 +1388,17 @@ static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, in
         const double ih = 1.0 / h;
         // the scaled row i (with f - g at l) and rv1 = row / h, in every lane
         for (int k = l; k < n; k++) rv1[k] = (k == l ? f - g : A_(i, k) * is) * ih;
-        __syncwarp();
-        if (lane >= l && lane < n) A_(i, lane) = lane == l ? f - g : A_(i, lane) * is;
-        __syncwarp();
-        if (lane >= l && lane < m) {
+        GSYNC();
+        for (int k = l + lane; k < n; k += G) A_(i, k) = k == l ? f - g : A_(i, k) * is;
+        GSYNC();
+        for (int j = l + lane; j < m; j += G) {
           double sj = 0.0;
-          for (int k = l; k < n; k++) sj += A_(lane, k) * A_(i, k);
-          for (int k = l; k < n; k++) A_(lane, k) += sj * rv1[k];
+          for (int k = l; k < n; k++) sj += A_(j, k) * A_(i, k);
+          for (int k = l; k < n; k++) A_(j, k) += sj * rv1[k];
         }
-        __syncwarp();
-        if (lane >= l && lane < n) A_(i, lane) *= scale;
-        __syncwarp();
+        GSYNC();
+        for (int k = l + lane; k < n; k += G) A_(i, k) *= scale;
+        GSYNC();
       }
     }
     const double t = fabs(w[i]) + fabs(rv1[i]);
@@ -1401,28 +1407,28 @@ static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, in
   for (int i = n - 1; i >= 0; i--) {
     l = i + 1;
     g = w[i];
-    if (lane >= l && lane < n) A_(i, lane) = 0.0;
-    __syncwarp();
+    for (int j = l + lane; j < n; j += G) A_(i, j) = 0.0;
+    GSYNC();
     if (g != 0.0) {
       g = 1.0 / g;
       const double iaii = 1.0 / A_(i, i);
-      if (lane >= l && lane < n) {
+      for (int j = l + lane; j < n; j += G) {
         double sj = 0.0;
-        for (int k = l; k < m; k++) sj += A_(k, i) * A_(k, lane);
+        for (int k = l; k < m; k++) sj += A_(k, i) * A_(k, j);
         const double fj = (sj * iaii) * g;
-        for (int k = i; k < m; k++) A_(k, lane) += fj * A_(k, i);
+        for (int k = i; k < m; k++) A_(k, j) += fj * A_(k, i);
       }
-      __syncwarp();
-      if (lane >= i && lane < m) A_(lane, i) *= g;
+      GSYNC();
+      for (int j = i + lane; j < m; j += G) A_(j, i) *= g;
     } else {
-      if (lane >= i && lane < m) A_(lane, i) = 0.0;
+      for (int j = i + lane; j < m; j += G) A_(j, i) = 0.0;
     }
-    __syncwarp();
-    if (lane == i) A_(i, i) += 1.0;
-    __syncwarp();
+    GSYNC();
+    if (lane == 0) A_(i, i) += 1.0;
+    GSYNC();
   }
-  // QR sweeps: each rotation touches row `lane` only, so the lanes need no
-  // synchronisation until the end
+  // QR sweeps: each rotation touches the lane's own rows only, so the lanes
+  // need no synchronisation until the end
   for (int k = n - 1; k >= 0; k--) {
     for (int its = 0; its < 50; its++) {
       int flag = 1;
@@ -1447,10 +1453,10 @@ static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, in
           h = 1.0 / h;
           c = g * h;
           s = -f * h;
-          if (lane < m) {
-            const double yy = A_(lane, nm), zz = A_(lane, i);
-            A_(lane, nm) = yy * c + zz * s;
-            A_(lane, i) = zz * c - yy * s;
+          for (int jj = lane; jj < m; jj += G) {
+            const double yy = A_(jj, nm), zz = A_(jj, i);
+            A_(jj, nm) = yy * c + zz * s;
+            A_(jj, i) = zz * c - yy * s;
           }
         }
       }
@@ -1493,10 +1499,10 @@ static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, in
         }
         f = c * g + s * y;
         x = c * y - s * g;
-        if (lane < m) {
-          const double yy = A_(lane, j), zz = A_(lane, i);
-          A_(lane, j) = yy * c + zz * s;
-          A_(lane, i) = zz * c - yy * s;
+        for (int jj = lane; jj < m; jj += G) {
+          const double yy = A_(jj, j), zz = A_(jj, i);
+          A_(jj, j) = yy * c + zz * s;
+          A_(jj, i) = zz * c - yy * s;
         }
       }
       rv1[l] = 0.0;
@@ -1504,8 +1510,9 @@ static __device__ __noinline__ int gr_svd_u_warp(double *a, int n, double *w, in
       w[k] = x;
     }
   }
-  __syncwarp();
+  GSYNC();
   return hit;
+#undef GSYNC
 #undef A_
 }
 

@@ -297,28 +297,28 @@ __device__ __forceinline__ void jac_store(const DevPlan &P, const Slots &S, int 
 // ran at trial k-1 (whose U only trial k+1 needs) is run here at trial k >= 3,
 // i.e. only when the iteration really goes on.
 //
-// WARP = false: one thread, its matrix a column of shared memory (stride
-// STR), w and rv1 likewise.  WARP = true: all 32 lanes of a warp, the matrix
-// row-major in the warp's shared memory, w and rv1 private to each lane (the
-// decomposition is gr_svd_u_warp, the rest runs redundantly in every lane and
-// lane 0 stores).  Returns the number of decompositions that hit the
-// 50-sweep limit.
-template <int STR, bool WARP>
+// G = 1: one thread, its matrix a column of shared memory (stride STR), w
+// and rv1 likewise.  G > 1: a group of G lanes (`mask`), the matrix
+// row-major in the group's shared memory, w and rv1 private to each lane (the
+// decomposition is gr_svd_u_grp, the rest runs redundantly in every lane and
+// lane 0 stores).  Returns the number of decompositions that hit the 50-sweep
+// limit.
+template <int STR, int G>
 __device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int s, double *a,
-                                          double *w, double *rv1, int lane) {
+                                          double *w, double *rv1, int lane, unsigned mask) {
+  constexpr bool WARP = G > 1;
   const int W = S.W;
   const int n = P.npar;
-  const int nthr = WARP ? 32 : 1;
   int hits = 0;
   int tk = S.tk[s];
-  if (WARP) tk = __shfl_sync(0xffffffffu, tk, 0);
+  if (WARP) tk = __shfl_sync(mask, tk, 0, G);
   double g[9], x[9];
   for (int k = 0; k < n; k++) g[k] = S.jvec[(size_t)k * W + s];
-  for (int k = WARP ? lane : 0; k < n * n; k += nthr) a[k * STR] = S.hess[(size_t)k * W + s];
-  if (WARP) __syncwarp();
+  for (int k = WARP ? lane : 0; k < n * n; k += G) a[k * STR] = S.hess[(size_t)k * W + s];
+  if (WARP) __syncwarp(mask);
   auto decompose = [&]() {
     if constexpr (WARP)
-      return gr_svd_u_warp(a, n, w, lane);
+      return gr_svd_u_grp<G>(a, n, w, lane, mask);
     else
       return gr_svd_u<STR>(a, n, w, rv1);
   };
@@ -368,7 +368,7 @@ __device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int 
     }
   }
   if (tk != 2)
-    for (int k = WARP ? lane : 0; k < n * n; k += nthr) S.hess[(size_t)k * W + s] = a[k * STR];
+    for (int k = WARP ? lane : 0; k < n * n; k += G) S.hess[(size_t)k * W + s] = a[k * STR];
   if (!WARP || lane == 0) {
     double ptmp[9], step_ia;
     load9(S.par, W, s, ptmp);
@@ -380,7 +380,7 @@ __device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int 
     bounds_fold(ptmp, P, S.sc[SC_L70 * W + s], S.sc[SC_L71 * W + s]);
     store9(S.ptmp, W, s, ptmp);
   }
-  if (WARP) __syncwarp();
+  if (WARP) __syncwarp(mask);
   return hits;
 }
 
@@ -597,7 +597,7 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_cons
   for (int i = blockIdx.x * kSvdBlock + t; i < count; i += gridDim.x * kSvdBlock) {
     const int s = list[i];
     if (S.state[s] != SL_TRIAL) continue;
-    tl.svdlim += solve_slot<kSvdBlock, false>(P, S, s, a, w, rv1, 0);
+    tl.svdlim += solve_slot<kSvdBlock, 1>(P, S, s, a, w, rv1, 0, 0u);
   }
   tl.flush(A, S);
 }
@@ -651,7 +651,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
 // each to completion with the same per-slot steps: the synthesis's
 // wavelengths spread over the lanes (deriv_warp / forward_warp: per-point
 // terms staged in shared memory, every sum formed by one lane in the
-// thread-serial order), the SVD on gr_svd_u_warp, and the scalar transitions
+// thread-serial order), the SVD on gr_svd_u_grp<32>, and the scalar transitions
 // in lane 0.  No lists, no refills.  The operations and their order are the
 // rounds'; only the compiler's contraction of multiply-adds may differ in
 // this kernel, so results agree to rounding (and, the LM being sensitive to
@@ -837,7 +837,7 @@ __global__ void __launch_bounds__(kBlock) finish_kernel(const __grid_constant__ 
       double chi_new = 0.0;
       if (st == SL_TRIAL) {
         double w[9];
-        const int hits = solve_slot<1, true>(P, S, s, a, w, nullptr, lane);
+        const int hits = solve_slot<1, 32>(P, S, s, a, w, nullptr, lane, 0xffffffffu);
         if (lane == 0) t.svdlim += hits;
         double ptmp[9];
         load9(S.ptmp, W, s, ptmp);
@@ -847,6 +847,206 @@ __global__ void __launch_bounds__(kBlock) finish_kernel(const __grid_constant__ 
     }
   }
   if (lane == 0) t.flush(A, S);
+}
+
+// ---------------------------------------------------------------------------
+// Lane-split rounds.  Once the queue is empty, the pixels still in flight are
+// too few to fill the GPU one thread each, and every round waits for one
+// thread's synthesis and SVD.  These variants of the round kernels give each
+// slot a group of G consecutive lanes (G = 2 ... 32, chosen by the host from
+// the number in flight): the group splits the wavelengths of the synthesis
+// (partial sums of H, g and chi^2 per lane, then a butterfly over the group)
+// and the vector loops of the SVD (gr_svd_u_grp); lane 0 makes the scalar
+// transitions.  The trial kernel runs over this round's lists only (no
+// refills are left).  Sums over the wavelengths are formed in another order
+// than the thread-per-slot kernels', so results agree with them to rounding.
+// The SVD variant also serves the full rounds (svd_lanes).
+// ---------------------------------------------------------------------------
+template <int G>
+struct Grp {
+  int lane;       // 0 .. G-1
+  unsigned mask;  // the group's lanes in its warp
+  __device__ __forceinline__ Grp() {
+    const int wl = threadIdx.x & 31;
+    lane = wl & (G - 1);
+    mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (wl & ~(G - 1)));
+  }
+  template <class V>
+  __device__ __forceinline__ V sum(V v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
+    return v;
+  }
+};
+
+namespace detail {
+
+// deriv_pass over a group: lane t takes wavelengths t, t + G, ...; every lane
+// returns the full H45, g9 and chi^2 / (4 nl).
+template <class T, int G>
+__device__ __forceinline__ double deriv_grp(const DevPlan &P, VoigtK<T> &K, T *rden,
+                                            const double *par, const double *step,
+                                            const double *prof, const double sw[4],
+                                            const Grp<G> &grp, double *H45, double *g9) {
+  SynthCall<T> c;
+  synth_setup<T>(c, par, P, step);
+  voigt_prepare<T>(K, c.p5, rden, blockDim.x);
+  T h[45], g[9];
+#pragma unroll
+  for (int i = 0; i < 45; i++) h[i] = T(0);
+#pragma unroll
+  for (int i = 0; i < 9; i++) g[i] = T(0);
+  double chi = 0.0;
+  const int nl = P.nl;
+  const T tsw[4] = {T(sw[0]), T(sw[1]), T(sw[2]), T(sw[3])};
+#pragma unroll 1
+  for (int iw = grp.lane; iw < nl; iw += G) {
+    T syn[4], J[4][9];
+    me_point<T, true>(c, shift_w<T>(c, P, iw), K, tsw, syn, J);
+    T r[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+      chi += rd * rd;
+      r[s] = T(rd);
+    }
+    int idx = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+#pragma unroll
+      for (int j = i; j < 9; j++) {
+        h[idx] += J[0][i] * J[0][j] + J[1][i] * J[1][j] + J[2][i] * J[2][j] + J[3][i] * J[3][j];
+        idx++;
+      }
+      g[i] -= J[0][i] * r[0] + J[1][i] * r[1] + J[2][i] * r[2] + J[3][i] * r[3];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 45; i++) H45[i] = (double)grp.sum(h[i]);
+#pragma unroll
+  for (int i = 0; i < 9; i++) g9[i] = (double)grp.sum(g[i]);
+  return grp.sum(chi) / (4.0 * nl);
+}
+
+// forward_pass over a group (chi^2 only); every lane gets the result.
+template <class T, int G>
+__device__ __forceinline__ double forward_grp(const DevPlan &P, VoigtK<T> &K, T *rden,
+                                              const double *par, const double *step,
+                                              const double *prof, const double sw[4],
+                                              const Grp<G> &grp) {
+  SynthCall<T> c;
+  synth_setup<T>(c, par, P, step);
+  voigt_prepare<T>(K, c.p5, rden, blockDim.x);
+  const T ones[4] = {T(1), T(1), T(1), T(1)};
+  double chi = 0.0;
+  const int nl = P.nl;
+#pragma unroll 1
+  for (int iw = grp.lane; iw < nl; iw += G) {
+    T syn[4];
+    me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+      chi += rd * rd;
+    }
+  }
+  return grp.sum(chi) / (4.0 * nl);
+}
+
+}  // namespace detail
+
+// jac_kernel with G lanes per slot of jlist[parity].
+template <class T, int G>
+__global__ void __launch_bounds__(kBlock, ME_JAC_MINB)
+    jac_grp_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ InvertArgs A,
+                   const __grid_constant__ Slots S, int parity) {
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * kBlock];
+  VoigtK<T> K;
+  voigt_block_setup<T>(K, P, s_tab);
+  T *rden = s_rden + threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S.jcount[parity ^ 1] = 0;
+    S.rcount[parity ^ 1] = 0;
+  }
+  const Grp<G> grp;
+  const int count = S.jcount[parity];
+  const int W = S.W;
+  const int nl = P.nl;
+  Tally t;
+  const int per_grid = gridDim.x * (blockDim.x / G);
+  for (int i = blockIdx.x * (blockDim.x / G) + threadIdx.x / G; i < count; i += per_grid) {
+    const int s = S.jlist[parity * W + i];
+    const double *pp = A.prof + (size_t)S.pix[s] * 4 * nl;
+    double par[9], step[9], sw[4];
+    load9(S.par, W, s, par);
+    slot_weights(P, S, s, step, sw);
+    double H45[45], g9[9];
+    const double chi0 = deriv_grp<T, G>(P, K, rden, par, step, pp, sw, grp, H45, g9);
+    if (grp.lane == 0) {
+      t.jac++;
+      jac_store(P, S, s, par, chi0, H45, g9);
+    }
+  }
+  t.flush(A, S);
+}
+
+// svd_kernel with G lanes per slot, its matrix row-major in shared memory.
+template <int G>
+__global__ void __launch_bounds__(kBlock)
+    svd_grp_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ InvertArgs A,
+                   const __grid_constant__ Slots S, int parity, int which) {
+  __shared__ double s_a[kBlock / G][81];
+  const Grp<G> grp;
+  double *a = s_a[threadIdx.x / G];
+  const int W = S.W;
+  Tally tl;
+  const int *list = which == 0 ? S.jlist + parity * W : S.rlist + parity * W;
+  const int count = which == 0 ? S.jcount[parity] : S.rcount[parity];
+  const int per_grid = gridDim.x * (blockDim.x / G);
+  for (int i = blockIdx.x * (blockDim.x / G) + threadIdx.x / G; i < count; i += per_grid) {
+    const int s = list[i];
+    if (S.state[s] != SL_TRIAL) continue;  // uniform across the group
+    double w[9];
+    const int hits = solve_slot<1, G>(P, S, s, a, w, nullptr, grp.lane, grp.mask);
+    if (grp.lane == 0) tl.svdlim += hits;
+  }
+  tl.flush(A, S);
+}
+
+// trial_kernel with G lanes per slot, over this round's lists (jlist: first
+// trials or run ends; rlist: later trials); no refills.
+template <class T, int G>
+__global__ void __launch_bounds__(kBlock)
+    trial_grp_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ InvertArgs A,
+                     const __grid_constant__ Slots S, int parity) {
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * kBlock];
+  VoigtK<T> K;
+  voigt_block_setup<T>(K, P, s_tab);
+  T *rden = s_rden + threadIdx.x;
+  const Grp<G> grp;
+  const int W = S.W;
+  const int nl = P.nl;
+  const int next_parity = parity ^ 1;
+  const int nj = S.jcount[parity], nr = S.rcount[parity];
+  Tally t;
+  const int per_grid = gridDim.x * (blockDim.x / G);
+  for (int i = blockIdx.x * (blockDim.x / G) + threadIdx.x / G; i < nj + nr; i += per_grid) {
+    const int s = i < nj ? S.jlist[parity * W + i] : S.rlist[parity * W + (i - nj)];
+    const int st = S.state[s];
+    if (st != SL_TRIAL && st != SL_RUN_END) continue;  // uniform across the group
+    double chi_new = 0.0;
+    if (st == SL_TRIAL) {
+      double ptmp[9], step[9], sw[4];
+      load9(S.ptmp, W, s, ptmp);
+      slot_weights(P, S, s, step, sw);
+      chi_new = forward_grp<T, G>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl,
+                                  sw, grp);
+    }
+    if (grp.lane == 0) trial_transition<true>(P, A, S, s, st, chi_new, next_parity, t);
+  }
+  if (grp.lane == 0) t.flush(A, S);
 }
 
 }  // namespace me

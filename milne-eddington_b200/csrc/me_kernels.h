@@ -113,12 +113,20 @@ int round_grid(int precision, int which, int device);
 // queue is exhausted (it does not refill).
 cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                           int *cursor, int grid, cudaStream_t st);
-// One round: jac_kernel, svd_kernel (first trials), svd_kernel (later
-// trials), trial_kernel.  ev (nullable): 5 events recorded before, between
-// and after the four launches (per-kernel device time when profiling).
+// One round: jac_kernel, svd (first trials), svd (later trials),
+// trial_kernel.  grids: jac, trial, svd CTAs.  ev (nullable): 5 events
+// recorded before, between and after the four launches (per-kernel device
+// time when profiling).  svd_lanes: lanes per matrix of the SVD launches
+// (1: svd_kernel; 2, 4, 8: svd_grp_kernel).
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                          int parity, const int grids[3], cudaStream_t st,
-                         cudaEvent_t *ev = nullptr);
+                         cudaEvent_t *ev = nullptr, int svd_lanes = 1);
+// A round with G lanes per slot (G = 2, 4, 8, 16, 32): for when the queue is
+// empty and the slots in flight are too few to fill the device one thread
+// each.  The trial kernel runs over the round's lists and does not refill.
+cudaError_t launch_round_grp(int precision, int G, const DevPlan &P, const InvertArgs &A,
+                             const Slots &S, int parity, const int grids[3], cudaStream_t st,
+                             cudaEvent_t *ev = nullptr);
 // Best-fit profiles after a batch: synthesis at fitpar for the inverted
 // pixels (flags bit 0), zeros for the skipped ones.
 cudaError_t launch_fit(int precision, const DevPlan &P, const double *d_fitpar,

@@ -133,9 +133,9 @@ __global__ void init_guess_kernel(const DevPlan P, const double *prof, long long
 int round_grid_f32(int which, int device);
 int round_grid_f64(int which, int device);
 cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                             const int grids[3], cudaStream_t st, cudaEvent_t *ev);
+                             const int grids[3], cudaStream_t st, cudaEvent_t *ev, int svd_lanes);
 cudaError_t launch_round_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                             const int grids[3], cudaStream_t st, cudaEvent_t *ev);
+                             const int grids[3], cudaStream_t st, cudaEvent_t *ev, int svd_lanes);
 
 cudaError_t launch_finish_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
                               int grid, cudaStream_t st);
@@ -147,14 +147,26 @@ cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, 
                         : launch_finish_f32(P, A, S, cursor, grid, st);
 }
 
+cudaError_t launch_round_grp_f32(int G, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                               int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev);
+cudaError_t launch_round_grp_f64(int G, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                               int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev);
+cudaError_t launch_round_grp(int precision, int G, const DevPlan &P, const InvertArgs &A,
+                             const Slots &S, int parity, const int grids[3], cudaStream_t st,
+                             cudaEvent_t *ev) {
+  return precision == 1 ? launch_round_grp_f64(G, P, A, S, parity, grids, st, ev)
+                        : launch_round_grp_f32(G, P, A, S, parity, grids, st, ev);
+}
+
 int round_grid(int precision, int which, int device) {
   return precision == 1 ? round_grid_f64(which, device) : round_grid_f32(which, device);
 }
 
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
-                         int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev) {
-  return precision == 1 ? launch_round_f64(P, A, S, parity, grids, st, ev)
-                        : launch_round_f32(P, A, S, parity, grids, st, ev);
+                         int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev,
+                         int svd_lanes) {
+  return precision == 1 ? launch_round_f64(P, A, S, parity, grids, st, ev, svd_lanes)
+                        : launch_round_f32(P, A, S, parity, grids, st, ev, svd_lanes);
 }
 
 cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,

@@ -140,7 +140,8 @@ EXPORTED = [
     "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
     "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
-    "me_plan_set_profiling",
+    "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
+    "me_plan_svd_lanes", "me_plan_set_svd_lanes",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
@@ -211,6 +212,12 @@ def lib() -> ctypes.CDLL:
         L.me_plan_set_tail_slots.restype = None
         L.me_plan_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_profiling.restype = None
+        L.me_plan_max_group.argtypes = [ctypes.c_void_p]
+        L.me_plan_set_max_group.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_max_group.restype = None
+        L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
+        L.me_plan_set_svd_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_svd_lanes.restype = None
         L.me_invert_batch.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                       ctypes.POINTER(MeStats)]
         L.me_invert_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
@@ -365,6 +372,22 @@ class Plan:
     @tail_slots.setter
     def tail_slots(self, n: int):
         lib().me_plan_set_tail_slots(self._h, int(n))
+
+    @property
+    def max_group(self) -> int:
+        return lib().me_plan_max_group(self._h)
+
+    @max_group.setter
+    def max_group(self, lanes: int):
+        lib().me_plan_set_max_group(self._h, int(lanes))
+
+    @property
+    def svd_lanes(self) -> int:
+        return lib().me_plan_svd_lanes(self._h)
+
+    @svd_lanes.setter
+    def svd_lanes(self, lanes: int):
+        lib().me_plan_set_svd_lanes(self._h, int(lanes))
 
     def set_profiling(self, on: bool = True):
         """Per-kernel device time in the stats (CUDA events around every launch)."""

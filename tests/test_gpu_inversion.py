@@ -53,22 +53,26 @@ def cfg0_map():
                 self=agreement(pert, base))
 
 
-@pytest.mark.parametrize("tail", [0, -1], ids=["rounds", "tail_kernel"])
+# (max_group, tail_slots, svd_lanes): one thread per pixel throughout;
+# lane-split rounds once the queue is empty, with 4 lanes per SVD in the full
+# rounds; the warp-per-pixel tail kernel (for a batch this small the last two
+# run most of the LM steps)
+MODES = {"threads": (1, 0, 1), "lane_split": (32, 0, 4), "tail_kernel": (1, -1, 1)}
+
+
+@pytest.mark.parametrize("mode", list(MODES))
 @pytest.mark.parametrize("prec", ["FP64", "FP32"])
-def test_inversion_parity_vs_oracle(cfg0_map, prec, tail):
-    """Rounds only (tail_slots = 0), and with the warp-per-pixel tail kernel
-    taking over once the queue is empty (the default; for a batch this small
-    it runs most of the LM steps)."""
+def test_inversion_parity_vs_oracle(cfg0_map, prec, mode):
     m = cfg0_map
     cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
     with me_b200.Plan(cfg, m["lam"]) as plan:
-        plan.tail_slots = tail
+        plan.max_group, plan.tail_slots, plan.svd_lanes = MODES[mode]
         res, st = plan.invert(m["prof"])
     tail_launches = st["launches"] - 4 * st["rounds"]
-    assert tail_launches == (0 if tail == 0 else 1)
+    assert tail_launches == (0 if MODES[mode][1] == 0 else 1)
     same, within, med = agreement(res, m["base"])
     s_same, s_within, _ = m["self"]
-    print(f"{prec} tail={tail}: identical {same:.3f} (self {s_same:.3f}), chi2<=1.05x "
+    print(f"{prec} {mode}: identical {same:.3f} (self {s_same:.3f}), chi2<=1.05x "
           f"{within:.3f} (self {s_within:.3f}), median ratio {med:.6f}, rounds {st['rounds']}")
     assert st["valid"] == np.sum(m["base"][:, 9] > 0)
     assert abs(med - 1) < 1e-3

@@ -41,10 +41,12 @@ def test_noalloc_matches_allocating_entry_point_two_calls():
 
     res_ref = torch.zeros((2 * npix, 10), dtype=torch.float64, device="cuda")
     with me_b200.Plan(cfg, lam) as plan:
-        # the no-alloc entry point runs LM rounds to the end; the plan's tail
-        # kernel (same arithmetic up to multiply-add contraction) is switched
-        # off so that the two can be compared bit for bit
+        # the no-alloc entry point runs one-thread-per-pixel LM rounds to the
+        # end; the plan's lane-split rounds and tail kernel (the same
+        # arithmetic up to summation order and multiply-add contraction) are
+        # switched off so that the two can be compared bit for bit
         plan.tail_slots = 0
+        plan.max_group = 1
         plan.carry_chisq = 0.0
         for c in range(2):
             sl = slice(c * npix, (c + 1) * npix)
