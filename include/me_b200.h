@@ -363,6 +363,58 @@ int me_mlp_set_params(me_mlp *mlp, const float *params);
 int me_mlp_loss_grad(me_mlp *mlp, const float *x, const float *t, int rows, double *loss,
                      float *grad);
 
+/* ---------------------------------------------------------------------------
+ * FITS primary-HDU I/O, the subset of cfitsio the reference's driver uses
+ * (Src/IO.c:120-742): dimensions and BITPIX, reads of doubles from an element
+ * offset with BSCALE / BZERO applied (fits_read_pix with TDOUBLE), creation of
+ * a zero-filled BITPIX -64 image (fits_create_img), writes of doubles at an
+ * element offset (fits_write_pix).  Element offsets count in the FITS order
+ * (NAXIS1 fastest).  CPU only.
+ * ------------------------------------------------------------------------- */
+int me_fits_image_info(const char *path, int *bitpix, int *naxis, long naxes[8]);
+int me_fits_read(const char *path, long first, long n, double *out);
+int me_fits_create(const char *path, int naxis, const long *naxes);
+int me_fits_write(const char *path, long first, long n, const double *v);
+
+/* ---------------------------------------------------------------------------
+ * The driver: the reference's MEINV program around INVERSION_MULTI
+ * (Src/ME_INV.c:64-295 with rWavelength, rProfile, rProfilesll, PixelMV,
+ * CACHE_INIT, WRITE_RESULT of Src/IO.c and INIT_INV's chunking,
+ * Src/INV_INIT.c:207-250).  It reads data_path / wavelength_path, inverts the
+ * pixels of sol_box in chunks of nprofiles (all at once with Cache_prof),
+ * writes result_path [10][nx'][ny'] and, with output_fit, fit_path
+ * [nw][4][nx'][ny'], and with Cache_inv keeps the reference's checkpoint file
+ * (cache_path) and skips the chunks it marks done.  Consecutive chunks are
+ * inverted together (batch_pixels per GPU call); several GPUs take batches in
+ * turn (batch b on device b mod N) in place of the MPI farm.
+ * ------------------------------------------------------------------------- */
+typedef struct me_run_options {
+  int ndevices;            /* plans, one per entry of devices (default 1)           */
+  const int *devices;      /* CUDA device of each plan (NULL: 0, 1, ...)            */
+  long batch_pixels;       /* pixels per GPU call, in whole chunks (131072)         */
+  int max_group;           /* me_plan_set_max_group for every plan (-1: default)    */
+  int tail_slots;          /* me_plan_set_tail_slots for every plan (-2: default)   */
+  long stop_after_chunks;  /* stop once this many chunks are done (0: run to the
+                              end); an interrupted run, for checkpoint tests        */
+  me_mlp *initializer;     /* learned initialiser for every plan (NULL: none)       */
+} me_run_options;
+
+typedef struct me_run_report {
+  long nx, ny, nw;         /* data cube                                      */
+  long counts;             /* pixels of sol_box                              */
+  long chunk_pixels;       /* nProf                                          */
+  long nchunks;            /* chunks of sol_box                              */
+  long chunks_done;        /* chunks inverted by this run                    */
+  long chunks_skipped;     /* chunks the checkpoint file marked done         */
+  long pixels_inverted;    /* pixels inverted by this run                    */
+  double seconds;          /* wall time of the run                           */
+} me_run_report;
+
+int me_run_options_default(me_run_options *opt);
+/* opt and report may be NULL. */
+int me_run(const char *ctl_path, const me_run_options *opt, me_run_report *report);
+int me_run_config(const me_config *cfg, const me_run_options *opt, me_run_report *report);
+
 #ifdef __cplusplus
 }
 #endif

@@ -145,7 +145,30 @@ EXPORTED = [
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
+    "me_fits_image_info", "me_fits_read", "me_fits_create", "me_fits_write",
+    "me_run_options_default", "me_run", "me_run_config",
 ]
+
+
+class MeRunOptions(ctypes.Structure):
+    _fields_ = [
+        ("ndevices", ctypes.c_int),
+        ("devices", ctypes.POINTER(ctypes.c_int)),
+        ("batch_pixels", ctypes.c_long),
+        ("max_group", ctypes.c_int),
+        ("tail_slots", ctypes.c_int),
+        ("stop_after_chunks", ctypes.c_long),
+        ("initializer", ctypes.c_void_p),
+    ]
+
+
+class MeRunReport(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_long) for n in ("nx", "ny", "nw", "counts", "chunk_pixels",
+                                             "nchunks", "chunks_done", "chunks_skipped",
+                                             "pixels_inverted")] + [("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class MeMlpTrainParams(ctypes.Structure):
@@ -259,6 +282,17 @@ def lib() -> ctypes.CDLL:
         L.me_mlp_get_params.argtypes = [ctypes.c_void_p, _F]
         L.me_mlp_set_params.argtypes = [ctypes.c_void_p, _F]
         L.me_mlp_loss_grad.argtypes = [ctypes.c_void_p, _F, _F, ctypes.c_int, _D, _F]
+        _L8 = ctypes.c_long * 8
+        L.me_fits_image_info.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int), _L8]
+        L.me_fits_read.argtypes = [ctypes.c_char_p, ctypes.c_long, ctypes.c_long, _D]
+        L.me_fits_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
+        L.me_fits_write.argtypes = [ctypes.c_char_p, ctypes.c_long, ctypes.c_long, _D]
+        L.me_run_options_default.argtypes = [ctypes.POINTER(MeRunOptions)]
+        L.me_run.argtypes = [ctypes.c_char_p, ctypes.POINTER(MeRunOptions),
+                             ctypes.POINTER(MeRunReport)]
+        L.me_run_config.argtypes = [ctypes.POINTER(MeConfig), ctypes.POINTER(MeRunOptions),
+                                    ctypes.POINTER(MeRunReport)]
         _lib = L
     return _lib
 
@@ -606,3 +640,64 @@ class Initializer:
         _check(lib().me_mlp_loss_grad(self._h, _fptr(x), _fptr(t), x.shape[0], _ptr(loss),
                                       _fptr(grad)), "me_mlp_loss_grad")
         return float(loss[0]), grad
+
+
+# ---------------------------------------------------------------------------
+# FITS primary-HDU I/O and the driver
+# ---------------------------------------------------------------------------
+def fits_info(path):
+    """(bitpix, shape in FITS order NAXIS1, NAXIS2, ...)."""
+    b, n = ctypes.c_int(), ctypes.c_int()
+    ax = (ctypes.c_long * 8)()
+    _check(lib().me_fits_image_info(str(path).encode(), ctypes.byref(b), ctypes.byref(n), ax),
+           "me_fits_image_info")
+    return b.value, tuple(ax[i] for i in range(n.value))
+
+
+def fits_read(path, first: int = 0, n: int = -1) -> np.ndarray:
+    """Elements [first, first + n) of the primary array as doubles (FITS order)."""
+    _, shape = fits_info(path)
+    total = int(np.prod(shape)) if shape else 0
+    if n < 0:
+        n = total - first
+    out = np.zeros(n)
+    _check(lib().me_fits_read(str(path).encode(), first, n, _ptr(out)), "me_fits_read")
+    return out
+
+
+def fits_create(path, shape):
+    """Zero-filled BITPIX -64 image; shape in FITS order (NAXIS1 first)."""
+    ax = (ctypes.c_long * len(shape))(*shape)
+    _check(lib().me_fits_create(str(path).encode(), len(shape), ax), "me_fits_create")
+
+
+def fits_write(path, first: int, values: np.ndarray):
+    v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+    _check(lib().me_fits_write(str(path).encode(), first, v.size, _ptr(v)), "me_fits_write")
+
+
+def run_options(**kw) -> MeRunOptions:
+    o = MeRunOptions()
+    _check(lib().me_run_options_default(ctypes.byref(o)), "me_run_options_default")
+    devices = kw.pop("devices", None)
+    init = kw.pop("initializer", None)
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    if devices is not None:
+        arr = (ctypes.c_int * len(devices))(*devices)
+        o.devices = arr
+        o.ndevices = len(devices)
+        o._devices_keepalive = arr
+    if init is not None:
+        o.initializer = init.handle.value if hasattr(init.handle, "value") else init.handle
+    return o
+
+
+def run(ctl_path, **kw) -> dict:
+    """me_run: the driver on a control file; returns the run report."""
+    o = run_options(**kw)
+    rep = MeRunReport()
+    _check(lib().me_run(str(ctl_path).encode(), ctypes.byref(o), ctypes.byref(rep)), "me_run")
+    return rep.as_dict()
