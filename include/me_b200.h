@@ -25,6 +25,7 @@ extern "C" {
 #define ME_MAX_LINES 20   /* Src/RINPUT.h:15 NUM_LINES */
 #define ME_PATH_LEN 512   /* Src/STR.h:15 Max_Line_Length */
 #define ME_MAX_NL 512     /* largest wavelength grid a plan accepts */
+#define ME_MAX_FILTER 63  /* most sub-wavelengths of an instrument filter */
 
 /* status codes */
 #define ME_OK 0
@@ -89,6 +90,11 @@ typedef struct me_config {
   unsigned long long rng_seed;        /* rng_seed (0): key of the per-(pixel, run) draws */
   int lines_seen;                     /* bookkeeping: `lines` present      */
   int data_path_seen, wavelength_path_seen;
+  /* filter = FWHM [mA], points (0 = none): each observed wavelength is the
+   * Gaussian-weighted mean of the synthesis over `points` offsets spanning
+   * +-1.5 FWHM (an instrument filter; not in the reference) */
+  double filter_fwhm;
+  int filter_points;
 } me_config;
 
 /* Facts INIT_INV derives from the grid (Src/INV_INIT.c:121-177). */
@@ -160,6 +166,15 @@ int me_plan_get_facts(const me_plan *plan, me_plan_facts *out);
  * Src/ME_INV.c:91).  These read / reset it. */
 double me_plan_get_carry_chisq(const me_plan *plan);
 void me_plan_set_carry_chisq(me_plan *plan, double chisq);
+
+/* Instrument filter (no reference counterpart): each observed wavelength
+ * lambda_i becomes sum_q weights[q] * synthesis(lambda_i + offsets_mA[q] / 1e3)
+ * for the profiles and the Jacobian, everywhere the plan synthesises (the
+ * inversion, me_synthesize*, the fit profiles, initialiser training).  k = 1
+ * removes it; k <= ME_MAX_FILTER.  The control keyword `filter = FWHM, points`
+ * sets a Gaussian table at plan creation.  me_invert_batch_device_noalloc does
+ * not take filtered control files. */
+int me_plan_set_filter(me_plan *plan, const double *offsets_mA, const double *weights, int k);
 
 /* Persistent-grid size (CTAs) of the inversion kernel; set_grid overrides the
  * occupancy-derived default (used by the autotuner and the benchmarks). */

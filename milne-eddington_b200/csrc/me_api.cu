@@ -97,6 +97,8 @@ struct me_plan {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double carry = 0.0;  // LM->chisq carried between pixels (STRUCT_LM LM = {0})
   DevBuf d_lambda, d_dlambda;
+  DevBuf d_flambda, d_fdlambda;  // instrument filter sub-wavelengths
+  std::vector<double> h_lambda;  // the observed grid
   DevBuf d_prof, d_res, d_fit;  // staging of the host entry point
   DevBuf d_flags, d_pen0, d_lastchi, d_counters, d_totals, d_next, d_stale, d_list, d_fitpar;
   // slots of the pixels in flight (struct me::Slots), sized for `window`
@@ -153,6 +155,8 @@ extern "C" const char *me_strerror(int status) {
 namespace me {
 
 int record_error(int code, const char *msg) { return fail(code, msg); }
+
+void gaussian_filter(double fwhm, int points, std::vector<double> &off, std::vector<double> &w);
 
 // The plan constants INIT_INV derives (Src/INV_INIT.c:112-201) from a parsed
 // control file and a wavelength grid; P.lambda / P.dlambda are left null.
@@ -240,10 +244,72 @@ int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P
   P.regul_any = cfg->regul_any ? 1 : 0;
   P.seed = cfg->rng_seed;
   fill_voigt_consts(P, cfg->nfigures);
+  P.nsub = 1;
+  if (cfg->filter_fwhm > 0 && cfg->filter_points > 1) {
+    if (cfg->filter_points > ME_MAX_FILTER || cfg->filter_points % 2 == 0)
+      return fail(ME_ERR_CONFIG, "filter needs an odd number of points up to 63");
+    std::vector<double> off, w;
+    gaussian_filter(cfg->filter_fwhm, cfg->filter_points, off, w);
+    P.nsub = cfg->filter_points;
+    for (int k = 0; k < P.nsub; k++) P.sub_w[k] = w[k];
+  }
   return ME_OK;
 }
 
+// The table of the `filter` keyword: `points` offsets [mA] uniform over +-1.5
+// FWHM, weights exp(-d^2 / 2 sigma^2) normalised to sum 1.
+void gaussian_filter(double fwhm, int points, std::vector<double> &off, std::vector<double> &w) {
+  off.assign(points, 0.0);
+  w.assign(points, 1.0);
+  if (points <= 1) return;
+  const double sigma = fwhm / (2.0 * sqrt(2.0 * log(2.0)));
+  double sum = 0.0;
+  for (int k = 0; k < points; k++) {
+    off[k] = -1.5 * fwhm + 3.0 * fwhm * k / (points - 1);
+    w[k] = exp(-off[k] * off[k] / (2.0 * sigma * sigma));
+    sum += w[k];
+  }
+  for (int k = 0; k < points; k++) w[k] /= sum;
+}
+
 }  // namespace me
+
+namespace {
+// Sub-wavelengths and weights of an instrument filter on the plan's device.
+int set_filter_grid(me_plan *p, const double *off_mA, const double *w, int k) {
+  me::DevPlan &P = p->P;
+  const int nl = P.nl;
+  if (k <= 1) {
+    P.nsub = 1;
+    P.flambda = P.fdlambda = nullptr;
+    return ME_OK;
+  }
+  std::vector<double> fl((size_t)nl * k), fdl((size_t)nl * k);
+  for (int i = 0; i < nl; i++)
+    for (int q = 0; q < k; q++) {
+      fl[(size_t)i * k + q] = p->h_lambda[i] + off_mA[q] * 1e-3;
+      fdl[(size_t)i * k + q] = fl[(size_t)i * k + q] - P.lambda0;
+    }
+  const size_t bytes = sizeof(double) * fl.size();
+  if (p->d_flambda.ensure(bytes) || p->d_fdlambda.ensure(bytes) ||
+      cudaMemcpy(p->d_flambda.p, fl.data(), bytes, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(p->d_fdlambda.p, fdl.data(), bytes, cudaMemcpyHostToDevice))
+    return fail(ME_ERR_CUDA, "filter grid allocation failed");
+  P.nsub = k;
+  for (int q = 0; q < k; q++) P.sub_w[q] = w[q];
+  P.flambda = p->d_flambda.as<double>();
+  P.fdlambda = p->d_fdlambda.as<double>();
+  return ME_OK;
+}
+}  // namespace
+
+extern "C" int me_plan_set_filter(me_plan *p, const double *offsets_mA, const double *weights,
+                                  int k) {
+  if (!p || k < 1 || k > ME_MAX_FILTER || (k > 1 && (!offsets_mA || !weights)))
+    return fail(ME_ERR_ARG, "filter: 1 <= k <= ME_MAX_FILTER offsets and weights");
+  CK(cudaSetDevice(p->device));
+  return set_filter_grid(p, offsets_mA, weights, k);
+}
 
 extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl, int device,
                               me_plan **out) {
@@ -276,6 +342,16 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
   }
   P.lambda = p->d_lambda.as<double>();
   P.dlambda = p->d_dlambda.as<double>();
+  p->h_lambda.assign(lambda, lambda + nl);
+  if (P.nsub > 1) {
+    std::vector<double> off, w;
+    me::gaussian_filter(cfg->filter_fwhm, cfg->filter_points, off, w);
+    const int rc = set_filter_grid(p, off.data(), w.data(), P.nsub);
+    if (rc) {
+      me_plan_destroy(p);
+      return rc;
+    }
+  }
   p->grid_jac = me::round_grid(p->precision, 0, device);
   p->grid_trial = me::round_grid(p->precision, 1, device);
   p->grid_svd = me::round_grid(p->precision, 2, device);
@@ -308,7 +384,8 @@ extern "C" void me_plan_destroy(me_plan *p) {
                     &p->d_counters, &p->d_totals, &p->d_next,    &p->d_stale,
                     &p->d_list,   &p->d_slot_pix, &p->d_slot_i32, &p->d_slot_cnt,
                     &p->d_slot_u8, &p->d_slot_sc, &p->d_slot_vec, &p->d_slot_hess,
-                    &p->d_slot_list, &p->d_slot_small, &p->d_fitpar};
+                    &p->d_slot_list, &p->d_slot_small, &p->d_fitpar, &p->d_init,
+                    &p->d_flambda, &p->d_fdlambda};
   for (DevBuf *b : bufs) b->release();
   if (p->h_poll) cudaFreeHost(p->h_poll);
   if (p->ev0) cudaEventDestroy(p->ev0);

@@ -37,7 +37,7 @@ enum Key {
   K_VCOEF, K_LCOEF, K_ICRIT, K_SVDTHR, K_HMIREF, K_CACHEPROF, K_NTHREADS, K_NFIG, K_STEP,
   K_NPROF, K_CACHEINV,
   // keywords of this library
-  K_PRECISION, K_RNGSEED,
+  K_PRECISION, K_RNGSEED, K_FILTER,
   K_COUNT
 };
 
@@ -106,6 +106,7 @@ const KeyDef kKeys[K_COUNT] = {
     {"Cache_inv", "No"},
     {"precision", "FP32"},
     {"rng_seed", "0"},
+    {"filter", "0"},
 };
 
 const size_t kKeyLen = 64;    // Src/STR.h:14
@@ -300,6 +301,26 @@ int convert(const Parsed &P, me_config *c, char *err, size_t errlen) {
     return ME_ERR_CONFIG;
   }
   c->rng_seed = strtoull(P.val[K_RNGSEED].c_str(), nullptr, 0);
+  // filter = FWHM [mA], points: a Gaussian instrument filter (not in the
+  // reference); "0" = none
+  c->filter_fwhm = 0.0;
+  c->filter_points = 1;
+  {
+    double fw = 0.0;
+    int np = 0;
+    const int got = sscanf(P.val[K_FILTER].c_str(), "%lf, %d", &fw, &np);
+    if (got >= 1 && fw > 0.0) {
+      if (got != 2 || np < 1 || np > ME_MAX_FILTER || np % 2 == 0) {
+        set_err(err, errlen, "filter needs FWHM [mA] and an odd number of points up to 63");
+        return ME_ERR_CONFIG;
+      }
+      c->filter_fwhm = fw;
+      c->filter_points = np;
+    } else if (got < 1 || fw < 0.0) {
+      set_err(err, errlen, "filter must be 0 or `FWHM, points`");
+      return ME_ERR_CONFIG;
+    }
+  }
   // Nfigures selects a row of the region table (Src/FADDEEVA.c:471-477);
   // rows exist for Nfigures <= 8 only.
   if (c->nfigures > 8) {

@@ -22,6 +22,8 @@
 
 #include <type_traits>
 
+#include "../../include/me_b200.h"
+
 namespace me {
 
 constexpr double kPi = 3.14159265358979323846;
@@ -50,6 +52,12 @@ struct DevPlan {
   double thr[5];  // |z|^2 region boundaries of this Nfigures row
   const double *lambda;   // [nl] wavelength grid [A]
   const double *dlambda;  // [nl] lambda - lambda0 [A]
+  // instrument filter (no reference counterpart): observed wavelength i is
+  // sum_k sub_w[k] * synthesis at flambda[i * nsub + k]; nsub = 1: none
+  int nsub;
+  double sub_w[ME_MAX_FILTER];
+  const double *flambda;   // [nl * nsub] sub-wavelengths [A]
+  const double *fdlambda;  // [nl * nsub] minus lambda0 [A]
 };
 
 // ---------------------------------------------------------------------------
@@ -595,6 +603,20 @@ __device__ __forceinline__ double shift_w<double>(const SynthCall<double> &c, co
   return 1e3 * __ldg(P.lambda + iw) / c.p4 + c.vshift;
 }
 
+// shift_w at sub-wavelength j of the instrument filter
+template <class T>
+__device__ __forceinline__ T shift_wf(const SynthCall<T> &c, const DevPlan &P, int j);
+template <>
+__device__ __forceinline__ float shift_wf<float>(const SynthCall<float> &c, const DevPlan &P,
+                                                 int j) {
+  return (1e3f * float(__ldg(P.fdlambda + j)) - c.vshift) * c.inv_p4;
+}
+template <>
+__device__ __forceinline__ double shift_wf<double>(const SynthCall<double> &c, const DevPlan &P,
+                                                   int j) {
+  return 1e3 * __ldg(P.flambda + j) / c.p4 + c.vshift;
+}
+
 // One wavelength of Milne_Eddington_Single.  syn[4] = I, Q, U, V.  With
 // DERIV also J[s][k] = d syn_s / d p_k * step[k] * sw[s] (sw: per-Stokes
 // weights the caller wants folded in, 1 for the plain Jacobian).
@@ -785,6 +807,40 @@ __device__ __forceinline__ void me_point(const SynthCall<T> &c, T w0, const Voig
   J[0][8] = (c.p7 * c.step[8] - t8 * num[0]) * sw[0];
 #pragma unroll
   for (int s = 1; s < 4; s++) J[s][8] = t8 * num[s] * sw[s];
+}
+
+// One observed wavelength of the synthesis: me_point at it, or, with the
+// instrument filter (FILT, P.nsub > 1), the weighted sum over its
+// sub-wavelengths, in order from zero, of the profiles and Jacobian rows.
+template <class T, bool DERIV, bool FILT>
+__device__ __forceinline__ void channel_point(const SynthCall<T> &c, const DevPlan &P,
+                                              const VoigtK<T> &K, const T sw[4], int iw, T syn[4],
+                                              T (*J)[9]) {
+  if constexpr (!FILT) {
+    me_point<T, DERIV>(c, shift_w<T>(c, P, iw), K, sw, syn, J);
+  } else {
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      syn[s] = T(0);
+      if (DERIV)
+#pragma unroll
+        for (int k = 0; k < 9; k++) J[s][k] = T(0);
+    }
+    const int ns = P.nsub;
+#pragma unroll 1
+    for (int q = 0; q < ns; q++) {
+      T ys[4], Jq[4][9];
+      me_point<T, DERIV>(c, shift_wf<T>(c, P, iw * ns + q), K, sw, ys, DERIV ? Jq : nullptr);
+      const T wq = T(P.sub_w[q]);
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        syn[s] += wq * ys[s];
+        if (DERIV)
+#pragma unroll
+          for (int k = 0; k < 9; k++) J[s][k] += wq * Jq[s][k];
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

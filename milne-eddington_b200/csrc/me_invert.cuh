@@ -35,7 +35,7 @@ namespace detail {
 // W = weight^2 / norm0 (Noise_Init, Src/ME_SOLVER.c:410-441).  H45 = upper
 // triangle of the full 9x9 (row-major, i <= j), g9 = -J^T W r; returns
 // sum (r sw)^2 / (4 nl) accumulated in FP64.
-template <class T>
+template <class T, bool FILT>
 __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                              const double *par, const double *step,
                                              const double *prof, const double sw[4], double *H45,
@@ -54,7 +54,7 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *
 #pragma unroll 1
   for (int iw = 0; iw < nl; iw++) {
     T syn[4], J[4][9];
-    me_point<T, true>(c, shift_w<T>(c, P, iw), K, tsw, syn, J);
+    channel_point<T, true, FILT>(c, P, K, tsw, iw, syn, J);
     T r[4];
 #pragma unroll
     for (int s = 0; s < 4; s++) {
@@ -82,7 +82,7 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *
 
 // Forward synthesis + chi^2 (Trial_Synthesis's synthesis and Loss_Function);
 // residuals and their squares in FP64.  fit (nullable) receives the profile.
-template <class T>
+template <class T, bool FILT>
 __device__ __forceinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                             const double *par, const double *step,
                                             const double *prof, const double sw[4],
@@ -96,7 +96,7 @@ __device__ __forceinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T
 #pragma unroll 1
   for (int iw = 0; iw < nl; iw++) {
     T syn[4];
-    me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
+    channel_point<T, false, FILT>(c, P, K, ones, iw, syn, nullptr);
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       if (prof) {
@@ -542,7 +542,7 @@ using namespace detail;
 // ---------------------------------------------------------------------------
 // Synthesis with Jacobian + normal equations for the slots of jlist[parity].
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, bool FILT>
 __global__ void __launch_bounds__(kBlock, ME_JAC_MINB) jac_kernel(const __grid_constant__ DevPlan P,
                                                      const __grid_constant__ InvertArgs A,
                                                      const __grid_constant__ Slots S, int parity) {
@@ -566,7 +566,7 @@ __global__ void __launch_bounds__(kBlock, ME_JAC_MINB) jac_kernel(const __grid_c
     load9(S.par, W, s, par);
     slot_weights(P, S, s, step, sw);
     double H45[45], g9[9];
-    const double chi0 = deriv_pass<T>(P, K, rden, par, step, pp, sw, H45, g9);
+    const double chi0 = deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9);
     t.jac++;
     jac_store(P, S, s, par, chi0, H45, g9);
   }
@@ -605,7 +605,7 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_cons
 // ---------------------------------------------------------------------------
 // One trial step for every slot; run and pixel transitions; refills.
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, bool FILT>
 __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ DevPlan P,
                                                        const __grid_constant__ InvertArgs A,
                                                        const __grid_constant__ Slots S,
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
       double ptmp[9], step[9], sw[4];
       load9(S.ptmp, W, s, ptmp);
       slot_weights(P, S, s, step, sw);
-      chi_new = forward_pass<T>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl, sw,
+      chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl, sw,
                                 nullptr);
     }
     trial_transition<true>(P, A, S, s, st, chi_new, next_parity, t);
@@ -683,7 +683,7 @@ __device__ __forceinline__ void voigt_prepare_warp(VoigtK<T> &K, T y, T *rden, i
 
 // deriv_pass across a warp.  H45 / g9 land in hg[0..53] (shared, all lanes
 // may read after the call); returns chi^2 / (4 nl) in every lane.
-template <class T>
+template <class T, bool FILT>
 __device__ double deriv_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const double *par,
                              const double *step, const double *prof, const double sw[4],
                              int lane, T *stJ, double *stR, double *hg) {
@@ -710,7 +710,7 @@ __device__ double deriv_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const doub
     const int iw = base + lane;
     if (iw < nl) {
       T syn[4], J[4][9];
-      me_point<T, true>(c, shift_w<T>(c, P, iw), K, tsw, syn, J);
+      channel_point<T, true, FILT>(c, P, K, tsw, iw, syn, J);
 #pragma unroll
       for (int s = 0; s < 4; s++) stR[lane * 4 + s] = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
 #pragma unroll
@@ -747,7 +747,7 @@ __device__ double deriv_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const doub
 }
 
 // forward_pass across a warp (chi^2 only); every lane gets the result.
-template <class T>
+template <class T, bool FILT>
 __device__ double forward_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const double *par,
                                const double *step, const double *prof, const double sw[4],
                                int lane, double *stR) {
@@ -761,7 +761,7 @@ __device__ double forward_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const do
     const int iw = base + lane;
     if (iw < nl) {
       T syn[4];
-      me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
+      channel_point<T, false, FILT>(c, P, K, ones, iw, syn, nullptr);
 #pragma unroll
       for (int s = 0; s < 4; s++) stR[lane * 4 + s] = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
     }
@@ -780,7 +780,7 @@ __device__ double forward_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const do
 
 }  // namespace detail
 
-template <class T>
+template <class T, bool FILT>
 __global__ void __launch_bounds__(kBlock) finish_kernel(const __grid_constant__ DevPlan P,
                                                         const __grid_constant__ InvertArgs A,
                                                         const __grid_constant__ Slots S,
@@ -824,7 +824,7 @@ __global__ void __launch_bounds__(kBlock) finish_kernel(const __grid_constant__ 
       if (st == SL_JAC_START || st == SL_JAC_NEXT) {
         double par[9];
         load9(S.par, W, s, par);
-        const double chi0 = deriv_warp<T>(P, K, rden, par, step, pp, sw, lane, stJ, stR, stR);
+        const double chi0 = deriv_warp<T, FILT>(P, K, rden, par, step, pp, sw, lane, stJ, stR, stR);
         if (lane == 0) {
           double H45[45], g9[9];
           for (int k = 0; k < 45; k++) H45[k] = stR[k];
@@ -841,7 +841,7 @@ __global__ void __launch_bounds__(kBlock) finish_kernel(const __grid_constant__ 
         if (lane == 0) t.svdlim += hits;
         double ptmp[9];
         load9(S.ptmp, W, s, ptmp);
-        chi_new = forward_warp<T>(P, K, rden, ptmp, step, pp, sw, lane, stR);
+        chi_new = forward_warp<T, FILT>(P, K, rden, ptmp, step, pp, sw, lane, stR);
       }
       if (lane == 0) trial_transition<false>(P, A, S, s, st, chi_new, 0, t);
     }
@@ -883,7 +883,7 @@ namespace detail {
 
 // deriv_pass over a group: lane t takes wavelengths t, t + G, ...; every lane
 // returns the full H45, g9 and chi^2 / (4 nl).
-template <class T, int G>
+template <class T, int G, bool FILT>
 __device__ __forceinline__ double deriv_grp(const DevPlan &P, VoigtK<T> &K, T *rden,
                                             const double *par, const double *step,
                                             const double *prof, const double sw[4],
@@ -902,7 +902,7 @@ __device__ __forceinline__ double deriv_grp(const DevPlan &P, VoigtK<T> &K, T *r
 #pragma unroll 1
   for (int iw = grp.lane; iw < nl; iw += G) {
     T syn[4], J[4][9];
-    me_point<T, true>(c, shift_w<T>(c, P, iw), K, tsw, syn, J);
+    channel_point<T, true, FILT>(c, P, K, tsw, iw, syn, J);
     T r[4];
 #pragma unroll
     for (int s = 0; s < 4; s++) {
@@ -929,7 +929,7 @@ __device__ __forceinline__ double deriv_grp(const DevPlan &P, VoigtK<T> &K, T *r
 }
 
 // forward_pass over a group (chi^2 only); every lane gets the result.
-template <class T, int G>
+template <class T, int G, bool FILT>
 __device__ __forceinline__ double forward_grp(const DevPlan &P, VoigtK<T> &K, T *rden,
                                               const double *par, const double *step,
                                               const double *prof, const double sw[4],
@@ -943,7 +943,7 @@ __device__ __forceinline__ double forward_grp(const DevPlan &P, VoigtK<T> &K, T 
 #pragma unroll 1
   for (int iw = grp.lane; iw < nl; iw += G) {
     T syn[4];
-    me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
+    channel_point<T, false, FILT>(c, P, K, ones, iw, syn, nullptr);
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
@@ -956,7 +956,7 @@ __device__ __forceinline__ double forward_grp(const DevPlan &P, VoigtK<T> &K, T 
 }  // namespace detail
 
 // jac_kernel with G lanes per slot of jlist[parity].
-template <class T, int G>
+template <class T, int G, bool FILT>
 __global__ void __launch_bounds__(kBlock, ME_JAC_MINB)
     jac_grp_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ InvertArgs A,
                    const __grid_constant__ Slots S, int parity) {
@@ -982,7 +982,7 @@ __global__ void __launch_bounds__(kBlock, ME_JAC_MINB)
     load9(S.par, W, s, par);
     slot_weights(P, S, s, step, sw);
     double H45[45], g9[9];
-    const double chi0 = deriv_grp<T, G>(P, K, rden, par, step, pp, sw, grp, H45, g9);
+    const double chi0 = deriv_grp<T, G, FILT>(P, K, rden, par, step, pp, sw, grp, H45, g9);
     if (grp.lane == 0) {
       t.jac++;
       jac_store(P, S, s, par, chi0, H45, g9);
@@ -1016,7 +1016,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // trial_kernel with G lanes per slot, over this round's lists (jlist: first
 // trials or run ends; rlist: later trials); no refills.
-template <class T, int G>
+template <class T, int G, bool FILT>
 __global__ void __launch_bounds__(kBlock)
     trial_grp_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ InvertArgs A,
                      const __grid_constant__ Slots S, int parity) {
@@ -1041,12 +1041,119 @@ __global__ void __launch_bounds__(kBlock)
       double ptmp[9], step[9], sw[4];
       load9(S.ptmp, W, s, ptmp);
       slot_weights(P, S, s, step, sw);
-      chi_new = forward_grp<T, G>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl,
+      chi_new = forward_grp<T, G, FILT>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl,
                                   sw, grp);
     }
     if (grp.lane == 0) trial_transition<true>(P, A, S, s, st, chi_new, next_parity, t);
   }
   if (grp.lane == 0) t.flush(A, S);
 }
+
+// ---------------------------------------------------------------------------
+// Launchers, instantiated per synthesis precision T and instrument-filter
+// variant FILT by me_invert_{f32,f64}{,f}.cu (ME_INSTANTIATE_ROUNDS).
+// ---------------------------------------------------------------------------
+// which: 0 = jac_kernel, 1 = trial_kernel, 2 = svd_kernel, 3 = finish_kernel
+// (CTAs for a full device)
+template <class T, bool FILT>
+int round_grid_impl(int which, int device) {
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (which == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jac_kernel<T, FILT>, kBlock, 0);
+  } else if (which == 1) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trial_kernel<T, FILT>, kBlock, 0);
+  } else if (which == 3) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finish_kernel<T, FILT>, kBlock, 0);
+  } else {
+    cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSvdSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, svd_kernel, kSvdBlock, kSvdSmem);
+  }
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
+}
+
+inline void launch_svd_lanes(int lanes, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                             int parity, int which, int grid, cudaStream_t st) {
+  switch (lanes) {
+    case 2: svd_grp_kernel<2><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
+    case 4: svd_grp_kernel<4><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
+    case 8: svd_grp_kernel<8><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
+    default: svd_kernel<<<grid, kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, which); break;
+  }
+}
+
+// grids: jac_kernel, trial_kernel, svd; svd_lanes: lanes per matrix of the
+// SVD launches (1: svd_kernel, one thread each; 2, 4, 8: svd_grp_kernel).
+template <class T, bool FILT>
+cudaError_t launch_round_impl(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
+                              const int grids[3], cudaStream_t st, cudaEvent_t *ev,
+                              int svd_lanes) {
+  if (ev) cudaEventRecord(ev[0], st);
+  jac_kernel<T, FILT><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
+  if (ev) cudaEventRecord(ev[1], st);
+  launch_svd_lanes(svd_lanes, P, A, S, parity, 0, grids[2], st);
+  if (ev) cudaEventRecord(ev[2], st);
+  launch_svd_lanes(svd_lanes, P, A, S, parity, 1, grids[2], st);
+  if (ev) cudaEventRecord(ev[3], st);
+  trial_kernel<T, FILT><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
+  if (ev) cudaEventRecord(ev[4], st);
+  return cudaGetLastError();
+}
+
+template <class T, int G, bool FILT>
+void launch_grp(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
+                const int grids[3], cudaStream_t st, cudaEvent_t *ev) {
+  if (ev) cudaEventRecord(ev[0], st);
+  jac_grp_kernel<T, G, FILT><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
+  if (ev) cudaEventRecord(ev[1], st);
+  svd_grp_kernel<G><<<grids[2], kBlock, 0, st>>>(P, A, S, parity, 0);
+  if (ev) cudaEventRecord(ev[2], st);
+  svd_grp_kernel<G><<<grids[2], kBlock, 0, st>>>(P, A, S, parity, 1);
+  if (ev) cudaEventRecord(ev[3], st);
+  trial_grp_kernel<T, G, FILT><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
+  if (ev) cudaEventRecord(ev[4], st);
+}
+
+// A round with G lanes per slot (G = 2, 4, 8, 16, 32), after the queue is empty.
+template <class T, bool FILT>
+cudaError_t launch_round_grp_impl(int G, const DevPlan &P, const InvertArgs &A, const Slots &S,
+                                  int parity, const int grids[3], cudaStream_t st,
+                                  cudaEvent_t *ev) {
+  switch (G) {
+    case 2: launch_grp<T, 2, FILT>(P, A, S, parity, grids, st, ev); break;
+    case 4: launch_grp<T, 4, FILT>(P, A, S, parity, grids, st, ev); break;
+    case 8: launch_grp<T, 8, FILT>(P, A, S, parity, grids, st, ev); break;
+    case 16: launch_grp<T, 16, FILT>(P, A, S, parity, grids, st, ev); break;
+    case 32: launch_grp<T, 32, FILT>(P, A, S, parity, grids, st, ev); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <class T, bool FILT>
+cudaError_t launch_finish_impl(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
+                               int grid, cudaStream_t st) {
+  finish_kernel<T, FILT><<<grid, kBlock, 0, st>>>(P, A, S, cursor);
+  return cudaGetLastError();
+}
+
+// The externally visible launchers of one (T, FILT) variant, named by SUF.
+#define ME_INSTANTIATE_ROUNDS(T, FILT, SUF)                                                      \
+  int round_grid_##SUF(int which, int device) { return round_grid_impl<T, FILT>(which, device); } \
+  cudaError_t launch_round_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,          \
+                                 int parity, const int grids[3], cudaStream_t st,                \
+                                 cudaEvent_t *ev, int svd_lanes) {                               \
+    return launch_round_impl<T, FILT>(P, A, S, parity, grids, st, ev, svd_lanes);                \
+  }                                                                                              \
+  cudaError_t launch_round_grp_##SUF(int G, const DevPlan &P, const InvertArgs &A,               \
+                                     const Slots &S, int parity, const int grids[3],             \
+                                     cudaStream_t st, cudaEvent_t *ev) {                         \
+    return launch_round_grp_impl<T, FILT>(G, P, A, S, parity, grids, st, ev);                    \
+  }                                                                                              \
+  cudaError_t launch_finish_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,         \
+                                  int *cursor, int grid, cudaStream_t st) {                      \
+    return launch_finish_impl<T, FILT>(P, A, S, cursor, grid, st);                               \
+  }
 
 }  // namespace me

@@ -232,7 +232,10 @@ __global__ void synth_train_kernel(const __grid_constant__ DevPlan P, Prior pr,
   unsigned long long nseed = seed ^ 0x9E3779B97F4A7C15ull;
   for (int iw = 0; iw < nl; iw++) {
     float syn[4];
-    me_point<float, false>(c, shift_w<float>(c, P, iw), K, ones, syn, nullptr);
+    if (P.nsub > 1)
+      channel_point<float, false, true>(c, P, K, ones, iw, syn, nullptr);
+    else
+      channel_point<float, false, false>(c, P, K, ones, iw, syn, nullptr);
     // noise: 4 normals per wavelength from one Philox call
     uint32_t cc[4] = {(uint32_t)((unsigned long long)i & 0xffffffffu),
                       (uint32_t)((unsigned long long)i >> 32), (uint32_t)iw, 0x4E4F4953u};

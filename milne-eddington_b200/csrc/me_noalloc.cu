@@ -175,6 +175,9 @@ extern "C" int me_invert_batch_device_noalloc(const me_config *cfg, const double
   me::DevPlan P;
   int rc = me::build_devplan(cfg, lambda, nl, P);
   if (rc) return set_err(rc, "invalid control file or wavelength grid");
+  // the sub-wavelength grid of an instrument filter would need scratch of its
+  // own: filtered plans go through me_invert_batch_device
+  if (P.nsub > 1) return set_err(ME_ERR_CONFIG, "no instrument filter without allocation");
   if (npix == 0) return ME_OK;
   const int prec = cfg->precision == ME_PREC_FP64 ? 1 : 0;
   DeviceSetup *d = nullptr;

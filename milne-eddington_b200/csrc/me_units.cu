@@ -39,13 +39,17 @@ __global__ void synth_kernel(const DevPlan P, const double *par, long long npix,
   const T ones[4] = {T(1), T(1), T(1), T(1)};
   for (int iw = 0; iw < nl; iw++) {
     T syn[4], J[4][9];
-    const T w0 = shift_w<T>(c, P, iw);
     if (jac) {
-      me_point<T, true>(c, w0, K, ones, syn, J);
+      if (P.nsub > 1)
+        channel_point<T, true, true>(c, P, K, ones, iw, syn, J);
+      else
+        channel_point<T, true, false>(c, P, K, ones, iw, syn, J);
       for (int s = 0; s < 4; s++)
         for (int k = 0; k < 9; k++) jac[((size_t)i * 36 + s * 9 + k) * nl + iw] = (double)J[s][k];
+    } else if (P.nsub > 1) {
+      channel_point<T, false, true>(c, P, K, ones, iw, syn, nullptr);
     } else {
-      me_point<T, false>(c, w0, K, ones, syn, J);
+      channel_point<T, false, false>(c, P, K, ones, iw, syn, nullptr);
     }
     for (int s = 0; s < 4; s++) prof[((size_t)i * 4 + s) * nl + iw] = (double)syn[s];
   }
@@ -75,7 +79,10 @@ __global__ void fit_kernel(const DevPlan P, const double *fitpar, const unsigned
   const T ones[4] = {T(1), T(1), T(1), T(1)};
   for (int iw = 0; iw < nl; iw++) {
     T syn[4];
-    me_point<T, false>(c, shift_w<T>(c, P, iw), K, ones, syn, nullptr);
+    if (P.nsub > 1)
+      channel_point<T, false, true>(c, P, K, ones, iw, syn, nullptr);
+    else
+      channel_point<T, false, false>(c, P, K, ones, iw, syn, nullptr);
     for (int s = 0; s < 4; s++) out[s * nl + iw] = (double)syn[s];
   }
 }
@@ -130,34 +137,39 @@ __global__ void init_guess_kernel(const DevPlan P, const double *prof, long long
 // launchers
 // ---------------------------------------------------------------------------
 
-int round_grid_f32(int which, int device);
-int round_grid_f64(int which, int device);
-cudaError_t launch_round_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                             const int grids[3], cudaStream_t st, cudaEvent_t *ev, int svd_lanes);
-cudaError_t launch_round_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                             const int grids[3], cudaStream_t st, cudaEvent_t *ev, int svd_lanes);
+#define ME_DECLARE_ROUNDS(SUF)                                                                   \
+  int round_grid_##SUF(int which, int device);                                                  \
+  cudaError_t launch_round_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,          \
+                                 int parity, const int grids[3], cudaStream_t st,                \
+                                 cudaEvent_t *ev, int svd_lanes);                                \
+  cudaError_t launch_round_grp_##SUF(int G, const DevPlan &P, const InvertArgs &A,               \
+                                     const Slots &S, int parity, const int grids[3],             \
+                                     cudaStream_t st, cudaEvent_t *ev);                          \
+  cudaError_t launch_finish_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,         \
+                                  int *cursor, int grid, cudaStream_t st);
+ME_DECLARE_ROUNDS(f32)
+ME_DECLARE_ROUNDS(f64)
+ME_DECLARE_ROUNDS(f32f)
+ME_DECLARE_ROUNDS(f64f)
 
-cudaError_t launch_finish_f32(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
-                              int grid, cudaStream_t st);
-cudaError_t launch_finish_f64(const DevPlan &P, const InvertArgs &A, const Slots &S, int *cursor,
-                              int grid, cudaStream_t st);
+// the variant of a plan: synthesis precision, and the instrument filter or not
+#define ME_PICK(FN, ...)                                                                   \
+  (precision == 1 ? (P.nsub > 1 ? FN##_f64f(__VA_ARGS__) : FN##_f64(__VA_ARGS__))           \
+                  : (P.nsub > 1 ? FN##_f32f(__VA_ARGS__) : FN##_f32(__VA_ARGS__)))
+
 cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                           int *cursor, int grid, cudaStream_t st) {
-  return precision == 1 ? launch_finish_f64(P, A, S, cursor, grid, st)
-                        : launch_finish_f32(P, A, S, cursor, grid, st);
+  return ME_PICK(launch_finish, P, A, S, cursor, grid, st);
 }
 
-cudaError_t launch_round_grp_f32(int G, const DevPlan &P, const InvertArgs &A, const Slots &S,
-                               int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev);
-cudaError_t launch_round_grp_f64(int G, const DevPlan &P, const InvertArgs &A, const Slots &S,
-                               int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev);
 cudaError_t launch_round_grp(int precision, int G, const DevPlan &P, const InvertArgs &A,
                              const Slots &S, int parity, const int grids[3], cudaStream_t st,
                              cudaEvent_t *ev) {
-  return precision == 1 ? launch_round_grp_f64(G, P, A, S, parity, grids, st, ev)
-                        : launch_round_grp_f32(G, P, A, S, parity, grids, st, ev);
+  return ME_PICK(launch_round_grp, G, P, A, S, parity, grids, st, ev);
 }
 
+// grids of the unfiltered kernels (the filtered ones run grid-stride loops
+// over the same grids)
 int round_grid(int precision, int which, int device) {
   return precision == 1 ? round_grid_f64(which, device) : round_grid_f32(which, device);
 }
@@ -165,8 +177,7 @@ int round_grid(int precision, int which, int device) {
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                          int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev,
                          int svd_lanes) {
-  return precision == 1 ? launch_round_f64(P, A, S, parity, grids, st, ev, svd_lanes)
-                        : launch_round_f32(P, A, S, parity, grids, st, ev, svd_lanes);
+  return ME_PICK(launch_round, P, A, S, parity, grids, st, ev, svd_lanes);
 }
 
 cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,

@@ -83,6 +83,8 @@ class MeConfig(ctypes.Structure):
         ("lines_seen", ctypes.c_int),
         ("data_path_seen", ctypes.c_int),
         ("wavelength_path_seen", ctypes.c_int),
+        ("filter_fwhm", ctypes.c_double),
+        ("filter_points", ctypes.c_int),
     ]
 
 
@@ -146,7 +148,7 @@ EXPORTED = [
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
     "me_fits_image_info", "me_fits_read", "me_fits_create", "me_fits_write",
-    "me_run_options_default", "me_run", "me_run_config",
+    "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
 ]
 
 
@@ -288,6 +290,7 @@ def lib() -> ctypes.CDLL:
         L.me_fits_read.argtypes = [ctypes.c_char_p, ctypes.c_long, ctypes.c_long, _D]
         L.me_fits_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_long)]
         L.me_fits_write.argtypes = [ctypes.c_char_p, ctypes.c_long, ctypes.c_long, _D]
+        L.me_plan_set_filter.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int]
         L.me_run_options_default.argtypes = [ctypes.POINTER(MeRunOptions)]
         L.me_run.argtypes = [ctypes.c_char_p, ctypes.POINTER(MeRunOptions),
                              ctypes.POINTER(MeRunReport)]
@@ -422,6 +425,15 @@ class Plan:
     @svd_lanes.setter
     def svd_lanes(self, lanes: int):
         lib().me_plan_set_svd_lanes(self._h, int(lanes))
+
+    def set_filter(self, offsets_mA, weights):
+        """Instrument filter: offsets [mA] and weights of each observed wavelength's
+        sub-wavelengths (one offset removes it)."""
+        off = np.ascontiguousarray(offsets_mA, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        assert off.shape == w.shape and off.ndim == 1
+        _check(lib().me_plan_set_filter(self._h, _ptr(off), _ptr(w), off.size),
+               "me_plan_set_filter")
 
     def set_profiling(self, on: bool = True):
         """Per-kernel device time in the stats (CUDA events around every launch)."""

@@ -15,6 +15,14 @@ Workloads (sizes and distributions of the reference-facing benchmark configs):
                           default bounds, Icriteria lowered to 0.01 (S = 1 data).
 * ``fe15648_1024x1024``  the same draws on 1024x1024 px, num_run = 5,
                           chisq_criteria = 1.5.
+* ``fe6173_4096x4096``   4096x4096 px, Fe I 6173.3 A (g_eff = 2.5), a filtergram:
+                          nl = 6 at lambda0 +-34, +-103, +-172 mA, each the mean
+                          through a Gaussian instrument filter of 76 mA FWHM
+                          (keyword ``filter = 76, 21``: 21 sub-wavelengths over
+                          +-1.5 FWHM); draws as fe15648 but Doppler width
+                          ~ U(20, 50) mA; noise sigma = 2e-3; num_run = 5,
+                          chisq_criteria = 1.5, Bounds_Damp 0.05-1.0 (the
+                          drawn damping reaches 0.1).
 * ``fe6302_2048x1024``   2048x1024 px, Fe I 6302.5 A (g_eff = 2.5), nl = 112 at
                           21.5 mA centred on lambda0; 60 % weak-field pixels
                           (B ~ U(0,200) G, eta0 ~ U(1,10)), 40 % strong-field
@@ -42,6 +50,11 @@ WORKLOADS = {
                               ctl={"num_run": "5", "num_iter": "100", "chisq_criteria": "1.5",
                                    "Icriteria": "0.01"},
                               noise=1e-3),
+    "fe6173_4096x4096": dict(lam0=6173.3, geff=2.5, nl=6, npix=4096 * 4096, kind="fe6173",
+                             ctl={"num_run": "5", "num_iter": "100", "chisq_criteria": "1.5",
+                                  "Icriteria": "0.01", "filter": "76, 21",
+                                  "Bounds_Damp": "0.05, 1.0"},
+                             noise=2e-3),
     "fe6302_2048x1024": dict(lam0=6302.5, geff=2.5, nl=112, npix=2048 * 1024, kind="fe6302",
                              ctl={"num_run": "10", "num_iter": "100", "weights": "1, 4, 4, 2",
                                   "Icriteria": "0.01"},
@@ -55,6 +68,8 @@ def wavelengths(name: str) -> np.ndarray:
         return w["lam0"] - 1.2 + 0.04 * np.arange(w["nl"])
     if w["kind"] == "fe6302":
         return w["lam0"] + 0.0215 * (np.arange(w["nl"]) - (w["nl"] - 1) / 2.0)
+    if w["kind"] == "fe6173":
+        return w["lam0"] + 1e-3 * np.array([-172.0, -103.0, -34.0, 34.0, 103.0, 172.0])
     raise KeyError(name)
 
 
@@ -101,9 +116,10 @@ def draw_parameters(name: str, npix: int, seed: int) -> np.ndarray:
     p[:, 5] = rng.uniform(0.1, 0.8, npix)
     p[:, 7] = 1.0
     p[:, 8] = rng.uniform(0.1, 0.6, npix)
-    if w["kind"] == "fe15648":
+    if w["kind"] in ("fe15648", "fe6173"):
         p[:, 0] = rng.uniform(0.0, 3000.0, npix)
-        p[:, 4] = rng.uniform(150.0, 350.0, npix)
+        p[:, 4] = rng.uniform(150.0, 350.0, npix) if w["kind"] == "fe15648" else \
+            rng.uniform(20.0, 50.0, npix)
         p[:, 6] = rng.uniform(2.0, 30.0, npix)
     else:
         weak = rng.uniform(0.0, 1.0, npix) < 0.6

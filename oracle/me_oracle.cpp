@@ -479,6 +479,10 @@ struct meo_plan {
   double w2[4];
   VoigtTables vt;
   std::vector<double> lambda;
+  // instrument filter (an extension; the reference has none): observed
+  // wavelength i = sum_k sub_w[k] * synthesis at flambda[i * nsub + k]
+  int nsub = 1;
+  std::vector<double> sub_w, flambda;
   // per-process scratch of the reference's structures
   std::vector<double> syn, fit, fit_best, ivnoise, jac;
   // STRUCT_STK's syn/fit/fit_best pointers, swapped per accepted trial and per
@@ -510,12 +514,11 @@ void bounds(double *p, const double lim[9][2]) {
   p[2] = ph;
 }
 
-// Milne_Eddington_Single (Src/ME_SOLVER.c:101-366).  syn [4][nw]; jac
-// [4][9][nw] scaled by step[] when deriv.
+// Milne_Eddington_Single (Src/ME_SOLVER.c:101-366) on the grid lambda[nw].
+// syn [4][nw]; jac [4][9][nw] scaled by step[] when deriv.
 template <class R>
-void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *step, R *syn,
-                R *jac) {
-  const int nw = P.nw;
+void synthesize_on(const meo_plan &P, const double *lambda, int nw, const double *mp, bool deriv,
+                   const double *step, R *syn, R *jac) {
   const R p4 = mp[4], p5 = mp[5], p6 = mp[6], p7 = mp[7], p8 = mp[8];
   const R eta_half = 0.5 * p6;
   const R b0 = p7 * p8;
@@ -541,7 +544,7 @@ void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *s
 
   for (int iw = 0; iw < nw; iw++) {
     R phi[3], psi[3], dphi[3][6], dpsi[3][6];
-    R shift_w = 1e3 * P.lambda[iw] / p4 + shift_v;
+    R shift_w = 1e3 * lambda[iw] / p4 + shift_v;
     for (int q = -1; q <= 1; q++) {
       int k = q + 1;
       R v = shift_w + q * shift_b;
@@ -682,6 +685,61 @@ void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *s
     jU[8 * nw + iw] = (T * (a1s * eta[2] + a1 * c2 + rho[2] * er)) * s8;
     jV[8 * nw + iw] = (T * (a1s * eta[3] + a1 * c3 + rho[3] * er)) * s8;
   }
+}
+
+// The synthesis the inversion sees: Milne_Eddington_Single on the plan's
+// grid, or, with an instrument filter (no reference counterpart), on the
+// filter's sub-wavelengths followed by the weighted sum over each observed
+// wavelength's sub-wavelengths (in order, from zero) of the profiles and of
+// the Jacobian rows.
+template <class R>
+void synthesize(const meo_plan &P, const double *mp, bool deriv, const double *step, R *syn,
+                R *jac) {
+  if (P.nsub <= 1) {
+    synthesize_on<R>(P, P.lambda.data(), P.nw, mp, deriv, step, syn, jac);
+    return;
+  }
+  const int nl = P.nw, K = P.nsub, nf = nl * K;
+  std::vector<R> fs((size_t)4 * nf), fj(deriv ? (size_t)36 * nf : 0);
+  synthesize_on<R>(P, P.flambda.data(), nf, mp, deriv, step, fs.data(),
+                   deriv ? fj.data() : nullptr);
+  for (int row = 0; row < 4; row++)
+    for (int i = 0; i < nl; i++) {
+      R acc = 0;
+      for (int k = 0; k < K; k++) acc += P.sub_w[k] * fs[(size_t)row * nf + i * K + k];
+      syn[row * nl + i] = acc;
+    }
+  if (deriv)
+    for (int row = 0; row < 36; row++)
+      for (int i = 0; i < nl; i++) {
+        R acc = 0;
+        for (int k = 0; k < K; k++) acc += P.sub_w[k] * fj[(size_t)row * nf + i * K + k];
+        jac[row * nl + i] = acc;
+      }
+}
+
+// The Gaussian table of the `filter` keyword: `points` offsets uniform over
+// +-1.5 FWHM [mA], weights exp(-d^2 / 2 sigma^2) normalised to sum 1.
+void gaussian_filter(double fwhm, int points, std::vector<double> &off, std::vector<double> &w) {
+  off.assign(points, 0.0);
+  w.assign(points, 1.0);
+  if (points <= 1) return;
+  const double sigma = fwhm / (2.0 * sqrt(2.0 * log(2.0)));
+  double sum = 0.0;
+  for (int k = 0; k < points; k++) {
+    off[k] = -1.5 * fwhm + 3.0 * fwhm * k / (points - 1);
+    w[k] = exp(-off[k] * off[k] / (2.0 * sigma * sigma));
+    sum += w[k];
+  }
+  for (int k = 0; k < points; k++) w[k] /= sum;
+}
+
+void set_filter(meo_plan *P, const double *off_mA, const double *w, int K) {
+  P->nsub = K;
+  P->sub_w.assign(w, w + K);
+  P->flambda.resize((size_t)P->nw * K);
+  for (int i = 0; i < P->nw; i++)
+    for (int k = 0; k < K; k++) P->flambda[(size_t)i * K + k] = P->lambda[i] + off_mA[k] * 1e-3;
 }
 
 // Per-pixel state of the reference's STRUCT_STK / STRUCT_PARA / STRUCT_LM.
@@ -1128,7 +1186,25 @@ extern "C" int meo_plan_create(const me_config *cfg, const double *lambda, int n
   P->syn_p = P->syn.data();
   P->fit_p = P->fit.data();
   P->fitbest_p = P->fit_best.data();
+  if (cfg->filter_fwhm > 0 && cfg->filter_points > 1) {
+    std::vector<double> off, w;
+    gaussian_filter(cfg->filter_fwhm, cfg->filter_points, off, w);
+    set_filter(P, off.data(), w.data(), cfg->filter_points);
+  }
   *out = P;
+  return ME_OK;
+}
+
+extern "C" int meo_plan_set_filter(meo_plan *p, const double *offsets_mA, const double *weights,
+                                   int k) {
+  if (!p || k < 1 || k > ME_MAX_FILTER || (k > 1 && (!offsets_mA || !weights))) return ME_ERR_ARG;
+  if (k == 1) {
+    p->nsub = 1;
+    p->sub_w.clear();
+    p->flambda.clear();
+    return ME_OK;
+  }
+  set_filter(p, offsets_mA, weights, k);
   return ME_OK;
 }
 

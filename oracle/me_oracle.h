@@ -25,6 +25,11 @@ extern "C" {
 typedef struct meo_plan meo_plan;
 
 int meo_plan_create(const me_config *cfg, const double *lambda, int nl, meo_plan **out);
+/* Instrument filter (an extension; the reference has none): observed
+ * wavelength i becomes sum_k weights[k] * synthesis(lambda_i + offsets_mA[k] / 1e3),
+ * for the profiles and the Jacobian; k = 1 removes it.  The `filter` keyword
+ * sets the Gaussian table (offsets uniform over +-1.5 FWHM). */
+int meo_plan_set_filter(meo_plan *p, const double *offsets_mA, const double *weights, int k);
 void meo_plan_destroy(meo_plan *p);
 int meo_plan_facts(const meo_plan *p, me_plan_facts *out);
 

@@ -47,6 +47,7 @@ def oracle_lib():
         L = ctypes.CDLL(ORACLE_SO)
         L.meo_plan_create.argtypes = [ctypes.POINTER(me_b200.MeConfig), _D, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_void_p)]
+        L.meo_plan_set_filter.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int]
         L.meo_plan_destroy.argtypes = [ctypes.c_void_p]
         L.meo_plan_destroy.restype = None
         L.meo_plan_facts.argtypes = [ctypes.c_void_p, ctypes.POINTER(me_b200.MePlanFacts)]
@@ -76,6 +77,12 @@ class Oracle:
         assert st == 0, st
         self.h = h
         self.carry = np.zeros(1)
+
+    def set_filter(self, offsets_mA, weights):
+        off = np.ascontiguousarray(offsets_mA, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        st = oracle_lib().meo_plan_set_filter(self.h, _p(off), _p(w), off.size)
+        assert st == 0, st
 
     def close(self):
         if self.h:
