@@ -88,7 +88,12 @@ def _cpu_worker_invert(prof):
     return eng.invert(prof, rng_mode=ob.MEO_RNG_NR, nr_seed=1)
 
 
-def cpu_kind():
+def cpu_kind(workload="fe15648_1024x1024"):
+    """The reference's own core where it was built here and the workload is
+    within its reach; the oracle port (the same algorithm restated, with the
+    instrument-filter extension) otherwise."""
+    if me_maps.WORKLOADS[workload]["ctl"].get("filter", "0") != "0":
+        return "port"
     return "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libmeref.so")) \
         else "port"
 
@@ -96,7 +101,7 @@ def cpu_kind():
 def cpu_invert(prof, workload, procs, widen):
     """Inverts prof [n][4][nl] with `procs` processes of the reference core;
     returns (results, seconds, kind)."""
-    kind = cpu_kind()
+    kind = cpu_kind(workload)
     n = prof.shape[0]
     procs = max(1, min(procs, n))
     chunks = np.array_split(np.arange(n), procs)
@@ -187,7 +192,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="fe15648_1024x1024", choices=list(me_maps.WORKLOADS))
-    ap.add_argument("--bounds", default="widened", choices=["widened", "literal"])
+    ap.add_argument("--bounds", default="auto", choices=["auto", "widened", "literal"],
+                    help="auto: widened Doppler/damping bounds for the Fe I 15648 A maps, "
+                         "the workload's own otherwise")
     ap.add_argument("--npix", type=int, default=0, help="override the map size (testing)")
     ap.add_argument("--precision", default="FP32", choices=["FP32", "FP64"])
     ap.add_argument("--sample", type=int, default=4096,
@@ -199,13 +206,19 @@ def parse():
     return ap.parse_args()
 
 
+def use_widened(args):
+    if args.bounds == "auto":
+        return me_maps.WORKLOADS[args.workload]["kind"] == "fe15648"
+    return args.bounds == "widened"
+
+
 def reference_arm(args):
     """The reference's own CPU implementation on this host's cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     w = me_maps.WORKLOADS[args.workload]
-    widen = args.bounds == "widened"
+    widen = use_widened(args)
     cores = host_cores()
     # ~7 ms of one core per pixel at num_run = 5: a step of ~2 s on all cores
     npix = args.npix or max(cores * 48, 256)
@@ -222,7 +235,8 @@ def reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded draws of the workload's parameter distributions)",
-            "config": {"workload": args.workload, "bounds": args.bounds,
+            "config": {"workload": args.workload,
+                       "bounds": "widened" if widen else "workload's own",
                        "pixels_per_step": npix,
                        "num_run": int(w["ctl"].get("num_run", 4)), "nl": w["nl"],
                        "init": "Init_Guess + random restarts (the reference's algorithm)",
@@ -342,7 +356,7 @@ def main():
 
     w = me_maps.WORKLOADS[args.workload]
     name = args.workload
-    widen = args.bounds == "widened"
+    widen = use_widened(args)
     npix = args.npix or w["npix"]
     lam = me_maps.wavelengths(name)
     nl = lam.size
@@ -372,7 +386,7 @@ def main():
     t0 = time.perf_counter()
     torch.cuda.nvtx.range_push("train")
     init = me_b200.Initializer.train(plan, samples=args.train_samples, epochs=args.train_epochs,
-                                     seed=20240607 + 7919 * rank)
+                                     seed=20240607 + 7919 * rank, **me_maps.train_prior(name))
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
@@ -491,7 +505,8 @@ def main():
             "dtype": "f32+f64 (MLP bf16)" if args.precision == "FP32" else "f64 (MLP bf16)",
             "data": "synthetic (seeded draws of the workload's parameter distributions, "
                     "GPU FP64 synthesis + Gaussian noise)",
-            "config": {"workload": name, "bounds": args.bounds, "pixels_per_gpu": npix,
+            "config": {"workload": name, "bounds": "widened" if widen else "workload's own",
+                       "pixels_per_gpu": npix,
                        "nl": nl, "num_run": int(w["ctl"].get("num_run", 4)),
                        "chisq_criteria": float(w["ctl"].get("chisq_criteria", 1.0)),
                        "precision": args.precision,

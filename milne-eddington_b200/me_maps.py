@@ -129,6 +129,19 @@ def draw_parameters(name: str, npix: int, seed: int) -> np.ndarray:
     return p
 
 
+def train_prior(name: str) -> dict:
+    """Training-set overrides of me_mlp_train_params for a workload's learned
+    initialiser (its parameter distributions and noise; the defaults are the
+    Fe I 15648.5 A maps')."""
+    w = WORKLOADS[name]
+    if w["kind"] == "fe6173":
+        return {"doppler_range": (20.0, 50.0), "noise": w["noise"]}
+    if w["kind"] == "fe6302":
+        return {"b_range": (0.0, 3500.0), "doppler_range": (60.0, 140.0), "eta_range": (1.0, 30.0),
+                "noise": w["noise"]}
+    return {}
+
+
 def add_noise(prof: np.ndarray, sigma: float, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed + 7919)
     return prof + rng.normal(0.0, sigma, prof.shape)
