@@ -204,6 +204,11 @@ void me_plan_set_max_group(me_plan *plan, int lanes);
  * or 8); more lanes cut the decomposition's latency, fewer keep more of them
  * in flight.  Default 1. */
 int me_plan_svd_lanes(const me_plan *plan);
+/* The LM rounds between two checks of the queue go to the GPU as one CUDA
+ * graph, captured once per batch for each lane-group size (default on; off:
+ * one launch per kernel).  Profiling (me_plan_set_profiling) launches
+ * directly. */
+void me_plan_set_graphs(me_plan *plan, int on);
 void me_plan_set_svd_lanes(me_plan *plan, int lanes);
 /* Records CUDA events around every inversion launch and reports per-kernel
  * device time in me_stats (off by default; costs a little host time). */

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "../../include/me_b200.h"
@@ -113,6 +114,7 @@ struct me_plan {
   // largest lane group per slot in the rounds once the queue is empty (1: one
   // thread per slot throughout)
   int max_group = 32;
+  bool use_graphs = true;  // rounds between polls as one CUDA graph launch
   int svd_lanes = 1;  // lanes per matrix of the SVD launches in the full rounds
   long long finish_launches = 0;  // tail-kernel launches of the current batch
   // per-kernel device time (me_plan_set_profiling): events recorded around
@@ -420,6 +422,10 @@ extern "C" void me_plan_set_profiling(me_plan *p, int on) {
   if (p) p->profile = on != 0;
 }
 
+extern "C" void me_plan_set_graphs(me_plan *p, int on) {
+  if (p) p->use_graphs = on != 0;
+}
+
 extern "C" int me_plan_svd_lanes(const me_plan *p) { return p ? p->svd_lanes : 0; }
 extern "C" void me_plan_set_svd_lanes(me_plan *p, int lanes) {
   if (p) p->svd_lanes = lanes >= 8 ? 8 : lanes >= 4 ? 4 : lanes >= 2 ? 2 : 1;
@@ -540,25 +546,81 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
   int parity = 0;
   int group = 1;              // lanes per slot of the next rounds
   int ggrids[3] = {1, 1, 1};  // their grids
+  // executable graphs of poll_rounds rounds: index 0 one thread per slot,
+  // 1..5 lane groups of 2..32; they hold this queue's arguments, so they live
+  // for this call only
+  cudaGraphExec_t graphs[6] = {};
+  auto group_index = [](int g) {
+    int i = 0;
+    while (g > 1) {
+      g >>= 1;
+      i++;
+    }
+    return i;
+  };
+  auto release_graphs = [&]() {
+    for (cudaGraphExec_t &x : graphs)
+      if (x) {
+        cudaGraphExecDestroy(x);
+        x = nullptr;
+      }
+  };
+  struct GraphGuard {
+    std::function<void()> f;
+    ~GraphGuard() { f(); }
+  } graph_guard{release_graphs};
   rounds = 0;
   // every slot step is one round: a bound no valid batch reaches
   const double round_cap = (double)me::slot_step_cap(p->P) * (double)((A.count + W - 1) / W + 1);
   while (true) {
     if ((double)rounds > round_cap)
       return fail(ME_ERR_TIMEOUT, "inversion rounds exceeded their bound");
-    for (int r = 0; r < p->poll_rounds; r++) {
-      cudaEvent_t *ev = nullptr;
-      if (p->profile) {
-        const size_t first = p->ev_used;
-        ev = take_events(p, 5);
-        if (ev) p->ev_marks.push_back({0, first});
+    // the rounds between two polls: one CUDA graph per lane-group size,
+    // captured once per queue on the plan's stream (an even number of rounds
+    // starts every batch at parity 0), or direct launches when profiling
+    cudaGraphExec_t *gx = (p->use_graphs && !p->profile && p->poll_rounds % 2 == 0)
+                              ? &graphs[group_index(group)]
+                              : nullptr;
+    if (gx && !*gx) {
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = cudaSuccess;
+      for (int r = 0; r < p->poll_rounds && e == cudaSuccess; r++)
+        e = group > 1 ? me::launch_round_grp(p->precision, group, p->P, A, S, r & 1, ggrids,
+                                             p->stream)
+                      : me::launch_round(p->precision, p->P, A, S, r & 1, grids, p->stream,
+                                         nullptr, p->svd_lanes);
+      const cudaError_t e2 = cudaStreamEndCapture(p->stream, &g);
+      if (e == cudaSuccess) e = e2;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(gx, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        release_graphs();
+        return fail(ME_ERR_CUDA, std::string("round graph: ") + cudaGetErrorString(e));
       }
-      if (group > 1)
-        CK(me::launch_round_grp(p->precision, group, p->P, A, S, parity, ggrids, st, ev));
-      else
-        CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st, ev, p->svd_lanes));
-      parity ^= 1;
-      rounds++;
+    }
+    if (gx) {
+      const cudaError_t e = cudaGraphLaunch(*gx, st);
+      if (e != cudaSuccess) {
+        release_graphs();
+        return fail(ME_ERR_CUDA, std::string("round graph launch: ") + cudaGetErrorString(e));
+      }
+      rounds += p->poll_rounds;
+    } else {
+      for (int r = 0; r < p->poll_rounds; r++) {
+        cudaEvent_t *ev = nullptr;
+        if (p->profile) {
+          const size_t first = p->ev_used;
+          ev = take_events(p, 5);
+          if (ev) p->ev_marks.push_back({0, first});
+        }
+        if (group > 1)
+          CK(me::launch_round_grp(p->precision, group, p->P, A, S, parity, ggrids, st, ev));
+        else
+          CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st, ev, p->svd_lanes));
+        parity ^= 1;
+        rounds++;
+      }
     }
     CK(cudaMemcpyAsync(p->h_poll, A.next, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(p->h_poll + 1, S.busy, sizeof(int), cudaMemcpyDeviceToHost, st));

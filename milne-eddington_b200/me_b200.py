@@ -143,7 +143,7 @@ EXPORTED = [
     "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
-    "me_plan_svd_lanes", "me_plan_set_svd_lanes",
+    "me_plan_svd_lanes", "me_plan_set_svd_lanes", "me_plan_set_graphs",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
@@ -240,6 +240,8 @@ def lib() -> ctypes.CDLL:
         L.me_plan_max_group.argtypes = [ctypes.c_void_p]
         L.me_plan_set_max_group.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_max_group.restype = None
+        L.me_plan_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_graphs.restype = None
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
         L.me_plan_set_svd_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_svd_lanes.restype = None
@@ -434,6 +436,10 @@ class Plan:
         assert off.shape == w.shape and off.ndim == 1
         _check(lib().me_plan_set_filter(self._h, _ptr(off), _ptr(w), off.size),
                "me_plan_set_filter")
+
+    def set_graphs(self, on: bool = True):
+        """Rounds between queue checks as one CUDA graph launch (default on)."""
+        lib().me_plan_set_graphs(self._h, int(bool(on)))
 
     def set_profiling(self, on: bool = True):
         """Per-kernel device time in the stats (CUDA events around every launch)."""
