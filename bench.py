@@ -203,6 +203,8 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--plain-steps", type=int, default=-1, help="timed plain-LM steps (-1: K)")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="tune each arm's plan on the map before timing (me_plan_autotune)")
     return ap.parse_args()
 
 
@@ -391,6 +393,9 @@ def main():
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     plan.set_initializer(init)
+    tuned, tuned_plain = None, None
+    if args.autotune:
+        tuned = plan.autotune(prof.data_ptr(), npix, stream.cuda_stream)
 
     def step():
         return plan.invert_device(prof.data_ptr(), npix, res.data_ptr(), 0, stream.cuda_stream)
@@ -424,6 +429,8 @@ def main():
     plain_steps = args.steps if args.plain_steps < 0 else args.plain_steps
     plain_s, plain_last = None, None
     if plain_steps > 0:
+        if args.autotune:
+            tuned_plain = plain.autotune(prof.data_ptr(), npix, stream.cuda_stream)
         step_plain()  # warm-up (slot buffers, caches)
         nvtx.range_push("plain")
         el, pst = timed_steps(torch, step_plain, plain_steps, stream, dist)
@@ -525,6 +532,7 @@ def main():
                        "runs_per_pixel": last["runs"] / max(1, last["valid"]),
                        "ended_after_learned_start": last["learned_done"] / max(1, last["valid"]),
                        "init_ms_per_step": init_ms,
+                       "autotuned": {"learned": tuned, "plain": tuned_plain},
                        "plain_lm": plain_cfg,
                        "learned_vs_plain": (value / plain_cfg["converged_pixels_per_s"]
                                             if plain_cfg else None),

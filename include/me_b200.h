@@ -215,6 +215,22 @@ void me_plan_set_svd_lanes(me_plan *plan, int lanes);
 void me_plan_set_profiling(me_plan *plan, int on);
 void me_plan_set_tail_slots(me_plan *plan, int slots);
 
+/* Autotuner: times me_invert_batch_device on the caller's batch (device
+ * profiles d_prof [npix][4][nl], ideally of the size and kind the plan will
+ * invert) for candidate values of the plan's runtime knobs -- pixels in
+ * flight (window), lanes per pixel after the queue drains (max_group), the
+ * tail kernel's threshold (tail_slots), lanes per SVD (svd_lanes) -- one knob
+ * at a time, keeping each improvement, and leaves the best setting on the
+ * plan.  The carried LM chi^2 is restored afterwards.  out (may be NULL)
+ * receives the choice, its time and the number of timed runs. */
+typedef struct me_tune_result {
+  int window, max_group, tail_slots, svd_lanes;
+  double ms;    /* device time of the batch with the chosen setting */
+  int trials;   /* batches timed */
+} me_tune_result;
+int me_plan_autotune(me_plan *plan, const double *d_prof, long npix, void *stream,
+                     me_tune_result *out);
+
 /* Inverts npix pixels.  prof: host [npix][4][nl]; res: host [npix][10];
  * fit: host [npix][4][nl] or NULL (best-fit profiles, zeros when skipped);
  * stats may be NULL.  Replaces INVERSION_MULTI (Src/LM_FIT.c:746-811). */

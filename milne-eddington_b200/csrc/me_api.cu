@@ -1035,3 +1035,81 @@ extern "C" int me_synthesize_jacobian_device(me_plan *p, const double *d_par, lo
   if (!stream) CK(cudaStreamSynchronize(st));
   return ME_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Autotuner: a greedy coordinate search over the plan's runtime knobs, each
+// candidate timed (CUDA events on the stream) on the caller's batch.
+// ---------------------------------------------------------------------------
+extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, void *stream,
+                                me_tune_result *out) {
+  if (!p || !d_prof || npix <= 0) return fail(ME_ERR_ARG, "autotune needs a non-empty batch");
+  CK(cudaSetDevice(p->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+  CK(p->d_res.ensure((size_t)npix * 10 * sizeof(double)));
+  const double carry = p->carry;
+  const bool prof = p->profile;
+  p->profile = false;
+  int trials = 0;
+  auto run = [&](double &ms) -> int {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    p->carry = carry;
+    cudaEventRecord(a, st);
+    int rc = me_invert_batch_device(p, d_prof, npix, p->d_res.as<double>(), nullptr, st, nullptr);
+    cudaEventRecord(b, st);
+    if (!rc) rc = cudaEventSynchronize(b) == cudaSuccess ? ME_OK : fail(ME_ERR_CUDA, "autotune");
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ms = t;
+    trials++;
+    return rc;
+  };
+  double best = 0.0;
+  int rc = run(best);  // warm-up (buffers sized for the batch)
+  if (!rc) rc = run(best);
+  struct Knob {
+    int *field;
+    std::vector<int> cand;
+  };
+  const int w0 = p->window > 0 ? p->window : 131072;
+  std::vector<Knob> knobs = {
+      {&p->window, {w0 / 2, w0, w0 * 2}},
+      {&p->max_group, {1, 8, 32}},
+      {&p->tail_slots, {0, -1, p->grid_fin * (me::kBlock / 32) * 2}},
+      {&p->svd_lanes, {1, 2}},
+  };
+  for (Knob &k : knobs) {
+    if (rc) break;
+    int keep = *k.field;
+    for (int c : k.cand) {
+      if (c == keep) continue;
+      const int old = *k.field;
+      *k.field = c;
+      double ms = 0.0;
+      rc = run(ms);
+      if (rc) break;
+      if (ms < best) {
+        best = ms;
+        keep = c;
+      } else {
+        *k.field = old;
+      }
+    }
+    *k.field = keep;
+  }
+  p->carry = carry;
+  p->profile = prof;
+  if (rc) return rc;
+  if (out) {
+    out->window = p->window;
+    out->max_group = p->max_group;
+    out->tail_slots = p->tail_slots;
+    out->svd_lanes = p->svd_lanes;
+    out->ms = best;
+    out->trials = trials;
+  }
+  return ME_OK;
+}

@@ -144,12 +144,22 @@ EXPORTED = [
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
     "me_plan_svd_lanes", "me_plan_set_svd_lanes", "me_plan_set_graphs",
+    "me_plan_autotune",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
     "me_fits_image_info", "me_fits_read", "me_fits_create", "me_fits_write",
     "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
 ]
+
+
+class MeTuneResult(ctypes.Structure):
+    _fields_ = [("window", ctypes.c_int), ("max_group", ctypes.c_int),
+                ("tail_slots", ctypes.c_int), ("svd_lanes", ctypes.c_int),
+                ("ms", ctypes.c_double), ("trials", ctypes.c_int)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class MeRunOptions(ctypes.Structure):
@@ -240,6 +250,8 @@ def lib() -> ctypes.CDLL:
         L.me_plan_max_group.argtypes = [ctypes.c_void_p]
         L.me_plan_set_max_group.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_max_group.restype = None
+        L.me_plan_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                       ctypes.c_void_p, ctypes.POINTER(MeTuneResult)]
         L.me_plan_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_graphs.restype = None
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
@@ -436,6 +448,14 @@ class Plan:
         assert off.shape == w.shape and off.ndim == 1
         _check(lib().me_plan_set_filter(self._h, _ptr(off), _ptr(w), off.size),
                "me_plan_set_filter")
+
+    def autotune(self, d_prof: int, npix: int, stream: int = 0) -> dict:
+        """me_plan_autotune on device profiles; returns the chosen setting."""
+        r = MeTuneResult()
+        _check(lib().me_plan_autotune(self._h, ctypes.c_void_p(d_prof), npix,
+                                      ctypes.c_void_p(stream) if stream else None,
+                                      ctypes.byref(r)), "me_plan_autotune")
+        return r.as_dict()
 
     def set_graphs(self, on: bool = True):
         """Rounds between queue checks as one CUDA graph launch (default on)."""

@@ -188,3 +188,26 @@ def test_empty_batch_and_bad_args():
         assert res.shape == (0, 10) and st["pixels"] == 0
     with pytest.raises(me_b200.MeError):
         me_b200.Plan(cfg, lam[:3])
+
+
+def test_autotune_picks_a_setting_and_keeps_results_valid():
+    """me_plan_autotune times the plan's knobs on a batch, leaves the best on
+    the plan and restores the carried LM chi^2."""
+    import torch
+    name = "fe15648_64x64"
+    lam = me_maps.wavelengths(name)
+    cfg = me_b200.parse_config_text(me_maps.control_text(name, precision="FP32"))
+    with me_b200.Plan(cfg, lam) as plan:
+        par = me_maps.draw_parameters(name, 4096, 61)
+        prof = me_maps.add_noise(plan.synthesize(par), 1e-3, 61)
+        d_prof = torch.from_numpy(prof).cuda()
+        plan.carry_chisq = 0.25
+        r = plan.autotune(d_prof.data_ptr(), prof.shape[0])
+        assert plan.carry_chisq == 0.25
+        assert r["trials"] >= 4 and r["ms"] > 0
+        assert r["window"] in (65536, 131072, 262144) and r["max_group"] in (1, 8, 32)
+        assert r["svd_lanes"] in (1, 2)
+        assert (plan.window, plan.max_group, plan.tail_slots, plan.svd_lanes) == \
+            (r["window"], r["max_group"], r["tail_slots"], r["svd_lanes"])
+        res, st = plan.invert(prof)
+        assert st["valid"] == prof.shape[0] and (res[:, 9] > 0).all()
