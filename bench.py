@@ -203,6 +203,8 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--plain-steps", type=int, default=-1, help="timed plain-LM steps (-1: K)")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--fp64-sample", type=int, default=16384,
+                    help="pixels of the FP32-vs-FP64 comparison of the plain algorithm (0: off)")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune each arm's plan on the map before timing (me_plan_autotune)")
     return ap.parse_args()
@@ -301,6 +303,21 @@ def param_errors(res, ref):
     d[:, 2] = np.minimum(d[:, 2], np.pi - d[:, 2])  # azimuth is folded into [0, pi)
     return {n: [float(np.median(d[:, k]) * sc), float(np.quantile(d[:, k], 0.99) * sc)]
             for k, (n, sc) in enumerate(zip(names, scale))}
+
+
+def work_histograms(counts):
+    """Per-pixel LM iterations and runs of a step (inverted pixels only):
+    histogram bins 0..29 iterations and 30+, 1..20 runs and 21+."""
+    if counts is None:
+        return None
+    c = counts[counts[:, 0] > 0]
+    it = np.minimum(c[:, 1], 30)
+    runs = np.minimum(c[:, 0], 21)
+    return {"pixels": int(c.shape[0]),
+            "iterations": np.bincount(it, minlength=31).tolist(),
+            "runs": np.bincount(runs, minlength=22)[1:].tolist(),
+            "iterations_median_p99": [float(np.median(c[:, 1])), float(np.quantile(c[:, 1], 0.99))],
+            "trials_per_pixel": float(c[:, 2].mean())}
 
 
 def timed_steps(torch, step, n, stream, dist, clk=None):
@@ -418,6 +435,9 @@ def main():
     kernel_ms = statistics.mean(s["kernel_ms"] for s in stats)
     init_ms = statistics.mean(s["init_ms"] for s in stats)
 
+    # ---- per-pixel LM work of the last learned-start step
+    counts_learned = plan.last_counters(npix)
+
     # ---- one more step with per-kernel CUDA events (outside the timed region)
     nvtx.range_push("profiled")
     plan.set_profiling(True)
@@ -428,6 +448,7 @@ def main():
     # ---- the plain LM with the reference's restarts, same map and GPU
     plain_steps = args.steps if args.plain_steps < 0 else args.plain_steps
     plain_s, plain_last = None, None
+    counts_plain = None
     if plain_steps > 0:
         if args.autotune:
             tuned_plain = plain.autotune(prof.data_ptr(), npix, stream.cuda_stream)
@@ -436,6 +457,29 @@ def main():
         el, pst = timed_steps(torch, step_plain, plain_steps, stream, dist)
         nvtx.range_pop()
         plain_s, plain_last = el / plain_steps, pst[-1]
+        counts_plain = plain.last_counters(npix)
+
+    # ---- FP32 synthesis against the FP64 path on the GPU: the plain algorithm
+    # on a seeded sample of the map, same pixels, both precisions
+    fp_cmp = None
+    if args.fp64_sample > 0 and args.precision == "FP32":
+        ns = min(npix, args.fp64_sample)
+        sel = torch.from_numpy(np.sort(np.random.default_rng(11).choice(npix, ns, replace=False)))
+        sprof = prof[sel.cuda()].contiguous()
+        out32 = torch.zeros((ns, 10), dtype=torch.float64, device="cuda")
+        out64 = torch.zeros((ns, 10), dtype=torch.float64, device="cuda")
+        ctl64 = me_maps.control_text(name, precision="FP64", seed=seed, widen_bounds=widen)
+        with me_b200.Plan(me_b200.parse_config_text(ctl), lam, device=local) as p32, \
+                me_b200.Plan(me_b200.parse_config_text(ctl64), lam, device=local) as p64:
+            p32.invert_device(sprof.data_ptr(), ns, out32.data_ptr(), 0, stream.cuda_stream)
+            p64.invert_device(sprof.data_ptr(), ns, out64.data_ptr(), 0, stream.cuda_stream)
+        torch.cuda.synchronize()
+        a, b = out32.cpu().numpy(), out64.cpu().numpy()
+        v = b[:, 9] > 0
+        ratio = a[v, 9] / b[v, 9]
+        fp_cmp = {"pixels": int(ns), "param_err_median_p99": param_errors(a[v], b[v]),
+                  "chi2_ratio_q01_q50_q99": [float(np.quantile(ratio, q)) for q in (0.01, 0.5, 0.99)],
+                  "chi2_within_1.05": float(np.mean(ratio <= 1.05))}
 
     # ---- end to end through the host entry point (pinned host buffers)
     e2e = None
@@ -533,6 +577,9 @@ def main():
                        "ended_after_learned_start": last["learned_done"] / max(1, last["valid"]),
                        "init_ms_per_step": init_ms,
                        "autotuned": {"learned": tuned, "plain": tuned_plain},
+                       "histograms": {"learned": work_histograms(counts_learned),
+                                      "plain": work_histograms(counts_plain)},
+                       "fp32_vs_fp64_plain": fp_cmp,
                        "plain_lm": plain_cfg,
                        "learned_vs_plain": (value / plain_cfg["converged_pixels_per_s"]
                                             if plain_cfg else None),

@@ -215,6 +215,11 @@ void me_plan_set_svd_lanes(me_plan *plan, int lanes);
 void me_plan_set_profiling(me_plan *plan, int on);
 void me_plan_set_tail_slots(me_plan *plan, int slots);
 
+/* Per-pixel counters of the plan's last batch: [npix][4] = LM runs,
+ * iterations (syntheses with Jacobian), trial steps, accepted steps; zeros
+ * for skipped pixels.  npix at most the last batch's. */
+int me_plan_last_counters(const me_plan *plan, unsigned int *counters, long npix);
+
 /* Autotuner: times me_invert_batch_device on the caller's batch (device
  * profiles d_prof [npix][4][nl], ideally of the size and kind the plan will
  * invert) for candidate values of the plan's runtime knobs -- pixels in

@@ -422,6 +422,16 @@ extern "C" void me_plan_set_profiling(me_plan *p, int on) {
   if (p) p->profile = on != 0;
 }
 
+extern "C" int me_plan_last_counters(const me_plan *p, unsigned int *counters, long npix) {
+  if (!p || !counters || npix < 0) return fail(ME_ERR_ARG, "null argument");
+  if ((size_t)npix * 4 * sizeof(unsigned int) > p->d_counters.n)
+    return fail(ME_ERR_ARG, "more pixels than the last batch had");
+  CK(cudaSetDevice(p->device));
+  CK(cudaMemcpy(counters, p->d_counters.p, (size_t)npix * 4 * sizeof(unsigned int),
+                cudaMemcpyDeviceToHost));
+  return ME_OK;
+}
+
 extern "C" void me_plan_set_graphs(me_plan *p, int on) {
   if (p) p->use_graphs = on != 0;
 }

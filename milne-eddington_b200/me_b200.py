@@ -144,7 +144,7 @@ EXPORTED = [
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
     "me_plan_svd_lanes", "me_plan_set_svd_lanes", "me_plan_set_graphs",
-    "me_plan_autotune",
+    "me_plan_autotune", "me_plan_last_counters",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
@@ -252,6 +252,8 @@ def lib() -> ctypes.CDLL:
         L.me_plan_set_max_group.restype = None
         L.me_plan_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
                                        ctypes.c_void_p, ctypes.POINTER(MeTuneResult)]
+        L.me_plan_last_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint),
+                                            ctypes.c_long]
         L.me_plan_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_graphs.restype = None
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
@@ -456,6 +458,13 @@ class Plan:
                                       ctypes.c_void_p(stream) if stream else None,
                                       ctypes.byref(r)), "me_plan_autotune")
         return r.as_dict()
+
+    def last_counters(self, npix: int) -> np.ndarray:
+        """[npix][4] runs, iterations, trials, accepted of the last batch."""
+        out = np.zeros((npix, 4), dtype=np.uint32)
+        _check(lib().me_plan_last_counters(self._h, out.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_uint)), npix), "me_plan_last_counters")
+        return out
 
     def set_graphs(self, on: bool = True):
         """Rounds between queue checks as one CUDA graph launch (default on)."""
