@@ -54,6 +54,7 @@ PKG = os.path.join(ROOT, "milne-eddington_b200")
 sys.path.insert(0, PKG)
 
 import me_maps  # noqa: E402
+import me_ranks  # noqa: E402
 
 METRIC = "converged pixels/s on 1 B200 at chi2<=1.05x FP64 ref: learned-init vs plain LM"
 UNIT = "pixels/s"
@@ -218,7 +219,7 @@ def use_widened(args):
 
 def reference_arm(args):
     """The reference's own CPU implementation on this host's cores."""
-    rank = int(os.environ.get("RANK", "0"))
+    rank, _, _ = me_ranks.rank_env()
     if rank != 0:
         return 0
     w = me_maps.WORKLOADS[args.workload]
@@ -338,11 +339,7 @@ def timed_steps(torch, step, n, stream, dist, clk=None):
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    elapsed = ev0.elapsed_time(ev1) / 1e3
-    if dist:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = me_ranks.max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, "cuda")
     return elapsed, stats
 
 
@@ -362,16 +359,9 @@ def main():
     import torch
     import me_b200
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = me_ranks.rank_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+    dist = me_ranks.init("nccl", 600, torch.device("cuda", local))
 
     w = me_maps.WORKLOADS[args.workload]
     name = args.workload
@@ -379,7 +369,7 @@ def main():
     npix = args.npix or w["npix"]
     lam = me_maps.wavelengths(name)
     nl = lam.size
-    seed = 1000 + rank
+    seed = me_ranks.map_seed(rank)
 
     # ---- synthetic map resident in HBM: seeded draws -> GPU FP64 synthesis + noise
     gen = me_b200.Plan(me_b200.parse_config_text(me_maps.control_text(name, precision="FP64")),
@@ -492,11 +482,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             _, st_e2e = plan.invert(h_prof_np)
-        e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = me_ranks.max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, dist, "cuda")
         e2e = {"seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"], "d2h_ms": st_e2e["d2h_ms"]}
 
     res_np = res.cpu().numpy()
