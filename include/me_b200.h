@@ -209,6 +209,10 @@ int me_plan_svd_lanes(const me_plan *plan);
  * one launch per kernel).  Profiling (me_plan_set_profiling) launches
  * directly. */
 void me_plan_set_graphs(me_plan *plan, int on);
+/* The SVD solves of trials after a rejection run on a second stream beside
+ * the Jacobian kernel of the same round (they concern other pixels; default
+ * on).  Profiling launches serially. */
+void me_plan_set_overlap(me_plan *plan, int on);
 void me_plan_set_svd_lanes(me_plan *plan, int lanes);
 /* Records CUDA events around every inversion launch and reports per-kernel
  * device time in me_stats (off by default; costs a little host time). */

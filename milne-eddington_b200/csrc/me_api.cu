@@ -115,6 +115,10 @@ struct me_plan {
   // thread per slot throughout)
   int max_group = 32;
   bool use_graphs = true;  // rounds between polls as one CUDA graph launch
+  // the later-trial SVDs run on a second stream beside the Jacobian kernel
+  bool overlap = true;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int svd_lanes = 1;  // lanes per matrix of the SVD launches in the full rounds
   long long finish_launches = 0;  // tail-kernel launches of the current batch
   // per-kernel device time (me_plan_set_profiling): events recorded around
@@ -336,6 +340,9 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
       p->d_totals.ensure(sizeof(unsigned long long) * 8) ||
       p->d_next.ensure(sizeof(unsigned long long)) ||
       cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) ||
+      cudaStreamCreateWithFlags(&p->stream2, cudaStreamNonBlocking) ||
+      cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) ||
+      cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) ||
       cudaEventCreate(&p->ev0) || cudaEventCreate(&p->ev1) ||
       cudaMemcpy(p->d_lambda.p, lambda, sizeof(double) * nl, cudaMemcpyHostToDevice) ||
       cudaMemcpy(p->d_dlambda.p, dl.data(), sizeof(double) * nl, cudaMemcpyHostToDevice)) {
@@ -394,6 +401,9 @@ extern "C" void me_plan_destroy(me_plan *p) {
   if (p->ev1) cudaEventDestroy(p->ev1);
   for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
   if (p->stream) cudaStreamDestroy(p->stream);
+  if (p->stream2) cudaStreamDestroy(p->stream2);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   delete p;
 }
 
@@ -430,6 +440,10 @@ extern "C" int me_plan_last_counters(const me_plan *p, unsigned int *counters, l
   CK(cudaMemcpy(counters, p->d_counters.p, (size_t)npix * 4 * sizeof(unsigned int),
                 cudaMemcpyDeviceToHost));
   return ME_OK;
+}
+
+extern "C" void me_plan_set_overlap(me_plan *p, int on) {
+  if (p) p->overlap = on != 0;
 }
 
 extern "C" void me_plan_set_graphs(me_plan *p, int on) {
@@ -588,6 +602,8 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     // the rounds between two polls: one CUDA graph per lane-group size,
     // captured once per queue on the plan's stream (an even number of rounds
     // starts every batch at parity 0), or direct launches when profiling
+    me::Overlap ov_storage{p->stream2, p->ev_fork, p->ev_join};
+    const me::Overlap *ov = (p->overlap && !p->profile) ? &ov_storage : nullptr;
     cudaGraphExec_t *gx = (p->use_graphs && !p->profile && p->poll_rounds % 2 == 0)
                               ? &graphs[group_index(group)]
                               : nullptr;
@@ -597,9 +613,9 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
       cudaError_t e = cudaSuccess;
       for (int r = 0; r < p->poll_rounds && e == cudaSuccess; r++)
         e = group > 1 ? me::launch_round_grp(p->precision, group, p->P, A, S, r & 1, ggrids,
-                                             p->stream)
+                                             p->stream, nullptr, ov)
                       : me::launch_round(p->precision, p->P, A, S, r & 1, grids, p->stream,
-                                         nullptr, p->svd_lanes);
+                                         nullptr, p->svd_lanes, ov);
       const cudaError_t e2 = cudaStreamEndCapture(p->stream, &g);
       if (e == cudaSuccess) e = e2;
       if (e == cudaSuccess) e = cudaGraphInstantiate(gx, g, 0);
@@ -625,9 +641,10 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
           if (ev) p->ev_marks.push_back({0, first});
         }
         if (group > 1)
-          CK(me::launch_round_grp(p->precision, group, p->P, A, S, parity, ggrids, st, ev));
+          CK(me::launch_round_grp(p->precision, group, p->P, A, S, parity, ggrids, st, ev, ov));
         else
-          CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st, ev, p->svd_lanes));
+          CK(me::launch_round(p->precision, p->P, A, S, parity, grids, st, ev, p->svd_lanes,
+                              ov));
         parity ^= 1;
         rounds++;
       }

@@ -1088,13 +1088,22 @@ inline void launch_svd_lanes(int lanes, const DevPlan &P, const InvertArgs &A, c
 template <class T, bool FILT>
 cudaError_t launch_round_impl(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
                               const int grids[3], cudaStream_t st, cudaEvent_t *ev,
-                              int svd_lanes) {
+                              int svd_lanes, const Overlap *ov) {
+  if (ov) {  // later trials' SVDs beside the Jacobian kernel
+    cudaEventRecord(ov->fork, st);
+    cudaStreamWaitEvent(ov->aux, ov->fork, 0);
+    launch_svd_lanes(svd_lanes, P, A, S, parity, 1, grids[2], ov->aux);
+    cudaEventRecord(ov->join, ov->aux);
+  }
   if (ev) cudaEventRecord(ev[0], st);
   jac_kernel<T, FILT><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
   if (ev) cudaEventRecord(ev[1], st);
   launch_svd_lanes(svd_lanes, P, A, S, parity, 0, grids[2], st);
   if (ev) cudaEventRecord(ev[2], st);
-  launch_svd_lanes(svd_lanes, P, A, S, parity, 1, grids[2], st);
+  if (ov)
+    cudaStreamWaitEvent(st, ov->join, 0);
+  else
+    launch_svd_lanes(svd_lanes, P, A, S, parity, 1, grids[2], st);
   if (ev) cudaEventRecord(ev[3], st);
   trial_kernel<T, FILT><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
   if (ev) cudaEventRecord(ev[4], st);
@@ -1103,13 +1112,22 @@ cudaError_t launch_round_impl(const DevPlan &P, const InvertArgs &A, const Slots
 
 template <class T, int G, bool FILT>
 void launch_grp(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
-                const int grids[3], cudaStream_t st, cudaEvent_t *ev) {
+                const int grids[3], cudaStream_t st, cudaEvent_t *ev, const Overlap *ov) {
+  if (ov) {
+    cudaEventRecord(ov->fork, st);
+    cudaStreamWaitEvent(ov->aux, ov->fork, 0);
+    svd_grp_kernel<G><<<grids[2], kBlock, 0, ov->aux>>>(P, A, S, parity, 1);
+    cudaEventRecord(ov->join, ov->aux);
+  }
   if (ev) cudaEventRecord(ev[0], st);
   jac_grp_kernel<T, G, FILT><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
   if (ev) cudaEventRecord(ev[1], st);
   svd_grp_kernel<G><<<grids[2], kBlock, 0, st>>>(P, A, S, parity, 0);
   if (ev) cudaEventRecord(ev[2], st);
-  svd_grp_kernel<G><<<grids[2], kBlock, 0, st>>>(P, A, S, parity, 1);
+  if (ov)
+    cudaStreamWaitEvent(st, ov->join, 0);
+  else
+    svd_grp_kernel<G><<<grids[2], kBlock, 0, st>>>(P, A, S, parity, 1);
   if (ev) cudaEventRecord(ev[3], st);
   trial_grp_kernel<T, G, FILT><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
   if (ev) cudaEventRecord(ev[4], st);
@@ -1119,13 +1137,13 @@ void launch_grp(const DevPlan &P, const InvertArgs &A, const Slots &S, int parit
 template <class T, bool FILT>
 cudaError_t launch_round_grp_impl(int G, const DevPlan &P, const InvertArgs &A, const Slots &S,
                                   int parity, const int grids[3], cudaStream_t st,
-                                  cudaEvent_t *ev) {
+                                  cudaEvent_t *ev, const Overlap *ov) {
   switch (G) {
-    case 2: launch_grp<T, 2, FILT>(P, A, S, parity, grids, st, ev); break;
-    case 4: launch_grp<T, 4, FILT>(P, A, S, parity, grids, st, ev); break;
-    case 8: launch_grp<T, 8, FILT>(P, A, S, parity, grids, st, ev); break;
-    case 16: launch_grp<T, 16, FILT>(P, A, S, parity, grids, st, ev); break;
-    case 32: launch_grp<T, 32, FILT>(P, A, S, parity, grids, st, ev); break;
+    case 2: launch_grp<T, 2, FILT>(P, A, S, parity, grids, st, ev, ov); break;
+    case 4: launch_grp<T, 4, FILT>(P, A, S, parity, grids, st, ev, ov); break;
+    case 8: launch_grp<T, 8, FILT>(P, A, S, parity, grids, st, ev, ov); break;
+    case 16: launch_grp<T, 16, FILT>(P, A, S, parity, grids, st, ev, ov); break;
+    case 32: launch_grp<T, 32, FILT>(P, A, S, parity, grids, st, ev, ov); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -1143,13 +1161,13 @@ cudaError_t launch_finish_impl(const DevPlan &P, const InvertArgs &A, const Slot
   int round_grid_##SUF(int which, int device) { return round_grid_impl<T, FILT>(which, device); } \
   cudaError_t launch_round_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,          \
                                  int parity, const int grids[3], cudaStream_t st,                \
-                                 cudaEvent_t *ev, int svd_lanes) {                               \
-    return launch_round_impl<T, FILT>(P, A, S, parity, grids, st, ev, svd_lanes);                \
+                                 cudaEvent_t *ev, int svd_lanes, const Overlap *ov) {            \
+    return launch_round_impl<T, FILT>(P, A, S, parity, grids, st, ev, svd_lanes, ov);            \
   }                                                                                              \
   cudaError_t launch_round_grp_##SUF(int G, const DevPlan &P, const InvertArgs &A,               \
                                      const Slots &S, int parity, const int grids[3],             \
-                                     cudaStream_t st, cudaEvent_t *ev) {                         \
-    return launch_round_grp_impl<T, FILT>(G, P, A, S, parity, grids, st, ev);                    \
+                                     cudaStream_t st, cudaEvent_t *ev, const Overlap *ov) {      \
+    return launch_round_grp_impl<T, FILT>(G, P, A, S, parity, grids, st, ev, ov);                \
   }                                                                                              \
   cudaError_t launch_finish_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,         \
                                   int *cursor, int grid, cudaStream_t st) {                      \

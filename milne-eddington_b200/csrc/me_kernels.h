@@ -118,15 +118,23 @@ cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, 
 // recorded before, between and after the four launches (per-kernel device
 // time when profiling).  svd_lanes: lanes per matrix of the SVD launches
 // (1: svd_kernel; 2, 4, 8: svd_grp_kernel).
+// Overlap (nullable): the later-trial SVD launch runs on ov->aux, forked from
+// st before the Jacobian kernel and joined before the trial kernel (the two
+// lists hold disjoint slots).
+struct Overlap {
+  cudaStream_t aux;
+  cudaEvent_t fork, join;
+};
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                          int parity, const int grids[3], cudaStream_t st,
-                         cudaEvent_t *ev = nullptr, int svd_lanes = 1);
+                         cudaEvent_t *ev = nullptr, int svd_lanes = 1,
+                         const Overlap *ov = nullptr);
 // A round with G lanes per slot (G = 2, 4, 8, 16, 32): for when the queue is
 // empty and the slots in flight are too few to fill the device one thread
 // each.  The trial kernel runs over the round's lists and does not refill.
 cudaError_t launch_round_grp(int precision, int G, const DevPlan &P, const InvertArgs &A,
                              const Slots &S, int parity, const int grids[3], cudaStream_t st,
-                             cudaEvent_t *ev = nullptr);
+                             cudaEvent_t *ev = nullptr, const Overlap *ov = nullptr);
 // Best-fit profiles after a batch: synthesis at fitpar for the inverted
 // pixels (flags bit 0), zeros for the skipped ones.
 cudaError_t launch_fit(int precision, const DevPlan &P, const double *d_fitpar,

@@ -141,10 +141,10 @@ __global__ void init_guess_kernel(const DevPlan P, const double *prof, long long
   int round_grid_##SUF(int which, int device);                                                  \
   cudaError_t launch_round_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,          \
                                  int parity, const int grids[3], cudaStream_t st,                \
-                                 cudaEvent_t *ev, int svd_lanes);                                \
+                                 cudaEvent_t *ev, int svd_lanes, const Overlap *ov);             \
   cudaError_t launch_round_grp_##SUF(int G, const DevPlan &P, const InvertArgs &A,               \
                                      const Slots &S, int parity, const int grids[3],             \
-                                     cudaStream_t st, cudaEvent_t *ev);                          \
+                                     cudaStream_t st, cudaEvent_t *ev, const Overlap *ov);       \
   cudaError_t launch_finish_##SUF(const DevPlan &P, const InvertArgs &A, const Slots &S,         \
                                   int *cursor, int grid, cudaStream_t st);
 ME_DECLARE_ROUNDS(f32)
@@ -164,8 +164,8 @@ cudaError_t launch_finish(int precision, const DevPlan &P, const InvertArgs &A, 
 
 cudaError_t launch_round_grp(int precision, int G, const DevPlan &P, const InvertArgs &A,
                              const Slots &S, int parity, const int grids[3], cudaStream_t st,
-                             cudaEvent_t *ev) {
-  return ME_PICK(launch_round_grp, G, P, A, S, parity, grids, st, ev);
+                             cudaEvent_t *ev, const Overlap *ov) {
+  return ME_PICK(launch_round_grp, G, P, A, S, parity, grids, st, ev, ov);
 }
 
 // grids of the unfiltered kernels (the filtered ones run grid-stride loops
@@ -176,8 +176,8 @@ int round_grid(int precision, int which, int device) {
 
 cudaError_t launch_round(int precision, const DevPlan &P, const InvertArgs &A, const Slots &S,
                          int parity, const int grids[3], cudaStream_t st, cudaEvent_t *ev,
-                         int svd_lanes) {
-  return ME_PICK(launch_round, P, A, S, parity, grids, st, ev, svd_lanes);
+                         int svd_lanes, const Overlap *ov) {
+  return ME_PICK(launch_round, P, A, S, parity, grids, st, ev, svd_lanes, ov);
 }
 
 cudaError_t launch_synth(int precision, const DevPlan &P, const double *d_par, long long npix,

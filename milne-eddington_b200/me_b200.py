@@ -144,7 +144,7 @@ EXPORTED = [
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
     "me_plan_svd_lanes", "me_plan_set_svd_lanes", "me_plan_set_graphs",
-    "me_plan_autotune", "me_plan_last_counters",
+    "me_plan_autotune", "me_plan_last_counters", "me_plan_set_overlap",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
@@ -254,6 +254,8 @@ def lib() -> ctypes.CDLL:
                                        ctypes.c_void_p, ctypes.POINTER(MeTuneResult)]
         L.me_plan_last_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint),
                                             ctypes.c_long]
+        L.me_plan_set_overlap.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_overlap.restype = None
         L.me_plan_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_graphs.restype = None
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
@@ -465,6 +467,10 @@ class Plan:
         _check(lib().me_plan_last_counters(self._h, out.ctypes.data_as(
             ctypes.POINTER(ctypes.c_uint)), npix), "me_plan_last_counters")
         return out
+
+    def set_overlap(self, on: bool = True):
+        """Later-trial SVDs on a second stream beside the Jacobian kernel (default on)."""
+        lib().me_plan_set_overlap(self._h, int(bool(on)))
 
     def set_graphs(self, on: bool = True):
         """Rounds between queue checks as one CUDA graph launch (default on)."""
