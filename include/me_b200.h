@@ -17,6 +17,7 @@
 #define ME_B200_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -361,6 +362,8 @@ typedef struct me_mlp_train_params {
   double s;                     /* source function S0 (continuum units)    */
   double beta_range[2];         /* source function gradient ratio          */
   double noise;                 /* Gaussian noise sigma                    */
+  int gemm;                     /* GEMM kernel, ME_GEMM_TCGEN05 (default)  */
+                                /* or ME_GEMM_MMA_SYNC (defined below)     */
 } me_mlp_train_params;
 
 /* The defaults: the parameter distributions of the Fe I 15648.5 A maps
@@ -407,6 +410,28 @@ int me_mlp_set_params(me_mlp *mlp, const float *params);
  * of the parameters.  No optimiser step is taken. */
 int me_mlp_loss_grad(me_mlp *mlp, const float *x, const float *t, int rows, double *loss,
                      float *grad);
+
+/* The initialiser's GEMM kernel.  ME_GEMM_TCGEN05 (the default): TMA loads
+ * of 128-byte-swizzled BF16 tiles, tcgen05.mma with the FP32 accumulator in
+ * tensor memory, tcgen05.ld epilogue.  ME_GEMM_MMA_SYNC: warp-level
+ * mma.sync m16n8k16, kept for comparison.  Shapes the tcgen05 kernel does
+ * not take (N % 16 != 0, a split-K share not a multiple of 64) run on the
+ * mma.sync kernel whatever is set. */
+#define ME_GEMM_TCGEN05 0
+#define ME_GEMM_MMA_SYNC 1
+int me_mlp_set_gemm(me_mlp *mlp, int path);
+/* GEMM launches of each kernel since the initialiser was made. */
+int me_mlp_gemm_launches(const me_mlp *mlp, long long *tcgen05, long long *mma_sync);
+
+/* One GEMM of the initialiser's kernels, for testing them: with A [m][r] and
+ * Bt [n][r] row-major BF16 bit patterns (host), z [m][n] = A Bt^T + bias
+ * (bias [n] or NULL) and y [m][n] = GELU(z) if gelu else z, FP32 host
+ * buffers (z may be NULL).  split > 1 divides the reduction over that many
+ * CTAs that add into y with atomics (bias NULL, gelu 0, z NULL).  r % 32 ==
+ * 0 and r % (32 split) == 0.  Runs on CUDA device `device`; *ran (may be
+ * NULL) receives the kernel that ran. */
+int me_gemm_bf16(int device, int path, const uint16_t *a, const uint16_t *bt, int m, int n,
+                 int r, int split, const float *bias, int gelu, float *z, float *y, int *ran);
 
 /* ---------------------------------------------------------------------------
  * FITS primary-HDU I/O, the subset of cfitsio the reference's driver uses

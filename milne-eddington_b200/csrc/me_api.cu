@@ -742,6 +742,8 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     CK(cudaEventRecord(p->ev1, st));
     CK(cudaEventSynchronize(p->ev1));
     cudaEventElapsedTime(&init_ms, p->ev0, p->ev1);
+    const int grc = me::mlp_gemm_status(p->init);
+    if (grc) return grc;
     A.init_par = p->d_init.as<double>();
   }
 

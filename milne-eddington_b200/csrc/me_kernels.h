@@ -19,6 +19,9 @@ constexpr int kSvdSmem = (81 + 18) * kSvdBlock * 8;
 // learned initialiser inference: rows per chunk, kernel launches per chunk
 constexpr int kMlpPredChunk = 65536;
 constexpr int kMlpPredLaunches = 6;
+// error status of the initialiser's tensor-core GEMMs since the last call
+// (a bounded wait that expired); synchronises the device (me_mlp.cu)
+int mlp_gemm_status(me_mlp *m);
 
 // Life cycle of an inversion slot (one pixel in flight).
 enum SlotStateCode : int {

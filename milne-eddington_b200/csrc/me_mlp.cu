@@ -11,6 +11,8 @@
 // the backward pass, Adam with FP32 master weights, and the inference that
 // turns a map into per-pixel starting parameters for the LM.  The reference
 // has no learned part; the plain LM with its restarts stays the fallback.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -18,11 +20,13 @@
 #include <string.h>
 
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/me_b200.h"
 #include "me_kernels.h"
+#include "me_umma.cuh"
 
 namespace me {
 namespace mlp {
@@ -146,11 +150,292 @@ __global__ void __launch_bounds__(128) gemm_kernel(const bf16 *__restrict__ A,
   }
 }
 
-// split > 1: R % (split * kTK) == 0, only Yf (zeroed by the caller), no epilogue
-void gemm(const bf16 *A, const bf16 *Bt, int M, int N, int R, const float *bias, float *Z,
-          int gelu, bf16 *Y, float *Yf, cudaStream_t st, int split = 1) {
+// ---------------------------------------------------------------------------
+// The same GEMM and epilogue on the sm_100a tensor cores.  A CTA owns a
+// 128 x bn tile of C (bn = N up to 256, N % 16 == 0); TMA brings 128 x 64 and
+// bn x 64 BF16 tiles of A and Bt into a two-stage ring of 128-byte-swizzled
+// shared memory; thread 0 issues four tcgen05.mma (K = 16 each) per stage into
+// an FP32 accumulator of bn tensor-memory columns and commits each stage to
+// the mbarrier that frees it for the next load; after the last commit every
+// warp reads its 32 accumulator rows with tcgen05.ld and applies the epilogue
+// (bias, Z, GELU, Y, Yf, or split-K atomics) on 16-column chunks.  Waits are
+// bounded: on expiry the CTA writes a code to *err (1: operand load, 2: stage
+// release, 3: accumulator), drains what it issued, frees its tensor memory
+// and leaves C unwritten.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1)
+    umma_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                     const __grid_constant__ CUtensorMap tmB, int M, int N, int R, int bn,
+                     const float *__restrict__ bias, float *__restrict__ Z, int gelu,
+                     bf16 *__restrict__ Y, float *__restrict__ Yf, int *__restrict__ err) {
+  using namespace me::umma;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  const uint32_t stB = (uint32_t)bn * kBK * 2;  // a multiple of 2048: bn % 16 == 0
+  const uint32_t sA = base, sB = base + kStages * kStageA;
+  const uint32_t bars = sB + kStages * stB;
+  // full[s] = bars + 8 s, empty[s] = bars + 8 (kStages + s), done after them
+  const uint32_t done = bars + 8 * 2 * kStages;
+  uint32_t *misc = reinterpret_cast<uint32_t *>(smem_raw + (done + 8 - raw));
+  volatile uint32_t *abort_flag = misc + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ncols = tmem_cols(bn);
+
+  if (warp == 0) {
+    tmem_alloc(smem_u32(misc), ncols);
+    tmem_relinquish();
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < kStages; s++) {
+      mbar_init(bars + 8 * s, 1);
+      mbar_init(bars + 8 * (kStages + s), 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    mbar_fence_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = misc[0];
+
+  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * bn;
+  const int rz = R / (int)gridDim.z, kbeg = blockIdx.z * rz;
+  const int nk = (rz + kBK - 1) / kBK;
+  const uint32_t tx = (uint32_t)(kBM + bn) * kBK * 2;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(kBM, bn);
+      int code = 0, loaded = 0, kb = 0;
+      for (; loaded < nk && loaded < kStages; loaded++) {
+        const uint32_t full = bars + 8 * loaded;
+        mbar_expect_tx(full, tx);
+        tma_load_2d(sA + loaded * kStageA, &tmA, full, kbeg + loaded * kBK, m0);
+        tma_load_2d(sB + loaded * stB, &tmB, full, kbeg + loaded * kBK, n0);
+      }
+      for (; kb < nk; kb++) {
+        const int s = kb % kStages;
+        if (!mbar_wait(bars + 8 * s, (uint32_t)(kb / kStages) & 1u)) {
+          code = 1;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int k = 0; k < kBK / 16; k++)
+          umma_bf16(tmem, sw128_kmajor_desc(sA + s * kStageA + 32 * k),
+                   sw128_kmajor_desc(sB + s * stB + 32 * k), idesc, (kb | k) != 0);
+        mma_commit(bars + 8 * (kStages + s));
+        // refill the stage of the previous k block once its MMAs have read it
+        if (kb >= 1 && loaded < nk) {
+          const int ls = loaded % kStages;  // == (kb - 1) % kStages
+          if (!mbar_wait(bars + 8 * (kStages + ls), (uint32_t)(loaded / kStages - 1) & 1u)) {
+            code = 2;
+            break;
+          }
+          const uint32_t full = bars + 8 * ls;
+          mbar_expect_tx(full, tx);
+          tma_load_2d(sA + ls * kStageA, &tmA, full, kbeg + loaded * kBK, m0);
+          tma_load_2d(sB + ls * stB, &tmB, full, kbeg + loaded * kBK, n0);
+          loaded++;
+        }
+      }
+      mma_commit(done);  // tracks every MMA issued above
+      if (code) {
+        // loads issued and not consumed: let them land before the CTA exits
+        for (int j = kb; j < loaded; j++) mbar_wait(bars + 8 * (j % kStages), (uint32_t)(j / kStages) & 1u);
+        *abort_flag = 1;
+        atomicExch(err, code);
+      }
+    }
+    __syncwarp();
+  }
+  if (!mbar_wait(done, 0)) {
+    *abort_flag = 1;
+    atomicExch(err, 3);
+  }
+  __syncthreads();
+  tc_fence_after();
+  if (!*abort_flag) {
+    const int row = m0 + warp * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c = 0; c < bn; c += 16) {
+      const int n = n0 + c;
+      if (n >= N) break;  // the same for the whole warp
+      float v[16];
+      tmem_ld16(trow + (uint32_t)c, v);
+      if (row >= M) continue;
+      const size_t o = (size_t)row * N + n;
+      if (gridDim.z > 1) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) atomicAdd(Yf + o + j, v[j]);
+        continue;
+      }
+      if (bias) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] += __ldg(bias + n + j);
+      }
+      if (Z) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4 *>(Z + o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+      }
+      if (gelu) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = gelu_f(v[j]);
+      }
+      if (Y) {
+        uint32_t pk[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+          pk[j] = *reinterpret_cast<const uint32_t *>(&h);
+        }
+        *reinterpret_cast<uint4 *>(Y + o) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        *reinterpret_cast<uint4 *>(Y + o + 8) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+      }
+      if (Yf) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4 *>(Yf + o + j) =
+              make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (the library does not link libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                         &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of a row-major BF16 matrix [rows][cols] read in boxes of
+// box_rows x 64 with the 128-byte swizzle; boxes reaching past the matrix
+// read zeros
+bool tile_map(CUtensorMap *map, const bf16 *p, int rows, int cols, int box_rows) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(p) & 15) || (cols * 2) % 16 || box_rows < 1 ||
+      box_rows > 256)
+    return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)me::umma::kBK, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(p), dims, strides, box,
+             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Which GEMM runs: the tcgen05 kernel wherever its shape rules hold (N % 16 ==
+// 0, each split-K share a multiple of 64, tensor maps encodable), else the
+// mma.sync kernel; GemmPath::mma_sync forces the latter.
+enum class GemmPath { tcgen05 = 0, mma_sync = 1 };
+
+// Tensor maps already encoded for a model's buffers: a map is a function of
+// (address, rows, columns, box rows) alone, so a hit is always valid.
+struct TileMapCache {
+  struct Entry {
+    const void *p;
+    int rows, cols, box_rows;
+    CUtensorMap map;
+  };
+  std::vector<Entry> entries;
+};
+
+struct GemmCtx {
+  GemmPath path = GemmPath::tcgen05;
+  int *err = nullptr;             // device flag of the tcgen05 kernel's bounded waits
+  long long *launches = nullptr;  // [2]: launches of each kernel, indexed by GemmPath
+  TileMapCache *maps = nullptr;   // may be null (no caching)
+};
+
+bool cached_tile_map(TileMapCache *c, CUtensorMap *map, const bf16 *p, int rows, int cols,
+                     int box_rows) {
+  if (c)
+    for (const TileMapCache::Entry &e : c->entries)
+      if (e.p == p && e.rows == rows && e.cols == cols && e.box_rows == box_rows) {
+        *map = e.map;
+        return true;
+      }
+  if (!tile_map(map, p, rows, cols, box_rows)) return false;
+  if (c) {
+    if (c->entries.size() >= 256) c->entries.clear();
+    c->entries.push_back({p, rows, cols, box_rows, *map});
+  }
+  return true;
+}
+
+// Per-device facts the launch needs, looked up once per device: the SM count
+// and whether the kernel's shared-memory limit has been raised.
+struct DeviceFacts {
+  int sms = 0;
+  bool smem_ok = false;
+};
+
+const DeviceFacts &device_facts() {
+  static DeviceFacts facts[64];
+  static std::once_flag once[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    static const DeviceFacts none;
+    return none;
+  }
+  std::call_once(once[dev], [dev]() {
+    DeviceFacts f;
+    if (cudaDeviceGetAttribute(&f.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      f.sms = 0;
+    f.smem_ok = cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     me::umma::kSmemMax) == cudaSuccess;
+    facts[dev] = f;
+  });
+  return facts[dev];
+}
+
+// split > 1: R % (split * kTK) == 0, only Yf (zeroed by the caller), no
+// epilogue.  Returns the kernel that ran.
+GemmPath gemm(const GemmCtx &g, const bf16 *A, const bf16 *Bt, int M, int N, int R,
+              const float *bias, float *Z, int gelu, bf16 *Y, float *Yf, cudaStream_t st,
+              int split = 1) {
+  if (g.path == GemmPath::tcgen05 && g.err && N % 16 == 0 && R % split == 0 &&
+      (split == 1 || (R / split) % me::umma::kBK == 0)) {
+    // column tile: all of N up to 256, halved (in multiples of 16, down to
+    // 32) while the grid has fewer than two CTAs per SM, so that small
+    // batches still spread over the GPU
+    const DeviceFacts &dv = device_facts();
+    int bn = N <= me::umma::kMaxBN ? N : me::umma::kMaxBN;
+    const long long tiles_m = (M + me::umma::kBM - 1) / me::umma::kBM;
+    while (bn > 32 && bn % 32 == 0 &&
+           (long long)((N + bn - 1) / bn) * tiles_m * split < 2LL * dv.sms)
+      bn /= 2;
+    CUtensorMap ma, mb;
+    if (dv.smem_ok && cached_tile_map(g.maps, &ma, A, M, R, me::umma::kBM) &&
+        cached_tile_map(g.maps, &mb, Bt, N, R, bn)) {
+      dim3 grid((N + bn - 1) / bn, (M + me::umma::kBM - 1) / me::umma::kBM, split);
+      umma_gemm_kernel<<<grid, 128, me::umma::smem_bytes(bn), st>>>(ma, mb, M, N, R, bn, bias, Z,
+                                                                    gelu, Y, Yf, g.err);
+      if (g.launches) g.launches[(int)GemmPath::tcgen05]++;
+      return GemmPath::tcgen05;
+    }
+  }
   dim3 grid((N + kTN - 1) / kTN, (M + kTM - 1) / kTM, split);
   gemm_kernel<<<grid, 128, 0, st>>>(A, Bt, M, N, R, bias, Z, gelu, Y, Yf);
+  if (g.launches) g.launches[(int)GemmPath::mma_sync]++;
+  return GemmPath::mma_sync;
 }
 
 // out[c][r] = in[r][c] (BF16), rows x cols
@@ -532,11 +817,37 @@ struct me_mlp {
   int cap = 0;
   DBuf xb, xbt, z[kLayers], a[kLayers], at[kLayers], yf, dyb, dybt, dh, dz, dzt, loss;
   DBuf imax;
+  // GEMM kernel choice and the tcgen05 kernel's error flag (device int)
+  GemmPath gemm_path = GemmPath::tcgen05;
+  DBuf gerr;
+  long long gemm_launches[2] = {0, 0};
+  TileMapCache maps;
 };
 
 namespace {
 
 size_t wcount(const me_mlp *m, int l) { return (size_t)m->dout[l] * m->din[l]; }
+
+GemmCtx ctx(me_mlp *m) {
+  GemmCtx g;
+  g.path = m->gemm_path;
+  g.err = m->gerr.as<int>();
+  g.launches = m->gemm_launches;
+  g.maps = &m->maps;
+  return g;
+}
+
+// reads and clears the tcgen05 GEMM's error flag (synchronises the device)
+int gemm_status(me_mlp *m) {
+  if (!m->gerr.p) return ME_OK;
+  int e = 0;
+  MCK(cudaMemcpy(&e, m->gerr.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!e) return ME_OK;
+  MCK(cudaMemset(m->gerr.p, 0, sizeof(int)));
+  static const char *what[] = {"", "operand load", "stage release", "accumulator"};
+  return fail(ME_ERR_CUDA, std::string("tensor-core GEMM: wait for the ") +
+                               what[e >= 1 && e <= 3 ? e : 0] + " timed out");
+}
 
 long long param_count(const me_mlp *m) {
   long long n = 0;
@@ -615,6 +926,8 @@ int alloc_model(me_mlp *m, int nl) {
   m->nl = nl;
   m->nin = 4 * nl;
   m->nip = (m->nin + 31) / 32 * 32;
+  MCK(m->gerr.ensure(sizeof(int)));
+  MCK(cudaMemset(m->gerr.p, 0, sizeof(int)));
   const int din[kLayers] = {m->nip, kHidden, kHidden, kHidden};
   const int dout[kLayers] = {kHidden, kHidden, kHidden, kOutPad};
   for (int l = 0; l < kLayers; l++) {
@@ -670,7 +983,7 @@ void forward(me_mlp *m, int B, bool keep, cudaStream_t st) {
   const bf16 *in = m->xb.as<bf16>();
   for (int l = 0; l < kLayers; l++) {
     const bool last = l == kLayers - 1;
-    gemm(in, m->wb[l].as<bf16>(), B, m->dout[l], m->din[l], m->b[l].as<float>(),
+    gemm(ctx(m), in, m->wb[l].as<bf16>(), B, m->dout[l], m->din[l], m->b[l].as<float>(),
          (!last && keep) ? m->z[l].as<float>() : nullptr, last ? 0 : 1,
          last ? nullptr : m->a[l].as<bf16>(), last ? m->yf.as<float>() : nullptr, st);
     in = m->a[l].as<bf16>();
@@ -691,14 +1004,14 @@ void backward(me_mlp *m, int B, cudaStream_t st) {
     int split = 1;
     while (split < 16 && B % (2 * split * kTK) == 0 && B / (2 * split) >= 256) split *= 2;
     cudaMemsetAsync(m->gw[l].p, 0, wcount(m, l) * 4, st);
-    gemm(dzt, aprevt, dout, din, B, nullptr, nullptr, 0, nullptr, m->gw[l].as<float>(), st, split);
+    gemm(ctx(m), dzt, aprevt, dout, din, B, nullptr, nullptr, 0, nullptr, m->gw[l].as<float>(), st, split);
     cudaMemsetAsync(m->gb[l].p, 0, dout * 4, st);
     const int chunk = 256;
     bias_grad_kernel<<<dim3((dout + 31) / 32, (B + chunk - 1) / chunk), dim3(32, 8), 0, st>>>(
         dcur, B, dout, chunk, m->gb[l].as<float>());
     if (l == 0) break;
     // dA_prev [B][din] = dZ W: GEMM of dZ [B][dout] and W^T [din][dout]
-    gemm(dcur, m->wbt[l].as<bf16>(), B, din, dout, nullptr, nullptr, 0, nullptr,
+    gemm(ctx(m), dcur, m->wbt[l].as<bf16>(), B, din, dout, nullptr, nullptr, 0, nullptr,
          m->dh.as<float>(), st);
     gelu_back_kernel<<<nblk((long long)B * din), 256, 0, st>>>(
         m->dh.as<float>(), m->z[l - 1].as<float>(), (long long)B * din, m->dz.as<bf16>());
@@ -758,7 +1071,9 @@ void prior_from(const me_mlp_train_params *tp, Prior &pr) {
 namespace me {
 // plan constants with device grid pointers, and the plan's device (me_api.cu)
 int plan_devplan(const me_plan *p, DevPlan *out, int *device);
-}
+
+int mlp_gemm_status(me_mlp *m) { return gemm_status(m); }
+}  // namespace me
 
 extern "C" int me_mlp_train_params_default(me_mlp_train_params *tp) {
   if (!tp) return fail(ME_ERR_ARG, "null argument");
@@ -805,6 +1120,8 @@ extern "C" int me_mlp_train(me_plan *plan, const me_mlp_train_params *tp, me_mlp
       tp->samples > (1LL << 31) || !(tp->lr > 0))
     return fail(ME_ERR_ARG,
                 "batch a multiple of 256, batch <= samples <= 2^31, epochs >= 0, lr > 0");
+  if (tp->gemm != ME_GEMM_TCGEN05 && tp->gemm != ME_GEMM_MMA_SYNC)
+    return fail(ME_ERR_ARG, "gemm must be ME_GEMM_TCGEN05 or ME_GEMM_MMA_SYNC");
   me::DevPlan P;
   int device = 0;
   int rc = me::plan_devplan(plan, &P, &device);
@@ -812,6 +1129,7 @@ extern "C" int me_mlp_train(me_plan *plan, const me_mlp_train_params *tp, me_mlp
   MCK(cudaSetDevice(device));
   me_mlp *m = new me_mlp();
   m->device = device;
+  m->gemm_path = tp->gemm == ME_GEMM_TCGEN05 ? GemmPath::tcgen05 : GemmPath::mma_sync;
   rc = alloc_model(m, P.nl);
   if (!rc) rc = init_model(m, tp->seed);
   if (rc) {
@@ -893,6 +1211,8 @@ extern "C" int me_mlp_train(me_plan *plan, const me_mlp_train_params *tp, me_mlp
     double l = 0;
     MCK(cudaMemcpyAsync(&l, m->loss.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     MCK(cudaStreamSynchronize(st));
+    rc = gemm_status(m);
+    if (rc) return rc;
     last = l / (double)steps;
   }
   if (final_loss) *final_loss = last;
@@ -921,7 +1241,10 @@ extern "C" int me_mlp_predict_device(me_mlp *m, const double *d_prof, long npix,
                                                    m->imax.as<float>(), d_par + (size_t)r0 * 9);
   }
   MCK(cudaGetLastError());
-  if (!stream) MCK(cudaStreamSynchronize(st));
+  if (!stream) {
+    MCK(cudaStreamSynchronize(st));
+    return gemm_status(m);
+  }
   return ME_OK;
 }
 
@@ -1006,8 +1329,71 @@ extern "C" int me_mlp_loss_grad(me_mlp *m, const float *x, const float *t, int r
   loss_grad(m, rows, tf.as<float>(), idx.as<long long>(), nullptr);
   MCK(cudaGetLastError());
   MCK(cudaDeviceSynchronize());
+  rc = gemm_status(m);
+  if (rc) return rc;
   MCK(cudaMemcpy(loss, m->loss.p, sizeof(double), cudaMemcpyDeviceToHost));
   return copy_flat(m, true, grad, true);
+}
+
+extern "C" int me_mlp_set_gemm(me_mlp *m, int path) {
+  if (!m) return fail(ME_ERR_ARG, "null argument");
+  if (path != ME_GEMM_TCGEN05 && path != ME_GEMM_MMA_SYNC)
+    return fail(ME_ERR_ARG, "path must be ME_GEMM_TCGEN05 or ME_GEMM_MMA_SYNC");
+  m->gemm_path = path == ME_GEMM_TCGEN05 ? GemmPath::tcgen05 : GemmPath::mma_sync;
+  return ME_OK;
+}
+
+extern "C" int me_mlp_gemm_launches(const me_mlp *m, long long *tcgen05, long long *mma_sync) {
+  if (!m) return fail(ME_ERR_ARG, "null argument");
+  if (tcgen05) *tcgen05 = m->gemm_launches[(int)GemmPath::tcgen05];
+  if (mma_sync) *mma_sync = m->gemm_launches[(int)GemmPath::mma_sync];
+  return ME_OK;
+}
+
+extern "C" int me_gemm_bf16(int device, int path, const uint16_t *a, const uint16_t *bt, int m,
+                            int n, int r, int split, const float *bias, int gelu, float *z,
+                            float *y, int *ran) {
+  if (!a || !bt || !y) return fail(ME_ERR_ARG, "null argument");
+  if (path != ME_GEMM_TCGEN05 && path != ME_GEMM_MMA_SYNC)
+    return fail(ME_ERR_ARG, "path must be ME_GEMM_TCGEN05 or ME_GEMM_MMA_SYNC");
+  if (m < 1 || n < 1 || r < 32 || split < 1 || r % (32 * split))
+    return fail(ME_ERR_ARG, "need m, n >= 1, r >= 32 and r % (32 split) == 0");
+  if (split > 1 && (bias || gelu || z))
+    return fail(ME_ERR_ARG, "a split reduction has no bias, GELU or z");
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0)
+    return fail(ME_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= nd) return fail(ME_ERR_ARG, "device out of range");
+  MCK(cudaSetDevice(device));
+  DBuf da, db, dbias, dz, dy, derr;
+  const size_t mr = (size_t)m * r, nr = (size_t)n * r, mn = (size_t)m * n;
+  MCK(da.ensure(mr * 2));
+  MCK(db.ensure(nr * 2));
+  MCK(dy.ensure(mn * 4));
+  MCK(derr.ensure(sizeof(int)));
+  MCK(cudaMemcpy(da.p, a, mr * 2, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(db.p, bt, nr * 2, cudaMemcpyHostToDevice));
+  MCK(cudaMemset(dy.p, 0, mn * 4));
+  MCK(cudaMemset(derr.p, 0, sizeof(int)));
+  if (bias) {
+    MCK(dbias.ensure((size_t)n * 4));
+    MCK(cudaMemcpy(dbias.p, bias, (size_t)n * 4, cudaMemcpyHostToDevice));
+  }
+  if (z) MCK(dz.ensure(mn * 4));
+  GemmCtx g;
+  g.path = path == ME_GEMM_TCGEN05 ? GemmPath::tcgen05 : GemmPath::mma_sync;
+  g.err = derr.as<int>();
+  const GemmPath used = gemm(g, da.as<bf16>(), db.as<bf16>(), m, n, r, dbias.as<float>(),
+                             dz.as<float>(), gelu, nullptr, dy.as<float>(), nullptr, split);
+  if (ran) *ran = used == GemmPath::tcgen05 ? ME_GEMM_TCGEN05 : ME_GEMM_MMA_SYNC;
+  MCK(cudaGetLastError());
+  MCK(cudaDeviceSynchronize());
+  int e = 0;
+  MCK(cudaMemcpy(&e, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) return fail(ME_ERR_CUDA, "tensor-core GEMM: a bounded wait timed out");
+  MCK(cudaMemcpy(y, dy.p, mn * 4, cudaMemcpyDeviceToHost));
+  if (z) MCK(cudaMemcpy(z, dz.p, mn * 4, cudaMemcpyDeviceToHost));
+  return ME_OK;
 }
 
 // File: "MEMLP001", int32 nl, int32 nin_pad, float fmean[nin_pad],

@@ -150,6 +150,7 @@ EXPORTED = [
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
     "me_fits_image_info", "me_fits_read", "me_fits_create", "me_fits_write",
     "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
+    "me_mlp_set_gemm", "me_mlp_gemm_launches", "me_gemm_bf16",
 ]
 
 
@@ -200,6 +201,7 @@ class MeMlpTrainParams(ctypes.Structure):
         ("s", ctypes.c_double),
         ("beta_range", ctypes.c_double * 2),
         ("noise", ctypes.c_double),
+        ("gemm", ctypes.c_int),
     ]
 
 
@@ -302,6 +304,13 @@ def lib() -> ctypes.CDLL:
         L.me_mlp_get_params.argtypes = [ctypes.c_void_p, _F]
         L.me_mlp_set_params.argtypes = [ctypes.c_void_p, _F]
         L.me_mlp_loss_grad.argtypes = [ctypes.c_void_p, _F, _F, ctypes.c_int, _D, _F]
+        L.me_mlp_set_gemm.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_mlp_gemm_launches.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                           ctypes.POINTER(ctypes.c_longlong)]
+        _U16 = ctypes.POINTER(ctypes.c_uint16)
+        L.me_gemm_bf16.argtypes = [ctypes.c_int, ctypes.c_int, _U16, _U16, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int,
+                                   _F, _F, ctypes.POINTER(ctypes.c_int)]
         _L8 = ctypes.c_long * 8
         L.me_fits_image_info.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int), _L8]
@@ -693,6 +702,45 @@ class Initializer:
         _check(lib().me_mlp_loss_grad(self._h, _fptr(x), _fptr(t), x.shape[0], _ptr(loss),
                                       _fptr(grad)), "me_mlp_loss_grad")
         return float(loss[0]), grad
+
+    def set_gemm(self, path: str):
+        """"tcgen05" (the default) or "mma_sync": the GEMM kernel of training and
+        inference."""
+        _check(lib().me_mlp_set_gemm(self._h, GEMM_PATHS[path]), "me_mlp_set_gemm")
+
+    def gemm_launches(self):
+        """{"tcgen05": n, "mma_sync": n}: GEMM launches of each kernel so far."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().me_mlp_gemm_launches(self._h, ctypes.byref(a), ctypes.byref(b)),
+               "me_mlp_gemm_launches")
+        return {"tcgen05": a.value, "mma_sync": b.value}
+
+
+GEMM_PATHS = {"tcgen05": 0, "mma_sync": 1}
+
+
+def gemm_bf16(a: np.ndarray, bt: np.ndarray, path: str = "tcgen05", split: int = 1,
+              bias: Optional[np.ndarray] = None, gelu: bool = False, device: int = 0):
+    """One GEMM of the initialiser's kernels: a [m][r] and bt [n][r] are BF16
+    bit patterns (uint16); returns (z, y, kernel that ran) with z = a bt^T +
+    bias and y = GELU(z) or z (FP32; z is None for split > 1)."""
+    a = np.ascontiguousarray(a, dtype=np.uint16)
+    bt = np.ascontiguousarray(bt, dtype=np.uint16)
+    m, r = a.shape
+    n = bt.shape[0]
+    assert bt.shape[1] == r
+    y = np.zeros((m, n), dtype=np.float32)
+    z = np.zeros((m, n), dtype=np.float32) if split == 1 else None
+    b = None if bias is None else np.ascontiguousarray(bias, dtype=np.float32)
+    ran = ctypes.c_int(-1)
+    u16 = ctypes.POINTER(ctypes.c_uint16)
+    _check(lib().me_gemm_bf16(device, GEMM_PATHS[path], a.ctypes.data_as(u16),
+                              bt.ctypes.data_as(u16), m, n, r, split,
+                              None if b is None else _fptr(b), int(gelu),
+                              None if z is None else _fptr(z), _fptr(y), ctypes.byref(ran)),
+           "me_gemm_bf16")
+    names = {v: k for k, v in GEMM_PATHS.items()}
+    return z, y, names[ran.value]
 
 
 # ---------------------------------------------------------------------------

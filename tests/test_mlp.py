@@ -130,9 +130,12 @@ def trained():
 
 
 @pytest.mark.gpu
-def test_loss_and_gradient_match_oracle():
+@pytest.mark.parametrize("gemm", ["tcgen05", "mma_sync"])
+def test_loss_and_gradient_match_oracle(gemm):
     plan = fe15648_plan()
     init = me_b200.Initializer.train(plan, samples=256, batch=256, epochs=0)
+    init.set_gemm(gemm)
+    before = init.gemm_launches()
     nl, nip, npar = init.shape()
     assert (nl, nip) == (60, NIN_PAD)
     assert npar == sum(o * i + o for o, i in mo.shapes(nip))
@@ -154,6 +157,10 @@ def test_loss_and_gradient_match_oracle():
     l_x, g_x = mo.loss_grad(p.astype(np.float64), x, t, nip)
     assert abs(loss - l_x) <= 2e-2 * l_x
     assert np.linalg.norm(g - g_x) / np.linalg.norm(g_x) < 5e-2
+    # every GEMM of the forward and backward pass ran on the chosen kernel
+    after = init.gemm_launches()
+    other = "mma_sync" if gemm == "tcgen05" else "tcgen05"
+    assert after[gemm] - before[gemm] == 4 + 4 + 3 and after[other] == before[other]
     init.close()
     plan.close()
 
