@@ -592,23 +592,45 @@ __global__ void standardise_kernel(float *xf, long long n, int cols, const float
   if (X) X[i] = __float2bfloat16(v);
 }
 
-// features of map profiles (FP64 [n][4][nl]) for inference, standardised
-__global__ void map_features_kernel(const double *prof, long long n, int nl, int ld,
-                                    const float *mean, const float *istd, bf16 *X,
-                                    float *imax_out) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// features of map profiles (FP64 [n][4][nl]) for inference, standardised:
+// one warp per profile, each lane on pairs of consecutive features, so that a
+// warp reads 512 contiguous bytes (16-byte loads when the profiles are 16-byte
+// aligned, VEC) and writes 128 contiguous bytes per step.  Every value is the
+// same expression of the same inputs as in the training features.
+template <bool VEC>
+__global__ void __launch_bounds__(256)
+    map_features_kernel(const double *__restrict__ prof, long long n, int nl, int ld,
+                        const float *__restrict__ mean, const float *__restrict__ istd, bf16 *X,
+                        float *imax_out) {
+  const long long i = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;  // the same for the whole warp
   const double *p = prof + (size_t)i * 4 * nl;
   double imax = 0.0;
-  for (int iw = 0; iw < nl; iw++) imax = fmax(imax, p[iw]);
+  for (int iw = lane; iw < nl; iw += 32) imax = fmax(imax, p[iw]);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) imax = fmax(imax, __shfl_xor_sync(0xffffffffu, imax, o));
   const float inv = imax > 0 ? (float)(1.0 / imax) : 0.f;
-  bf16 *x = X + (size_t)i * ld;
-  for (int k = 0; k < 4 * nl; k++) {
-    const float v = feature_value(k / nl, (float)p[k], inv);
-    x[k] = __float2bfloat16((v - mean[k]) * istd[k]);
+  __nv_bfloat162 *x = reinterpret_cast<__nv_bfloat162 *>(X + (size_t)i * ld);
+  const int nf = 4 * nl;  // even, so a pair starting below nf ends below it
+  for (int k = 2 * lane; k < ld; k += 64) {
+    float v0 = 0.f, v1 = 0.f;  // the padding columns stay zero
+    if (k < nf) {
+      double q0, q1;
+      if (VEC) {
+        const double2 q = *reinterpret_cast<const double2 *>(p + k);
+        q0 = q.x;
+        q1 = q.y;
+      } else {
+        q0 = p[k];
+        q1 = p[k + 1];
+      }
+      v0 = (feature_value(k / nl, (float)q0, inv) - mean[k]) * istd[k];
+      v1 = (feature_value((k + 1) / nl, (float)q1, inv) - mean[k + 1]) * istd[k + 1];
+    }
+    x[k >> 1] = __floats2bfloat162_rn(v0, v1);
   }
-  for (int k = 4 * nl; k < ld; k++) x[k] = __float2bfloat16(0.f);
-  imax_out[i] = (float)imax;
+  if (lane == 0) imax_out[i] = (float)imax;
 }
 
 // network outputs (standardised) -> the nine ME parameters [n][9] (FP64)
@@ -1232,9 +1254,15 @@ extern "C" int me_mlp_predict_device(me_mlp *m, const double *d_prof, long npix,
   if (rc) return rc;
   for (long long r0 = 0; r0 < npix; r0 += chunk) {
     const int rows = (int)((npix - r0) < chunk ? (npix - r0) : chunk);
-    map_features_kernel<<<nblk(rows, 128), 128, 0, st>>>(
-        d_prof + (size_t)r0 * 4 * m->nl, rows, m->nl, m->nip, m->fmean.as<float>(),
-        m->fistd.as<float>(), m->xb.as<bf16>(), m->imax.as<float>());
+    // a chunk starts 32 nl r0 bytes in, so its alignment is the base's
+    if ((reinterpret_cast<uintptr_t>(d_prof) & 15) == 0)
+      map_features_kernel<true><<<nblk(rows, 8), 256, 0, st>>>(
+          d_prof + (size_t)r0 * 4 * m->nl, rows, m->nl, m->nip, m->fmean.as<float>(),
+          m->fistd.as<float>(), m->xb.as<bf16>(), m->imax.as<float>());
+    else
+      map_features_kernel<false><<<nblk(rows, 8), 256, 0, st>>>(
+          d_prof + (size_t)r0 * 4 * m->nl, rows, m->nl, m->nip, m->fmean.as<float>(),
+          m->fistd.as<float>(), m->xb.as<bf16>(), m->imax.as<float>());
     forward(m, rows, false, st);
     decode_kernel<<<nblk(rows, 128), 128, 0, st>>>(m->yf.as<float>(), rows, kOutPad,
                                                    m->tmean.as<float>(), m->tstd.as<float>(),

@@ -197,6 +197,75 @@ def test_save_load_roundtrip(trained, tmp_path):
     again.close()
 
 
+def read_initializer(path):
+    """The initialiser file as numpy arrays: nl, nin_pad, feature and target
+    standardisation, flat parameters (the documented layout)."""
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"MEMLP001"
+    nl, nip = np.frombuffer(raw, np.int32, 2, 8)
+    f = np.frombuffer(raw, np.float32, offset=16)
+    fmean, fistd = f[:nip], f[nip:2 * nip]
+    tmean, tstd = f[2 * nip:2 * nip + 10], f[2 * nip + 10:2 * nip + 20]
+    return int(nl), int(nip), fmean, fistd, tmean, tstd, f[2 * nip + 20:]
+
+
+def oracle_predict(path, prof):
+    """The inference restated in numpy: features (I / I_max - 1, 10 Q / I_max,
+    10 U / I_max, 10 V / I_max), standardisation, the network with BF16
+    operands (FP64 sums), de-standardisation and the parameter decode."""
+    nl, nip, fmean, fistd, tmean, tstd, params = read_initializer(path)
+    imax = np.maximum(prof[:, 0, :].max(1), 0.0)
+    inv = np.where(imax > 0, 1.0 / np.where(imax > 0, imax, 1), 0.0)
+    x = np.zeros((prof.shape[0], nip))
+    feat = prof.reshape(prof.shape[0], 4 * nl) * inv[:, None]
+    feat[:, :nl] -= 1.0
+    feat[:, nl:] *= 10.0
+    x[:, :4 * nl] = (feat - fmean[:4 * nl]) * fistd[:4 * nl]
+    y, _ = mo.forward(params.astype(np.float64), x, nip, bf16=True)
+    t = y[:, :10] * tstd + tmean
+    par = np.zeros((prof.shape[0], 9))
+    par[:, 0] = np.maximum(t[:, 0], 0)
+    par[:, 1] = np.arccos(np.clip(t[:, 1], -1, 1))
+    phi = 0.5 * np.arctan2(t[:, 2], t[:, 3])
+    par[:, 2] = np.where(phi < 0, phi + np.pi, phi)
+    par[:, 3:7] = t[:, 4:8]
+    par[:, 7] = t[:, 9] * imax
+    par[:, 8] = t[:, 8]
+    return par
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("aligned", [True, False])
+def test_predict_matches_oracle_inference(trained, tmp_path, aligned):
+    """Map inference (the warp-per-profile feature kernel, the four GEMMs and
+    the decode) against the numpy restatement.  BF16 rounding of activations
+    computed in FP32 on the device and FP64 in the oracle can fall on
+    opposite sides of a rounding boundary, so the bound is statistical."""
+    torch = pytest.importorskip("torch")
+    plan, init = trained
+    path = tmp_path / "init.bin"
+    init.save(path)
+    par = me_maps.draw_parameters("fe15648_1024x1024", 3000, 31)
+    prof = me_maps.add_noise(plan.synthesize(par), 1e-3, 31)
+    want = oracle_predict(path, prof)
+    flat = torch.from_numpy(np.ascontiguousarray(prof).ravel()).cuda()
+    if not aligned:  # profiles starting 8 bytes past a 16-byte boundary
+        buf = torch.zeros(flat.numel() + 1, dtype=torch.float64, device="cuda")
+        buf[1:] = flat
+        flat = buf[1:]
+    assert (flat.data_ptr() % 16 == 0) == aligned
+    out = torch.zeros((prof.shape[0], 9), dtype=torch.float64, device="cuda")
+    init.predict_device(flat.data_ptr(), prof.shape[0], out.data_ptr(), 0)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    np.testing.assert_array_equal(got, init.predict(prof))
+    err = np.abs(got - want)
+    err[:, 2] = np.minimum(err[:, 2], np.pi - err[:, 2])  # azimuth modulo pi
+    spread = np.quantile(want, 0.95, axis=0) - np.quantile(want, 0.05, axis=0)
+    assert np.all(np.median(err, 0) <= 2e-3 * spread), np.median(err, 0) / spread
+    assert np.all(np.quantile(err, 0.99, axis=0) <= 2e-2 * spread)
+
+
 @pytest.mark.gpu
 def test_attach_detach_leaves_plain_path_unchanged(trained):
     _, init = trained
