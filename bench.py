@@ -208,6 +208,9 @@ def parse():
                     help="pixels of the FP32-vs-FP64 comparison of the plain algorithm (0: off)")
     ap.add_argument("--autotune", type=int, default=1,
                     help="tune each arm's plan on the map before timing (me_plan_autotune)")
+    ap.add_argument("--mlp-compare", type=int, default=1,
+                    help="time the initialiser's map inference with each GEMM kernel "
+                         "(outside the timed region); 2: also retrain with mma.sync")
     return ap.parse_args()
 
 
@@ -319,6 +322,41 @@ def work_histograms(counts):
             "runs": np.bincount(runs, minlength=22)[1:].tolist(),
             "iterations_median_p99": [float(np.median(c[:, 1])), float(np.quantile(c[:, 1], 0.99))],
             "trials_per_pixel": float(c[:, 2].mean())}
+
+
+def initialiser_gemm_compare(torch, init, plan, prof, npix, stream, args, name, rank):
+    """The initialiser's map inference (features, four GEMMs, decode) timed with
+    each GEMM kernel on the resident map (CUDA events, mean of 5 after one
+    warm-up), and with --mlp-compare 2 the training wall time with mma.sync
+    beside the tcgen05 training of the run."""
+    import me_b200
+    out = torch.empty((npix, 9), dtype=torch.float64, device="cuda")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    res = {"map_pixels": npix, "inference_ms": {}}
+    for path in ("tcgen05", "mma_sync"):
+        init.set_gemm(path)
+        init.predict_device(prof.data_ptr(), npix, out.data_ptr(), stream.cuda_stream)
+        e0.record(stream)
+        for _ in range(5):
+            init.predict_device(prof.data_ptr(), npix, out.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res["inference_ms"][path] = e0.elapsed_time(e1) / 5
+    init.set_gemm("tcgen05")
+    if args.mlp_compare > 1:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        other = me_b200.Initializer.train(plan, samples=args.train_samples,
+                                          epochs=args.train_epochs, seed=20240607 + 7919 * rank,
+                                          gemm=me_b200.GEMM_PATHS["mma_sync"],
+                                          **me_maps.train_prior(name))
+        torch.cuda.synchronize()
+        res["train_s_mma_sync"] = time.perf_counter() - t0
+        res["final_loss_mma_sync"] = other.final_loss
+        other.close()
+    res["gemm_launches"] = init.gemm_launches()
+    return res
 
 
 def timed_steps(torch, step, n, stream, dist, clk=None):
@@ -434,6 +472,14 @@ def main():
     prof_stats = step()
     plan.set_profiling(False)
     nvtx.range_pop()
+
+    # ---- the initialiser's inference with each GEMM kernel (outside the timed region)
+    mlp_cmp = None
+    if args.mlp_compare:
+        nvtx.range_push("mlp_compare")
+        mlp_cmp = initialiser_gemm_compare(torch, init, plan, prof, npix, stream, args, name,
+                                           rank)
+        nvtx.range_pop()
 
     # ---- the plain LM with the reference's restarts, same map and GPU
     plain_steps = args.steps if args.plain_steps < 0 else args.plain_steps
@@ -562,6 +608,7 @@ def main():
                        "runs_per_pixel": last["runs"] / max(1, last["valid"]),
                        "ended_after_learned_start": last["learned_done"] / max(1, last["valid"]),
                        "init_ms_per_step": init_ms,
+                       "initialiser_gemm": mlp_cmp,
                        "autotuned": {"learned": tuned, "plain": tuned_plain},
                        "histograms": {"learned": work_histograms(counts_learned),
                                       "plain": work_histograms(counts_plain)},

@@ -214,6 +214,22 @@ void me_plan_set_graphs(me_plan *plan, int on);
  * the Jacobian kernel of the same round (they concern other pixels; default
  * on).  Profiling launches serially. */
 void me_plan_set_overlap(me_plan *plan, int on);
+
+/* With a learned start (an initialiser attached), the queue takes the pixels
+ * in descending order of the misfit of their start -- the chi^2 of the run -1
+ * parameters on about 16 of the grid's wavelengths, in quarter-octave
+ * buckets, ties in pixel order -- so that the pixels likely to need many
+ * iterations and restarts start early instead of running on alone at the end
+ * of the batch.  0 restores pixel order.  Default on.  A pixel's steps are the
+ * same in any order; which kernel runs each of them depends on when it is
+ * queued, so results agree with pixel order to rounding.  The time of the
+ * misfit and the sort is part of the stats' init_ms. */
+void me_plan_set_queue_order(me_plan *plan, int on);
+
+/* The stable counting sort behind the queue order, for testing: order [n]
+ * receives the indices of keys [n] (each < 128) by ascending key, equal keys
+ * in index order; host buffers, run on CUDA device `device`. */
+int me_order_by_key(int device, const unsigned char *keys, long n, long long *order);
 void me_plan_set_svd_lanes(me_plan *plan, int lanes);
 /* Records CUDA events around every inversion launch and reports per-kernel
  * device time in me_stats (off by default; costs a little host time). */

@@ -137,6 +137,10 @@ struct me_plan {
   std::vector<long long> h_list;
   me_mlp *init = nullptr;  // learned initialiser (not owned), or null
   DevBuf d_init;           // [npix][9] its guesses for the current batch
+  // with a learned start, queue the pixels by descending misfit of their
+  // start (me_plan_set_queue_order): keys, histograms and the order
+  bool queue_order = true;
+  DevBuf d_okey, d_ohist, d_order;
 };
 
 extern "C" const char *me_version(void) { return "me_b200 0.1 (sm_100a)"; }
@@ -394,7 +398,7 @@ extern "C" void me_plan_destroy(me_plan *p) {
                     &p->d_list,   &p->d_slot_pix, &p->d_slot_i32, &p->d_slot_cnt,
                     &p->d_slot_u8, &p->d_slot_sc, &p->d_slot_vec, &p->d_slot_hess,
                     &p->d_slot_list, &p->d_slot_small, &p->d_fitpar, &p->d_init,
-                    &p->d_flambda, &p->d_fdlambda};
+                    &p->d_flambda, &p->d_fdlambda, &p->d_okey, &p->d_ohist, &p->d_order};
   for (DevBuf *b : bufs) b->release();
   if (p->h_poll) cudaFreeHost(p->h_poll);
   if (p->ev0) cudaEventDestroy(p->ev0);
@@ -444,6 +448,31 @@ extern "C" int me_plan_last_counters(const me_plan *p, unsigned int *counters, l
 
 extern "C" void me_plan_set_overlap(me_plan *p, int on) {
   if (p) p->overlap = on != 0;
+}
+
+extern "C" void me_plan_set_queue_order(me_plan *p, int on) {
+  if (p) p->queue_order = on != 0;
+}
+
+extern "C" int me_order_by_key(int device, const unsigned char *keys, long n, long long *order) {
+  if (n < 0 || (n > 0 && (!keys || !order))) return fail(ME_ERR_ARG, "null argument");
+  for (long i = 0; i < n; i++)
+    if (keys[i] >= me::kOrderBuckets) return fail(ME_ERR_ARG, "keys must be below 128");
+  if (n == 0) return ME_OK;
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0)
+    return fail(ME_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= nd) return fail(ME_ERR_ARG, "device out of range");
+  CK(cudaSetDevice(device));
+  DevBuf dk, dh, dord;
+  CK(dk.ensure((size_t)n));
+  CK(dh.ensure((size_t)me::kOrderBuckets * me::kOrderBlocks * sizeof(int)));
+  CK(dord.ensure((size_t)n * sizeof(long long)));
+  CK(cudaMemcpy(dk.p, keys, (size_t)n, cudaMemcpyHostToDevice));
+  CK(me::launch_order_by_key(dk.as<unsigned char>(), n, dh.as<int>(), dord.as<long long>(), nullptr));
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(order, dord.p, (size_t)n * sizeof(long long), cudaMemcpyDeviceToHost));
+  return ME_OK;
 }
 
 extern "C" void me_plan_set_graphs(me_plan *p, int on) {
@@ -745,6 +774,21 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     const int grc = me::mlp_gemm_status(p->init);
     if (grc) return grc;
     A.init_par = p->d_init.as<double>();
+    if (p->queue_order) {
+      CK(p->d_okey.ensure(n));
+      CK(p->d_ohist.ensure((size_t)me::kOrderBuckets * me::kOrderBlocks * sizeof(int)));
+      CK(p->d_order.ensure(n * sizeof(long long)));
+      CK(cudaEventRecord(p->ev0, st));
+      CK(me::launch_start_order(p->precision, p->P, d_prof, A.init_par, npix,
+                            p->d_okey.as<unsigned char>(), p->d_ohist.as<int>(),
+                            p->d_order.as<long long>(), st));
+      CK(cudaEventRecord(p->ev1, st));
+      CK(cudaEventSynchronize(p->ev1));
+      float order_ms = 0.f;
+      cudaEventElapsedTime(&order_ms, p->ev0, p->ev1);
+      init_ms += order_ms;
+      A.list = p->d_order.as<long long>();
+    }
   }
 
   long long rounds = 0, rounds_total = 0;

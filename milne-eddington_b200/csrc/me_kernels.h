@@ -151,5 +151,16 @@ cudaError_t launch_svd(const double *d_a, long long nmat, int n, double *d_u, do
                        double *d_v, int *d_hits, cudaStream_t st);
 cudaError_t launch_init_guess(const DevPlan &P, const double *d_prof, long long npix,
                               double *d_guess, double *d_extra, int *d_status, cudaStream_t st);
+// Queue order of a learned start: pixels by descending misfit of their run -1
+// parameters (kOrderBuckets quarter-octave buckets of chi^2, stable), into
+// d_order [npix].  d_key: npix bytes; d_hist: kOrderBuckets * kOrderBlocks ints.
+constexpr int kOrderBuckets = 128;
+constexpr int kOrderBlocks = 1024;
+cudaError_t launch_start_order(int precision, const DevPlan &P, const double *d_prof,
+                               const double *d_init, long long npix, unsigned char *d_key,
+                               int *d_hist, long long *d_order, cudaStream_t st);
+// the stable counting sort alone (keys < kOrderBuckets)
+cudaError_t launch_order_by_key(const unsigned char *d_key, long long n, int *d_hist,
+                                long long *d_order, cudaStream_t st);
 
 }  // namespace me

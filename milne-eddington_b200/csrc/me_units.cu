@@ -134,6 +134,148 @@ __global__ void init_guess_kernel(const DevPlan P, const double *prof, long long
 }
 
 // ---------------------------------------------------------------------------
+// Queue order of a learned start.  A pixel whose start is far from its profile
+// tends to need many LM iterations and restarts; queued late, it runs on alone
+// at the end of the batch while the GPU idles.  The misfit of each pixel's
+// start -- the run -1 parameters exactly as the queue sets them up (Init_Guess,
+// the network's free parameters, the bounds fold) -- is Loss_Function's chi^2
+// (Src/LM_FIT.c:150-156; weights / sqrt(norm0), Src/ME_SOLVER.c:410-441) on
+// every `stride`-th wavelength.  Pixels are queued by descending misfit in
+// quarter-octave buckets, by a stable counting sort, so the order, and with it
+// every result, is reproducible.  A pixel's steps are the same in any order;
+// which kernel runs each of them (full rounds, lane-split rounds, the tail
+// kernel) depends on when it is queued, so results agree with pixel order to
+// rounding.
+// ---------------------------------------------------------------------------
+template <class T, bool FILT>
+__global__ void start_misfit_kernel(const DevPlan P, const double *prof, const double *init_par,
+                                    long long npix, int stride, unsigned char *key) {
+  __shared__ T s_tab[100];
+  __shared__ T s_rden[kRden * 128];
+  VoigtK<T> K;
+  voigt_block_setup<T>(K, P, s_tab);
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= npix) return;
+  const int nl = P.nl;
+  const double *pp = prof + (size_t)i * 4 * nl;
+  PixelInit pin;
+  if (init_guess(pp, P, pin, true) || P.nruns <= 0) {
+    key[i] = (unsigned char)(kOrderBuckets - 1);  // skipped by the queue: last
+    return;
+  }
+  double q[9], step[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const double v = init_par[(size_t)i * 9 + k];
+    q[k] = (P.fixed[k] || !isfinite(v)) ? pin.guess[k] : v;
+    step[k] = P.step[k];
+  }
+  bounds_fold(q, P, pin.l70, pin.l71);
+  step[7] = pin.step7;
+  const double isn = 1.0 / sqrt(pin.norm0);
+  SynthCall<T> c;
+  synth_setup<T>(c, q, P, step);
+  voigt_prepare<T>(K, c.p5, s_rden + threadIdx.x, blockDim.x);
+  const T ones[4] = {T(1), T(1), T(1), T(1)};
+  double chi = 0.0;
+  int used = 0;
+  for (int iw = 0; iw < nl; iw += stride, used++) {
+    T syn[4];
+    channel_point<T, false, FILT>(c, P, K, ones, iw, syn, nullptr);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const double rd = ((double)syn[s] - pp[s * nl + iw]) * P.weights[s] * isn;
+      chi += rd * rd;
+    }
+  }
+  chi /= 4.0 * used;
+  // bucket 0: chi^2 >= 2^32 or not finite; a quarter octave per bucket below,
+  // down to bucket kOrderBuckets - 2 (chi^2 < 2^0.5 and all below)
+  int b = 0;
+  if (chi < 4294967296.0) {
+    b = (int)floor((32.0 - log2(fmax(chi, 1e-300))) * 4.0);
+    b = b < 0 ? 0 : (b > kOrderBuckets - 2 ? kOrderBuckets - 2 : b);
+  }
+  key[i] = (unsigned char)b;
+}
+
+// Stable counting sort of pixel indices by an 8-bit key, in three launches:
+// per-block histograms of contiguous chunks (bucket-major), an exclusive scan
+// of them, and a scatter in which each block walks its chunk in index order.
+__global__ void order_hist_kernel(const unsigned char *key, long long n, long long chunk,
+                                  int *hist) {
+  __shared__ int h[kOrderBuckets];
+  for (int t = threadIdx.x; t < kOrderBuckets; t += blockDim.x) h[t] = 0;
+  __syncthreads();
+  const long long lo = blockIdx.x * chunk;
+  const long long hi = lo + chunk < n ? lo + chunk : n;
+  for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&h[key[i]], 1);
+  __syncthreads();
+  for (int t = threadIdx.x; t < kOrderBuckets; t += blockDim.x)
+    hist[(size_t)t * gridDim.x + blockIdx.x] = h[t];
+}
+
+// exclusive prefix sums of hist[0..m) in place; one block of 1024 threads
+__global__ void __launch_bounds__(1024) order_scan_kernel(int *hist, int m) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x;
+  const int per = (m + 1023) / 1024;
+  const int lo = t * per, hi = lo + per < m ? lo + per : m;
+  int sum = 0;
+  for (int i = lo; i < hi; i++) sum += hist[i];
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan of the segment sums
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (int i = lo; i < hi; i++) {
+    const int v = hist[i];
+    hist[i] = run;
+    run += v;
+  }
+}
+
+__global__ void __launch_bounds__(256) order_scatter_kernel(const unsigned char *key, long long n,
+                                                            long long chunk, const int *offs,
+                                                            long long *order) {
+  __shared__ int base[kOrderBuckets];
+  __shared__ int wcnt[8][kOrderBuckets];
+  for (int t = threadIdx.x; t < kOrderBuckets; t += blockDim.x) {
+    base[t] = offs[(size_t)t * gridDim.x + blockIdx.x];
+    for (int w = 0; w < 8; w++) wcnt[w][t] = 0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long lo = blockIdx.x * chunk;
+  const long long hi = lo + chunk < n ? lo + chunk : n;
+  for (long long r0 = lo; r0 < hi; r0 += 256) {
+    const long long i = r0 + threadIdx.x;
+    const bool in = i < hi;
+    const int k = in ? (int)key[i] : kOrderBuckets + lane;  // absent lanes match nobody
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    const bool leader = lane == __ffs(peers) - 1;
+    if (in && leader) wcnt[warp][k] = __popc(peers);
+    __syncthreads();
+    if (in) {
+      int pos = base[k] + rank;
+      for (int w = 0; w < warp; w++) pos += wcnt[w][k];
+      order[pos] = i;
+    }
+    __syncthreads();
+    if (in && leader) {
+      atomicAdd(&base[k], __popc(peers));
+      wcnt[warp][k] = 0;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 
@@ -224,6 +366,39 @@ cudaError_t launch_svd(const double *d_a, long long nmat, int n, double *d_u, do
   if (g == 0) return cudaSuccess;
   svd_kernel<<<g, b, 0, st>>>(d_a, nmat, n, d_u, d_w, d_v, d_hits);
   return cudaGetLastError();
+}
+
+cudaError_t launch_order_by_key(const unsigned char *d_key, long long n, int *d_hist,
+                                long long *d_order, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const long long chunk = n / kOrderBlocks + 1 > 1024 ? n / kOrderBlocks + 1 : 1024;
+  const int nb = (int)((n + chunk - 1) / chunk);
+  order_hist_kernel<<<nb, 256, 0, st>>>(d_key, n, chunk, d_hist);
+  order_scan_kernel<<<1, 1024, 0, st>>>(d_hist, kOrderBuckets * nb);
+  order_scatter_kernel<<<nb, 256, 0, st>>>(d_key, n, chunk, d_hist, d_order);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_start_order(int precision, const DevPlan &P, const double *d_prof,
+                               const double *d_init, long long npix, unsigned char *d_key,
+                               int *d_hist, long long *d_order, cudaStream_t st) {
+  if (npix <= 0) return cudaSuccess;
+  const int b = 128;
+  const unsigned g = (unsigned)((npix + b - 1) / b);
+  // about 16 wavelengths of the grid
+  const int stride = P.nl / 16 > 1 ? P.nl / 16 : 1;
+  if (precision == 1) {
+    if (P.nsub > 1)
+      start_misfit_kernel<double, true><<<g, b, 0, st>>>(P, d_prof, d_init, npix, stride, d_key);
+    else
+      start_misfit_kernel<double, false><<<g, b, 0, st>>>(P, d_prof, d_init, npix, stride, d_key);
+  } else {
+    if (P.nsub > 1)
+      start_misfit_kernel<float, true><<<g, b, 0, st>>>(P, d_prof, d_init, npix, stride, d_key);
+    else
+      start_misfit_kernel<float, false><<<g, b, 0, st>>>(P, d_prof, d_init, npix, stride, d_key);
+  }
+  return launch_order_by_key(d_key, npix, d_hist, d_order, st);
 }
 
 cudaError_t launch_init_guess(const DevPlan &P, const double *d_prof, long long npix,

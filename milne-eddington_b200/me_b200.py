@@ -150,7 +150,8 @@ EXPORTED = [
     "me_mlp_shape", "me_mlp_get_params", "me_mlp_set_params", "me_mlp_loss_grad",
     "me_fits_image_info", "me_fits_read", "me_fits_create", "me_fits_write",
     "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
-    "me_mlp_set_gemm", "me_mlp_gemm_launches", "me_gemm_bf16",
+    "me_mlp_set_gemm", "me_mlp_gemm_launches", "me_gemm_bf16", "me_plan_set_queue_order",
+    "me_order_by_key",
 ]
 
 
@@ -258,6 +259,10 @@ def lib() -> ctypes.CDLL:
                                             ctypes.c_long]
         L.me_plan_set_overlap.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_overlap.restype = None
+        L.me_plan_set_queue_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_queue_order.restype = None
+        L.me_order_by_key.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_ubyte), ctypes.c_long,
+                                      ctypes.POINTER(ctypes.c_longlong)]
         L.me_plan_set_graphs.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_graphs.restype = None
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
@@ -480,6 +485,11 @@ class Plan:
     def set_overlap(self, on: bool = True):
         """Later-trial SVDs on a second stream beside the Jacobian kernel (default on)."""
         lib().me_plan_set_overlap(self._h, int(bool(on)))
+
+    def set_queue_order(self, on: bool = True):
+        """With a learned start, queue pixels by descending misfit of their start
+        (default on); off: pixel order."""
+        lib().me_plan_set_queue_order(self._h, int(bool(on)))
 
     def set_graphs(self, on: bool = True):
         """Rounds between queue checks as one CUDA graph launch (default on)."""
@@ -717,6 +727,17 @@ class Initializer:
 
 
 GEMM_PATHS = {"tcgen05": 0, "mma_sync": 1}
+
+
+def order_by_key(keys: np.ndarray, device: int = 0) -> np.ndarray:
+    """The queue order's stable counting sort on the GPU: indices of keys
+    (uint8, each < 128) by ascending key, equal keys in index order."""
+    keys = np.ascontiguousarray(keys, dtype=np.uint8)
+    out = np.zeros(keys.size, dtype=np.int64)
+    _check(lib().me_order_by_key(device, keys.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                 keys.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))),
+           "me_order_by_key")
+    return out
 
 
 def gemm_bf16(a: np.ndarray, bt: np.ndarray, path: str = "tcgen05", split: int = 1,
