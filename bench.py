@@ -607,6 +607,13 @@ def main():
                        "chi2_ratio_q01_q50_q99": out["ratio_q"],
                        "runs_per_pixel": last["runs"] / max(1, last["valid"]),
                        "ended_after_learned_start": last["learned_done"] / max(1, last["valid"]),
+                       "fallback_rate": 1.0 - last["learned_done"] / max(1, last["valid"]),
+                       "profile_stream": {
+                           "bytes_per_pixel": 4 * nl * 8 + 10 * 8,
+                           "gb_per_s": npix * (4 * nl * 8 + 10 * 8) / step_s / 1e9,
+                           "note": "profiles read once and results written once per step "
+                                   "(HBM), far below the measured HBM bandwidth: the path is "
+                                   "compute bound"},
                        "init_ms_per_step": init_ms,
                        "initialiser_gemm": mlp_cmp,
                        "autotuned": {"learned": tuned, "plain": tuned_plain},
