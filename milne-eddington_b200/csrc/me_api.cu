@@ -1150,8 +1150,12 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
   const int w0 = p->window > 0 ? p->window : 131072;
   std::vector<Knob> knobs = {
       {&p->window, {w0 / 2, w0, w0 * 2}},
-      {&p->max_group, {1, 8, 32}},
-      {&p->tail_slots, {0, -1, p->grid_fin * (me::kBlock / 32) * 2}},
+      {&p->max_group, {1, 4, 8, 16, 32}},
+      // the tail kernel's threshold: none, a quarter, half (the default), one
+      // and two waves of its warps
+      {&p->tail_slots,
+       {0, p->grid_fin * (me::kBlock / 32) / 4, -1, p->grid_fin * (me::kBlock / 32),
+        p->grid_fin * (me::kBlock / 32) * 2}},
       {&p->svd_lanes, {1, 2}},
   };
   for (Knob &k : knobs) {
