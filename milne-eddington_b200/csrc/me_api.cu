@@ -1148,6 +1148,7 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
     std::vector<int> cand;
   };
   const int w0 = p->window > 0 ? p->window : 131072;
+  p->window = w0;  // the default made explicit, so the result names it
   std::vector<Knob> knobs = {
       {&p->window, {w0 / 2, w0, w0 * 2}},
       {&p->max_group, {1, 4, 8, 16, 32}},

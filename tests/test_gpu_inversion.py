@@ -205,7 +205,7 @@ def test_autotune_picks_a_setting_and_keeps_results_valid():
         r = plan.autotune(d_prof.data_ptr(), prof.shape[0])
         assert plan.carry_chisq == 0.25
         assert r["trials"] >= 4 and r["ms"] > 0
-        assert r["window"] in (65536, 131072, 262144) and r["max_group"] in (1, 8, 32)
+        assert r["window"] in (65536, 131072, 262144) and r["max_group"] in (1, 4, 8, 16, 32)
         assert r["svd_lanes"] in (1, 2)
         assert (plan.window, plan.max_group, plan.tail_slots, plan.svd_lanes) == \
             (r["window"], r["max_group"], r["tail_slots"], r["svd_lanes"])
