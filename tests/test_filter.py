@@ -144,6 +144,37 @@ def test_filtered_inversion_parity_vs_oracle(filt_map, prec):
 
 
 @pytest.mark.gpu
+def test_learned_start_with_queue_order_on_the_filtered_grid():
+    """The learned start on the filtered grid, queue order on and off (the
+    start-misfit kernel's filtered variant): the same pixels inverted, chi^2
+    that agree under the ulp-chaos bar, and a reproducible order."""
+    lam = me_maps.wavelengths(NAME)
+    par = me_maps.draw_parameters(NAME, 8192, 29)
+    with me_b200.Plan(cfg_of("FP32"), lam) as plan:
+        prof = me_maps.add_noise(plan.synthesize(par), 2e-3, 29)
+        init = me_b200.Initializer.train(plan, samples=1 << 18, epochs=4,
+                                         doppler_range=(20.0, 50.0), noise=2e-3)
+        plan.set_initializer(init)
+        plan.window = 2048
+        plan.set_queue_order(False)
+        plan.carry_chisq = 0.0
+        r0, s0 = plan.invert(prof)
+        plan.set_queue_order(True)
+        plan.carry_chisq = 0.0
+        r1, s1 = plan.invert(prof)
+        plan.carry_chisq = 0.0
+        r2, _ = plan.invert(prof)
+        plan.set_initializer(None)
+        init.close()
+    np.testing.assert_array_equal(r1, r2)
+    assert s1["valid"] == s0["valid"] and s1["init_ms"] > 0
+    valid = r0[:, 9] > 0
+    ratio = r1[valid, 9] / r0[valid, 9]
+    print(f"filtered learned start, queue order: chi2 within 1.05x {np.mean(ratio <= 1.05):.4f}")
+    assert np.mean(ratio <= 1.05) > 0.97 and abs(np.median(ratio) - 1) < 1e-6
+
+
+@pytest.mark.gpu
 def test_initialiser_trained_on_the_filtered_grid():
     """The configs' filtergram run retrains the learned initialiser for its
     grid: training profiles go through the same filter."""
