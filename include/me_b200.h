@@ -380,13 +380,19 @@ typedef struct me_mlp_train_params {
   double noise;                 /* Gaussian noise sigma                    */
   int gemm;                     /* GEMM kernel, ME_GEMM_TCGEN05 (default)  */
                                 /* or ME_GEMM_MMA_SYNC (defined below)     */
+  /* an optional second population: with probability mix_weight a sample
+   * draws B and eta0 from these ranges instead of b_range / eta_range
+   * (0, the default: one population) */
+  double mix_weight;
+  double mix_b_range[2];
+  double mix_eta_range[2];
 } me_mlp_train_params;
 
 /* The defaults: the parameter distributions of the Fe I 15648.5 A maps
  * (B ~ U(0, 3000) G, cos theta ~ U(-1, 1), phi ~ U(0, pi), v ~ N(0, 1.5) km/s,
  * Doppler width ~ U(150, 350) mA, a ~ U(0.1, 0.8), eta0 ~ U(2, 30), S0 = 1,
- * beta ~ U(0.1, 0.6), noise 1e-3); 2^22 samples, 16 epochs, batch 4096,
- * lr 1e-3. */
+ * beta ~ U(0.1, 0.6), noise 1e-3, one population); 2^22 samples, 16 epochs,
+ * batch 4096, lr 1e-3, tcgen05 GEMMs. */
 int me_mlp_train_params_default(me_mlp_train_params *tp);
 
 /* Trains a new initialiser for the plan's line and grid on the plan's device.

@@ -465,6 +465,8 @@ void transpose(const bf16 *in, int rows, int cols, bf16 *out, cudaStream_t st) {
 struct Prior {  // the training distribution
   float b_lo, b_hi, cost_lo, cost_hi, phi_lo, phi_hi, v_sigma, w_lo, w_hi, a_lo, a_hi, eta_lo,
       eta_hi, s, beta_lo, beta_hi, noise;
+  // second population (B and eta0 ranges) drawn with probability mix
+  float mix, mb_lo, mb_hi, meta_lo, meta_hi;
 };
 
 __device__ __forceinline__ void draws16(unsigned long long seed, long long i, float u[16]) {
@@ -496,7 +498,8 @@ __global__ void synth_train_kernel(const __grid_constant__ DevPlan P, Prior pr,
   float u[16];
   draws16(seed, i, u);
   double par[9];
-  par[0] = pr.b_lo + (pr.b_hi - pr.b_lo) * u[0];
+  const bool second = u[9] < pr.mix;  // u[9]: the population
+  par[0] = second ? pr.mb_lo + (pr.mb_hi - pr.mb_lo) * u[0] : pr.b_lo + (pr.b_hi - pr.b_lo) * u[0];
   const double cost = pr.cost_lo + (pr.cost_hi - pr.cost_lo) * u[1];
   par[1] = acos(cost);
   par[2] = pr.phi_lo + (pr.phi_hi - pr.phi_lo) * u[2];
@@ -504,7 +507,8 @@ __global__ void synth_train_kernel(const __grid_constant__ DevPlan P, Prior pr,
   par[3] = pr.v_sigma * sqrt(-2.0 * log((double)u[3])) * cos(6.283185307179586 * u[4]);
   par[4] = pr.w_lo + (pr.w_hi - pr.w_lo) * u[5];
   par[5] = pr.a_lo + (pr.a_hi - pr.a_lo) * u[6];
-  par[6] = pr.eta_lo + (pr.eta_hi - pr.eta_lo) * u[7];
+  par[6] = second ? pr.meta_lo + (pr.meta_hi - pr.meta_lo) * u[7]
+                  : pr.eta_lo + (pr.eta_hi - pr.eta_lo) * u[7];
   par[7] = pr.s;
   par[8] = pr.beta_lo + (pr.beta_hi - pr.beta_lo) * u[8];
   SynthCall<float> c;
@@ -1086,6 +1090,11 @@ void prior_from(const me_mlp_train_params *tp, Prior &pr) {
   pr.beta_lo = (float)tp->beta_range[0];
   pr.beta_hi = (float)tp->beta_range[1];
   pr.noise = (float)tp->noise;
+  pr.mix = (float)tp->mix_weight;
+  pr.mb_lo = (float)tp->mix_b_range[0];
+  pr.mb_hi = (float)tp->mix_b_range[1];
+  pr.meta_lo = (float)tp->mix_eta_range[0];
+  pr.meta_hi = (float)tp->mix_eta_range[1];
 }
 
 }  // namespace
@@ -1144,6 +1153,8 @@ extern "C" int me_mlp_train(me_plan *plan, const me_mlp_train_params *tp, me_mlp
                 "batch a multiple of 256, batch <= samples <= 2^31, epochs >= 0, lr > 0");
   if (tp->gemm != ME_GEMM_TCGEN05 && tp->gemm != ME_GEMM_MMA_SYNC)
     return fail(ME_ERR_ARG, "gemm must be ME_GEMM_TCGEN05 or ME_GEMM_MMA_SYNC");
+  if (!(tp->mix_weight >= 0.0 && tp->mix_weight <= 1.0))
+    return fail(ME_ERR_ARG, "mix_weight must lie in [0, 1]");
   me::DevPlan P;
   int device = 0;
   int rc = me::plan_devplan(plan, &P, &device);

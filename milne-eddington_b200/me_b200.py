@@ -203,6 +203,9 @@ class MeMlpTrainParams(ctypes.Structure):
         ("beta_range", ctypes.c_double * 2),
         ("noise", ctypes.c_double),
         ("gemm", ctypes.c_int),
+        ("mix_weight", ctypes.c_double),
+        ("mix_b_range", ctypes.c_double * 2),
+        ("mix_eta_range", ctypes.c_double * 2),
     ]
 
 

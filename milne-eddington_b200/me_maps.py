@@ -137,8 +137,10 @@ def train_prior(name: str) -> dict:
     if w["kind"] == "fe6173":
         return {"doppler_range": (20.0, 50.0), "noise": w["noise"]}
     if w["kind"] == "fe6302":
-        return {"b_range": (0.0, 3500.0), "doppler_range": (60.0, 140.0), "eta_range": (1.0, 30.0),
-                "noise": w["noise"]}
+        # the map's two populations: 40 % strong-field, 60 % weak-field
+        return {"b_range": (500.0, 3500.0), "eta_range": (2.0, 30.0),
+                "mix_weight": 0.6, "mix_b_range": (0.0, 200.0), "mix_eta_range": (1.0, 10.0),
+                "doppler_range": (60.0, 140.0), "noise": w["noise"]}
     return {}
 
 
