@@ -603,6 +603,12 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
   // 1..5 lane groups of 2..32; they hold this queue's arguments, so they live
   // for this call only
   cudaGraphExec_t graphs[6] = {};
+  // a group size's first rounds in this queue run as direct launches, so
+  // that every kernel a graph holds has run (and been loaded) before its
+  // capture; a capture that fails all the same falls back to direct launches
+  // for the rest of the queue
+  bool ran_direct[6] = {};
+  bool graphs_ok = true;
   auto group_index = [](int g) {
     int i = 0;
     while (g > 1) {
@@ -633,9 +639,12 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     // starts every batch at parity 0), or direct launches when profiling
     me::Overlap ov_storage{p->stream2, p->ev_fork, p->ev_join};
     const me::Overlap *ov = (p->overlap && !p->profile) ? &ov_storage : nullptr;
-    cudaGraphExec_t *gx = (p->use_graphs && !p->profile && p->poll_rounds % 2 == 0)
-                              ? &graphs[group_index(group)]
-                              : nullptr;
+    const int gi = group_index(group);
+    cudaGraphExec_t *gx =
+        (graphs_ok && ran_direct[gi] && p->use_graphs && !p->profile && p->poll_rounds % 2 == 0)
+            ? &graphs[gi]
+            : nullptr;
+    ran_direct[gi] = true;
     if (gx && !*gx) {
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
@@ -650,8 +659,11 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
       if (e == cudaSuccess) e = cudaGraphInstantiate(gx, g, 0);
       if (g) cudaGraphDestroy(g);
       if (e != cudaSuccess) {
+        // nothing captured ran; clear the capture's error and launch directly
+        cudaGetLastError();
         release_graphs();
-        return fail(ME_ERR_CUDA, std::string("round graph: ") + cudaGetErrorString(e));
+        graphs_ok = false;
+        gx = nullptr;
       }
     }
     if (gx) {
