@@ -1073,8 +1073,13 @@ int round_grid_impl(int which, int device) {
   return sms * per_sm;
 }
 
-inline void launch_svd_lanes(int lanes, const DevPlan &P, const InvertArgs &A, const Slots &S,
-                             int parity, int which, int grid, cudaStream_t st) {
+// static: svd_kernel has internal linkage, so each translation unit must launch
+// its own copy (the one whose shared-memory limit round_grid_impl raised); an
+// inline function with external linkage would be merged across the units by
+// the linker and launch one unit's kernel for every precision
+static inline void launch_svd_lanes(int lanes, const DevPlan &P, const InvertArgs &A,
+                                    const Slots &S, int parity, int which, int grid,
+                                    cudaStream_t st) {
   switch (lanes) {
     case 2: svd_grp_kernel<2><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
     case 4: svd_grp_kernel<4><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
