@@ -311,8 +311,17 @@ cudaError_t launch_round_grp(int precision, int G, const DevPlan &P, const Inver
 }
 
 // grids of the unfiltered kernels (the filtered ones run grid-stride loops
-// over the same grids)
+// over the same grids).  Each precision and filter unit has its own SVD
+// kernel, whose dynamic shared memory exceeds the default limit; the sizing of
+// the SVD grid raises that limit, so it is done in the filtered unit of the
+// precision too (a plan may take a filter after it is made).
 int round_grid(int precision, int which, int device) {
+  if (which == 2) {
+    if (precision == 1)
+      round_grid_f64f(2, device);
+    else
+      round_grid_f32f(2, device);
+  }
   return precision == 1 ? round_grid_f64(which, device) : round_grid_f32(which, device);
 }
 
