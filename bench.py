@@ -7,7 +7,8 @@ code reaches on the same profile -- with the learned initialiser, beside the
 plain LM with the reference's random restarts on the same map and GPU.  The
 converged share is measured on a seeded sample of the map against the
 reference core (oracle/_ref, the reference's own C sources compiled here; the
-oracle restatement where it was not built).
+oracle restatement where it was not built, and for the instrument filter the
+reference does not have).
 
 Workload (default): the 1024x1024 Fe I 15648.5 A map (nl = 60, seeded draws of
 B, theta, phi, v, Doppler width, damping, eta0, beta; S = 1; noise 1e-3),
@@ -15,7 +16,19 @@ num_run = 5, chisq_criteria = 1.5, FP32 synthesis with FP64 SVD solve and
 chi^2 test, with Bounds_Dopp = 100, 400 mA and Bounds_Damp = 0.05, 1.0: the
 default Doppler bounds (10-80 mA) cannot reach the drawn widths (150-350 mA),
 so with them no start can fit and chisq_criteria is met by a sixth of the
-pixels at best (`--bounds literal` runs that variant).
+pixels at best (`--bounds literal` runs that variant; the default line also
+reports it under `other_workloads`).
+
+The sample pixels (4096 by default) are the same in both arms: seeded indices
+into the map, the map's own parameter draws, synthesised on the host by the
+reference's own Milne_Eddington_Single and given seeded host noise.  The GPU
+arm writes them into its map before anything runs, inverts them with the map,
+and compares them with the reference core; the reference arm (`--impl
+reference`) times the reference core on exactly those pixels.
+
+The parity block puts every GPU arm beside the reference on the sample, next
+to the reference's own spread on the same pixels (another restart seed, and a
+one-ulp change of the input), with per-parameter tolerances.
 
 The initialiser is trained once per line and grid before the timed region
 (4M profiles synthesised on the GPU from seeded draws of the same
@@ -53,43 +66,68 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "milne-eddington_b200")
 sys.path.insert(0, PKG)
 
-import me_maps  # noqa: E402
-import me_ranks  # noqa: E402
+import me_maps  # noqa: E402  (pure Python: workload definitions)
+import me_ranks  # noqa: E402  (pure Python: rank plumbing)
 
 METRIC = "converged pixels/s on 1 B200 at chi2<=1.05x FP64 ref: learned-init vs plain LM"
 UNIT = "pixels/s"
+REF_SEED = 4242      # restart stream of the reference run that defines "converged"
+REF_SEED_B = 99991   # a second restart stream: the reference's seed-to-seed spread
+
+# Per-parameter tolerance on |GPU - reference| (units of param_errors):
+# G, deg, deg, m/s, mA, -, -, continuum, -.
+TOLERANCE = {"B_G": 1.0, "theta_deg": 0.1, "phi_deg": 0.1, "v_m_s": 1.0, "doppler_mA": 0.1,
+             "damping": 1e-3, "eta0": 0.1, "S": 1e-3, "beta": 1e-3}
 
 
 # ---------------------------------------------------------------------------
-# CPU side: the reference's own C core (or the oracle port) on host cores.
+# CPU side: the reference's own C core (or the oracle port) on host cores,
+# in spawned worker processes (one set-up per process, reseeded per run).
 # ---------------------------------------------------------------------------
 _W = {}
 
 
-def _cpu_worker_init(kind, workload, npix_max, seed, widen):
+def _cpu_worker_init(kind, workload, npix_max, widen):
     sys.path[:0] = [os.path.join(ROOT, "tests"), PKG]
     import oracle_bind as ob
-    import me_b200
     lam = me_maps.wavelengths(workload)
     _W["kind"] = kind
     if kind == "reference":
+        # the reference's own parser (RDINPUT) and INIT_INV; nothing of this
+        # library is loaded in this process
         _W["eng"] = ob.Reference(me_maps.reference_control_text(workload, widen_bounds=widen),
-                                 lam, npix_max, seed=seed)
+                                 lam, npix_max, seed=REF_SEED)
     else:
+        import me_b200
         cfg = me_b200.parse_config_text(me_maps.control_text(workload, precision="FP64",
                                                              widen_bounds=widen))
         _W["eng"] = ob.Oracle(cfg, lam)
 
 
-def _cpu_worker_invert(prof):
+def _ulp_perturb(prof):
+    rng = np.random.default_rng(5)
+    return prof * (1 + 2.3e-16 * rng.choice([-1, 1], prof.shape))
+
+
+def _cpu_worker_invert(job):
+    prof, seed, perturb = job
     eng = _W["eng"]
+    if perturb:
+        prof = _ulp_perturb(prof)
     if _W["kind"] == "reference":
+        eng.reseed(seed)
         return eng.invert(prof)
     import oracle_bind as ob
-    return eng.invert(prof, rng_mode=ob.MEO_RNG_NR, nr_seed=1)
+    eng.carry[0] = 0.0
+    return eng.invert(prof, rng_mode=ob.MEO_RNG_NR, nr_seed=seed)
 
 
-def cpu_kind(workload="fe15648_1024x1024"):
+def _cpu_worker_synth(par):
+    eng = _W["eng"]
+    return np.stack([eng.synth(p) for p in np.atleast_2d(par)])
+
+
+def cpu_kind(workload):
     """The reference's own core where it was built here and the workload is
     within its reach; the oracle port (the same algorithm restated, with the
     instrument-filter extension) otherwise."""
@@ -99,21 +137,33 @@ def cpu_kind(workload="fe15648_1024x1024"):
         else "port"
 
 
-def cpu_invert(prof, workload, procs, widen):
-    """Inverts prof [n][4][nl] with `procs` processes of the reference core;
-    returns (results, seconds, kind)."""
-    kind = cpu_kind(workload)
-    n = prof.shape[0]
-    procs = max(1, min(procs, n))
-    chunks = np.array_split(np.arange(n), procs)
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(procs, initializer=_cpu_worker_init,
-                  initargs=(kind, workload, max(len(c) for c in chunks), 4242, widen)) as pool:
-        pool.map(_cpu_worker_invert, [prof[c[:1]] for c in chunks])  # warm every worker
+class CpuPool:
+    """`procs` spawned processes of the reference core (or the port) for one
+    workload: host-side synthesis of sample pixels and timed inversions."""
+
+    def __init__(self, workload, procs, npix_max, widen):
+        self.kind = cpu_kind(workload)
+        self.procs = max(1, procs)
+        ctx = mp.get_context("spawn")
+        self.pool = ctx.Pool(self.procs, initializer=_cpu_worker_init,
+                             initargs=(self.kind, workload, max(1, npix_max), widen))
+
+    def synth(self, par):
+        chunks = np.array_split(np.arange(par.shape[0]), self.procs)
+        return np.concatenate(self.pool.map(_cpu_worker_synth, [par[c] for c in chunks if len(c)]))
+
+    def invert(self, prof, seed=REF_SEED, perturb=False):
+        """(results, seconds): prof split in `procs` contiguous slices, each
+        process one slice from a fresh restart stream (as independent
+        reference processes would)."""
+        chunks = [c for c in np.array_split(np.arange(prof.shape[0]), self.procs) if len(c)]
         t0 = time.perf_counter()
-        parts = pool.map(_cpu_worker_invert, [prof[c] for c in chunks])
-        dt = time.perf_counter() - t0
-    return np.concatenate(parts), dt, kind
+        parts = self.pool.map(_cpu_worker_invert, [(prof[c], seed, perturb) for c in chunks])
+        return np.concatenate(parts), time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
 
 
 def host_cores():
@@ -123,16 +173,17 @@ def host_cores():
         return os.cpu_count() or 1
 
 
-def cpu_sample_profiles(workload, npix, seed):
-    """Seeded profiles synthesised on the CPU by the oracle (FP64)."""
-    sys.path[:0] = [os.path.join(ROOT, "tests")]
-    import me_b200
-    import oracle_bind as ob
-    lam = me_maps.wavelengths(workload)
-    cfg = me_b200.parse_config_text(me_maps.control_text(workload, precision="FP64"))
-    o = ob.Oracle(cfg, lam)
-    par = me_maps.draw_parameters(workload, npix, seed)
-    return me_maps.add_noise(o.synth_many(par), me_maps.WORKLOADS[workload]["noise"], seed)
+def sample_size(args, cores):
+    return max(args.sample, cores * 32)
+
+
+def sample_profiles(pool, workload, npix, nsample, map_seed):
+    """The map's sample pixels: seeded indices, the map's own parameter draws,
+    synthesised on the host by the CPU pool's core, plus seeded host noise."""
+    idx = me_maps.sample_indices(npix, nsample)
+    par = me_maps.draw_parameters(workload, npix, map_seed)[idx]
+    prof = pool.synth(par) + me_maps.sample_noise(workload, idx.size, map_seed)
+    return idx, prof
 
 
 # ---------------------------------------------------------------------------
@@ -199,7 +250,7 @@ def parse():
     ap.add_argument("--npix", type=int, default=0, help="override the map size (testing)")
     ap.add_argument("--precision", default="FP32", choices=["FP32", "FP64"])
     ap.add_argument("--sample", type=int, default=4096,
-                    help="pixels of the CPU sample (reference timing + converged share)")
+                    help="pixels of the sample (converged share, parity, reference arm)")
     ap.add_argument("--train-samples", type=int, default=4 << 20)
     ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--plain-steps", type=int, default=-1, help="timed plain-LM steps (-1: K)")
@@ -211,53 +262,78 @@ def parse():
     ap.add_argument("--mlp-compare", type=int, default=1,
                     help="time the initialiser's map inference with each GEMM kernel "
                          "(outside the timed region); 2: also retrain with mma.sync")
+    ap.add_argument("--parity", type=int, default=1,
+                    help="reference self-spread and per-parameter parity block on the sample")
+    ap.add_argument("--other-workloads", default="fe6302_2048x1024,fe6173_4096x4096,literal",
+                    help="comma list of further workloads measured after the headline "
+                         "(N = 1 only; 'literal' = the headline map with the literal bounds); "
+                         "empty: none")
+    ap.add_argument("--other-budget-s", type=float, default=480.0,
+                    help="wall-time budget of the further workloads; one that would start "
+                         "past it is skipped")
     return ap.parse_args()
 
 
-def use_widened(args):
+def use_widened(args, workload=None):
     if args.bounds == "auto":
-        return me_maps.WORKLOADS[args.workload]["kind"] == "fe15648"
+        return me_maps.WORKLOADS[workload or args.workload]["kind"] == "fe15648"
     return args.bounds == "widened"
 
 
+def arm_config(workload, widen, npix, nsample, precision=None):
+    """The configuration both arms report: the workload and its sample."""
+    w = me_maps.WORKLOADS[workload]
+    return {"workload": workload, "map_pixels": npix, "nl": w["nl"],
+            "num_run": int(w["ctl"].get("num_run", 4)),
+            "chisq_criteria": float(w["ctl"].get("chisq_criteria", 1.0)),
+            "bounds": "widened" if widen else "workload's own",
+            "sample": f"{nsample} seeded pixels of the map (same in both arms)"}
+
+
 def reference_arm(args):
-    """The reference's own CPU implementation on this host's cores."""
+    """The reference's own CPU implementation on this host's cores, on the
+    GPU arm's sample pixels: the reference's parser, synthesis and
+    INVERSION_MULTI (oracle/_ref), nothing of this library."""
     rank, _, _ = me_ranks.rank_env()
     if rank != 0:
         return 0
-    w = me_maps.WORKLOADS[args.workload]
+    name = args.workload
     widen = use_widened(args)
     cores = host_cores()
-    # ~7 ms of one core per pixel at num_run = 5: a step of ~2 s on all cores
-    npix = args.npix or max(cores * 48, 256)
-    prof = cpu_sample_profiles(args.workload, npix, seed=99)
-    times = []
-    kind = None
-    for i in range(args.warmup + args.steps):
-        _, dt, kind = cpu_invert(prof, args.workload, cores, widen)
-        if i >= args.warmup:
-            times.append(dt)
-    step = max(times)
-    value = npix / step
+    npix = args.npix or me_maps.WORKLOADS[name]["npix"]
+    nb = min(npix, sample_size(args, cores))
+    pool = CpuPool(name, cores, (nb + cores - 1) // cores, widen)
+    try:
+        _, prof = sample_profiles(pool, name, npix, nb, me_ranks.map_seed(0))
+        pool.invert(prof[:cores])  # every worker set up
+        times = []
+        for i in range(args.warmup + args.steps):
+            _, dt = pool.invert(prof)
+            if i >= args.warmup:
+                times.append(dt)
+    finally:
+        pool.close()
+    step = statistics.median(times)
+    value = nb / step
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded draws of the workload's parameter distributions)",
-            "config": {"workload": args.workload,
-                       "bounds": "widened" if widen else "workload's own",
-                       "pixels_per_step": npix,
-                       "num_run": int(w["ctl"].get("num_run", 4)), "nl": w["nl"],
-                       "init": "Init_Guess + random restarts (the reference's algorithm)",
-                       "cpu_processes": cores},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": f"{npix} pixels of {args.workload} per step, "
-                                       f"{cores} processes of the reference core"},
+            "config": arm_config(name, widen, npix, nb),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": pool.kind,
+                             "sample": f"{nb} seeded pixels of {name} (the GPU arm's sample) "
+                                       f"per step, {cores} processes of the reference core, "
+                                       f"median step"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "init": "Init_Guess + random restarts (the reference's algorithm)"}
     print(json.dumps(line), flush=True)
     return 0
 
 
+# ---------------------------------------------------------------------------
+# rooflines, errors, parity
+# ---------------------------------------------------------------------------
 def _flops(c):
     return c.get("add", 0) + c.get("mul", 0) + c.get("div", 0) + c.get("sqrt", 0)
 
@@ -279,10 +355,11 @@ def event_flops(fc, nl, jacobians, trials):
                                     + _flops(fc["loss_per_lambda"]))}
 
 
-def kernel_rooflines(st, fc, nl, peak):
+def kernel_rooflines(st, fc, nl, peak, peak64):
     """Per-kernel algorithmic FLOP/s from a profiled batch (me_plan_set_profiling):
     the round kernels over the events the rounds did, the tail kernel over
-    the rest."""
+    the rest.  frac: of the FP32 peak; the SVD solve (FP64 arithmetic) also
+    against the FP64 peak."""
     tj, tt = st["tail_jacobians"], st["tail_trials"]
     rounds = event_flops(fc, nl, st["jacobians"] - tj, st["trials"] - tt)
     tail = event_flops(fc, nl, tj, tt)
@@ -294,19 +371,85 @@ def kernel_rooflines(st, fc, nl, peak):
         if ms > 0:
             tf = fl / (ms / 1e3) / 1e12
             out[name] = {"ms": ms, "algorithmic_flop": fl, "tflops": tf, "frac": tf / peak}
+            if name == "svd_kernel" and peak64:
+                out[name]["frac_of_fp64_peak"] = tf / peak64
     return out
 
 
-def param_errors(res, ref):
-    """Median and 99th percentile |res - ref| per parameter in G, deg, deg,
-    m/s, mA, -, -, -, - (S, beta in continuum units)."""
-    names = ["B_G", "theta_deg", "phi_deg", "v_m_s", "doppler_mA", "damping", "eta0", "S",
-             "beta"]
-    scale = [1.0, 180 / np.pi, 180 / np.pi, 1e3, 1.0, 1.0, 1.0, 1.0, 1.0]
+PARAMS = ["B_G", "theta_deg", "phi_deg", "v_m_s", "doppler_mA", "damping", "eta0", "S", "beta"]
+
+
+def abs_errors(res, ref):
+    """|res - ref| per pixel and parameter in G, deg, deg, m/s, mA, -, -, -, -
+    (the azimuth difference folded into [0, 90] deg)."""
+    scale = np.array([1.0, 180 / np.pi, 180 / np.pi, 1e3, 1.0, 1.0, 1.0, 1.0, 1.0])
     d = np.abs(res[:, :9] - ref[:, :9])
-    d[:, 2] = np.minimum(d[:, 2], np.pi - d[:, 2])  # azimuth is folded into [0, pi)
-    return {n: [float(np.median(d[:, k]) * sc), float(np.quantile(d[:, k], 0.99) * sc)]
-            for k, (n, sc) in enumerate(zip(names, scale))}
+    d[:, 2] = np.minimum(d[:, 2], np.pi - d[:, 2])
+    return d * scale
+
+
+def param_errors(res, ref):
+    """Median and 99th percentile |res - ref| per parameter."""
+    d = abs_errors(res, ref)
+    return {n: [float(np.median(d[:, k])), float(np.quantile(d[:, k], 0.99))]
+            for k, n in enumerate(PARAMS)}
+
+
+def chi2_agreement(res, ref):
+    """Share of the reference's inverted pixels with chi^2 <= 1.05 x the
+    reference's, the chi^2 ratio quantiles, and the share identical in all
+    ten outputs (1e-6 relative)."""
+    v = ref[:, 9] > 0
+    if not v.any():
+        return {"within_1.05": 0.0, "ratio_q01_q50_q99": None, "identical": 0.0}
+    ratio = res[v, 9] / ref[v, 9]
+    same = np.all(np.abs(res - ref) <= 1e-6 * np.abs(ref) + 1e-12, axis=1)[v]
+    return {"within_1.05": float(np.mean(ratio <= 1.05)),
+            "ratio_q01_q50_q99": [float(np.quantile(ratio, q)) for q in (0.01, 0.5, 0.99)],
+            "identical": float(same.mean())}
+
+
+def parity_vs_reference(res, ref, spread):
+    """A GPU arm against the reference on the sample: per parameter median /
+    p99 |delta| and pass/fail.  A parameter passes when its median is within
+    the stated tolerance or within 1.1 x the reference's own spread, and its
+    p99 within 1.1 x that spread (or the tolerance): the spread is the larger
+    of the reference against itself with another restart seed and with a
+    one-ulp input change, on the same pixels.  The chi^2 test passes when the
+    share within 1.05 x is no more than 0.02 below the reference's own."""
+    v = ref[:, 9] > 0
+    err = param_errors(res[v], ref[v])
+    params = {}
+    for n in PARAMS:
+        med, p99 = err[n]
+        smed = max(spread[k]["err"][n][0] for k in spread)
+        sp99 = max(spread[k]["err"][n][1] for k in spread)
+        tol = TOLERANCE[n]
+        params[n] = {"median_p99": [med, p99], "tolerance": tol,
+                     "ref_spread_median_p99": [smed, sp99],
+                     "pass": bool(med <= max(tol, 1.1 * smed) and p99 <= max(tol, 1.1 * sp99)),
+                     "within_tolerance_median": bool(med <= tol)}
+    chi = chi2_agreement(res, ref)
+    s_within = min(spread[k]["chi2"]["within_1.05"] for k in spread)
+    chi["ref_spread_within_1.05"] = s_within
+    chi["pass"] = bool(chi["within_1.05"] >= s_within - 0.02)
+    return {"params": params, "chi2": chi,
+            "all_pass": bool(chi["pass"] and all(p["pass"] for p in params.values()))}
+
+
+def truth_recovery(res, ref, truth):
+    """The learned start against the truth, beside the reference against the
+    truth on the same pixels: a parameter passes when neither its median nor
+    its p99 error exceeds the reference's (or the tolerance)."""
+    v = ref[:, 9] > 0
+    a = param_errors(res[v], truth[v])
+    b = param_errors(ref[v], truth[v])
+    out = {}
+    for n in PARAMS:
+        tol = TOLERANCE[n]
+        out[n] = {"gpu_vs_truth_median_p99": a[n], "ref_vs_truth_median_p99": b[n],
+                  "pass": bool(a[n][0] <= max(tol, b[n][0]) and a[n][1] <= max(tol, b[n][1]))}
+    return out
 
 
 def work_histograms(counts):
@@ -315,6 +458,8 @@ def work_histograms(counts):
     if counts is None:
         return None
     c = counts[counts[:, 0] > 0]
+    if c.shape[0] == 0:
+        return None
     it = np.minimum(c[:, 1], 30)
     runs = np.minimum(c[:, 0], 21)
     return {"pixels": int(c.shape[0]),
@@ -389,6 +534,120 @@ class _Null:
         return False
 
 
+def gpu_map(torch, me_b200, name, npix, seed, device):
+    """A seeded map resident in HBM: the workload's parameter draws, the GPU's
+    FP64 synthesis, Gaussian noise.  Returns (true parameters, profiles)."""
+    w = me_maps.WORKLOADS[name]
+    lam = me_maps.wavelengths(name)
+    gen = me_b200.Plan(me_b200.parse_config_text(me_maps.control_text(name, precision="FP64")),
+                       lam, device=device)
+    par_true = me_maps.draw_parameters(name, npix, seed)
+    d_par = torch.from_numpy(par_true).cuda()
+    prof = torch.empty((npix, 4, lam.size), dtype=torch.float64, device="cuda")
+    gen.synthesize_device(d_par.data_ptr(), npix, prof.data_ptr())
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    prof += w["noise"] * torch.randn(prof.shape, dtype=torch.float64, device="cuda", generator=g)
+    torch.cuda.synchronize()
+    gen.close()
+    del d_par
+    return par_true, prof
+
+
+# ---------------------------------------------------------------------------
+# further workloads (N = 1): the other configurations, measured after the
+# headline with the same method, fewer steps
+# ---------------------------------------------------------------------------
+def other_workload(torch, me_b200, args, key, stream, cores, init_headline):
+    """One further workload: learned start (1 warm-up + 2 timed steps) and
+    plain LM (1 timed step after a warm-up on a part of the map), the
+    converged share of each against the reference core (the port with the
+    filter) on a seeded sample, iteration histograms, fallback rate."""
+    if key == "literal":
+        name, widen, label = args.workload, False, f"{args.workload}_literal_bounds"
+    else:
+        name, widen, label = key, use_widened(args, key), key
+    w = me_maps.WORKLOADS[name]
+    lam = me_maps.wavelengths(name)
+    npix = w["npix"]
+    seed = me_ranks.map_seed(0)
+    t_start = time.perf_counter()
+    nb = min(npix, max(1024, cores * 32))
+    pool = CpuPool(name, cores, (nb + cores - 1) // cores, widen)
+    try:
+        idx, sprof = sample_profiles(pool, name, npix, nb, seed)
+        par_true, prof = gpu_map(torch, me_b200, name, npix, seed, torch.cuda.current_device())
+        prof[torch.from_numpy(idx).cuda()] = torch.from_numpy(sprof).cuda()
+        res = torch.zeros((npix, 10), dtype=torch.float64, device="cuda")
+        ctl = me_maps.control_text(name, precision=args.precision, seed=seed, widen_bounds=widen)
+        out = {"workload": name, "bounds": "widened" if widen else "workload's own",
+               "map_pixels": npix, "nl": w["nl"], "num_run": int(w["ctl"].get("num_run", 4)),
+               "chisq_criteria": float(w["ctl"].get("chisq_criteria", 1.0))}
+        with me_b200.Plan(me_b200.parse_config_text(ctl), lam) as plan:
+            if key == "literal":
+                init = init_headline  # same line, grid and prior as the headline
+                out["train_s"] = 0.0
+            else:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                init = me_b200.Initializer.train(plan, samples=args.train_samples,
+                                                 epochs=args.train_epochs, seed=20240607,
+                                                 **me_maps.train_prior(name))
+                torch.cuda.synchronize()
+                out["train_s"] = time.perf_counter() - t0
+            plan.set_initializer(init)
+
+            def step():
+                return plan.invert_device(prof.data_ptr(), npix, res.data_ptr(), 0,
+                                          stream.cuda_stream)
+
+            step()
+            el, st = timed_steps(torch, step, 2, stream, None)
+            learned_s = el / 2
+            counts = plan.last_counters(npix)
+            res_l = res.cpu().numpy()
+            plan.set_initializer(None)
+            if key != "literal":
+                init.close()
+            # plain LM: warm-up on the first eighth of the map, one timed step
+            part = max(1, npix // 8)
+            plan.invert_device(prof.data_ptr(), part, res.data_ptr(), 0, stream.cuda_stream)
+            el_p, st_p = timed_steps(torch, step, 1, stream, None)
+            plain_s = el_p
+            counts_p = plan.last_counters(npix)
+            res_p = res.cpu().numpy()
+        del prof, res
+        torch.cuda.empty_cache()
+        ref_res, ref_dt = pool.invert(sprof)
+    finally:
+        pool.close()
+    learned = chi2_agreement(res_l[idx], ref_res)
+    plain = chi2_agreement(res_p[idx], ref_res)
+    raw_l, raw_p = npix / learned_s, npix / plain_s
+    last = st[-1]
+    out.update({
+        "converged_pixels_per_s": raw_l * learned["within_1.05"],
+        "plain_converged_pixels_per_s": raw_p * plain["within_1.05"],
+        "learned_vs_plain": (raw_l * learned["within_1.05"]) / max(1e-9, raw_p * plain["within_1.05"]),
+        "raw_pixels_per_s": raw_l, "plain_raw_pixels_per_s": raw_p,
+        "ms_per_step": learned_s * 1e3, "plain_ms_per_step": plain_s * 1e3,
+        "steps": 2, "plain_steps": 1,
+        "converged_fraction": learned["within_1.05"], "plain_converged_fraction": plain["within_1.05"],
+        "chi2_ratio_q01_q50_q99": learned["ratio_q01_q50_q99"],
+        "plain_chi2_ratio_q01_q50_q99": plain["ratio_q01_q50_q99"],
+        "fallback_rate": 1.0 - last["learned_done"] / max(1, last["valid"]),
+        "runs_per_pixel": last["runs"] / max(1, last["valid"]),
+        "plain_runs_per_pixel": st_p[-1]["runs"] / max(1, st_p[-1]["valid"]),
+        "histograms": {"learned": work_histograms(counts), "plain": work_histograms(counts_p)},
+        "converged_sample": f"{nb} seeded pixels vs the {pool.kind} FP64 chi^2",
+        "cpu_pixels_per_s": nb / ref_dt,
+        "param_err_vs_truth_median_p99": param_errors(res_l, par_true),
+        "ref_param_err_vs_truth_median_p99": param_errors(ref_res[ref_res[:, 9] > 0],
+                                                          par_true[idx][ref_res[:, 9] > 0]),
+        "profile_stream_gb_per_s": npix * (4 * w["nl"] * 8 + 80) / learned_s / 1e9,
+        "wall_s": time.perf_counter() - t_start})
+    return label, out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -408,18 +667,21 @@ def main():
     lam = me_maps.wavelengths(name)
     nl = lam.size
     seed = me_ranks.map_seed(rank)
+    cores = host_cores()
+    nb = min(npix, sample_size(args, cores))
+
+    # ---- the sample pixels, built on the host (rank 0; same as the reference arm's)
+    pool = None
+    idx = sprof = None
+    if rank == 0:
+        pool = CpuPool(name, cores, (nb + cores - 1) // cores, widen)
+        idx, sprof = sample_profiles(pool, name, npix, nb, seed)
 
     # ---- synthetic map resident in HBM: seeded draws -> GPU FP64 synthesis + noise
-    gen = me_b200.Plan(me_b200.parse_config_text(me_maps.control_text(name, precision="FP64")),
-                       lam, device=local)
-    par_true = me_maps.draw_parameters(name, npix, seed)
-    d_par = torch.from_numpy(par_true).cuda()
-    prof = torch.empty((npix, 4, nl), dtype=torch.float64, device="cuda")
-    gen.synthesize_device(d_par.data_ptr(), npix, prof.data_ptr())
-    g = torch.Generator(device="cuda").manual_seed(seed)
-    prof += w["noise"] * torch.randn(prof.shape, dtype=torch.float64, device="cuda", generator=g)
-    torch.cuda.synchronize()
-    gen.close()
+    par_true, prof = gpu_map(torch, me_b200, name, npix, seed, local)
+    if rank == 0:
+        prof[torch.from_numpy(idx).cuda()] = torch.from_numpy(sprof).cuda()
+        torch.cuda.synchronize()
     res = torch.zeros((npix, 10), dtype=torch.float64, device="cuda")
     res_plain = torch.zeros((npix, 10), dtype=torch.float64, device="cuda")
 
@@ -501,14 +763,14 @@ def main():
     if args.fp64_sample > 0 and args.precision == "FP32":
         ns = min(npix, args.fp64_sample)
         sel = torch.from_numpy(np.sort(np.random.default_rng(11).choice(npix, ns, replace=False)))
-        sprof = prof[sel.cuda()].contiguous()
+        sprof32 = prof[sel.cuda()].contiguous()
         out32 = torch.zeros((ns, 10), dtype=torch.float64, device="cuda")
         out64 = torch.zeros((ns, 10), dtype=torch.float64, device="cuda")
         ctl64 = me_maps.control_text(name, precision="FP64", seed=seed, widen_bounds=widen)
         with me_b200.Plan(me_b200.parse_config_text(ctl), lam, device=local) as p32, \
                 me_b200.Plan(me_b200.parse_config_text(ctl64), lam, device=local) as p64:
-            p32.invert_device(sprof.data_ptr(), ns, out32.data_ptr(), 0, stream.cuda_stream)
-            p64.invert_device(sprof.data_ptr(), ns, out64.data_ptr(), 0, stream.cuda_stream)
+            p32.invert_device(sprof32.data_ptr(), ns, out32.data_ptr(), 0, stream.cuda_stream)
+            p64.invert_device(sprof32.data_ptr(), ns, out64.data_ptr(), 0, stream.cuda_stream)
         torch.cuda.synchronize()
         a, b = out32.cpu().numpy(), out64.cpu().numpy()
         v = b[:, 9] > 0
@@ -516,6 +778,17 @@ def main():
         fp_cmp = {"pixels": int(ns), "param_err_median_p99": param_errors(a[v], b[v]),
                   "chi2_ratio_q01_q50_q99": [float(np.quantile(ratio, q)) for q in (0.01, 0.5, 0.99)],
                   "chi2_within_1.05": float(np.mean(ratio <= 1.05))}
+
+    # ---- the plain algorithm in FP64 on the GPU, on the sample alone (parity)
+    res_fp64_sample = None
+    if rank == 0 and args.parity:
+        ctl64 = me_maps.control_text(name, precision="FP64", seed=seed, widen_bounds=widen)
+        d_s = torch.from_numpy(sprof).cuda()
+        o64 = torch.zeros((nb, 10), dtype=torch.float64, device="cuda")
+        with me_b200.Plan(me_b200.parse_config_text(ctl64), lam, device=local) as p64:
+            p64.invert_device(d_s.data_ptr(), nb, o64.data_ptr(), 0, stream.cuda_stream)
+        torch.cuda.synchronize()
+        res_fp64_sample = o64.cpu().numpy()
 
     # ---- end to end through the host entry point (pinned host buffers)
     e2e = None
@@ -530,102 +803,159 @@ def main():
             _, st_e2e = plan.invert(h_prof_np)
         e2e_s = me_ranks.max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, dist, "cuda")
         e2e = {"seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"], "d2h_ms": st_e2e["d2h_ms"]}
+        del h_prof, h_prof_np
 
     res_np = res.cpu().numpy()
     res_plain_np = res_plain.cpu().numpy()
     out = {}
     if rank == 0:
-        # ---- CPU leg: the reference core on a seeded sample of this map, timed on
-        # the host cores (cpu_baseline); its chi^2 decides which of the GPU's
-        # pixels count as converged (chi^2 <= 1.05 x the reference's)
-        cores = host_cores()
-        nb = min(npix, max(args.sample, cores * 32))
-        rng = np.random.default_rng(7)
-        idx = np.sort(rng.choice(npix, size=nb, replace=False))
-        sample_prof = prof[idx].cpu().numpy()
-        ref_res, base_dt, base_kind = cpu_invert(sample_prof, name, cores, widen)
+        # ---- CPU leg: the reference core on the sample, timed on the host
+        # cores (cpu_baseline); its chi^2 decides which of the GPU's pixels
+        # count as converged (chi^2 <= 1.05 x the reference's)
+        pool.invert(sprof[:cores])  # every worker set up
+        ref_res, base_dt = pool.invert(sprof, REF_SEED)
+        spread = {}
+        if args.parity:
+            ref_b, _ = pool.invert(sprof, REF_SEED_B)
+            ref_u, _ = pool.invert(sprof, REF_SEED, perturb=True)
+            v = ref_res[:, 9] > 0
+            spread = {"other_restart_seed": {"err": param_errors(ref_b[v], ref_res[v]),
+                                             "chi2": chi2_agreement(ref_b, ref_res)},
+                      "one_ulp_input": {"err": param_errors(ref_u[v], ref_res[v]),
+                                        "chi2": chi2_agreement(ref_u, ref_res)}}
         valid = ref_res[:, 9] > 0
-
-        def conv(r):
-            ratio = r[idx, 9][valid] / ref_res[valid, 9]
-            return (float(np.mean(ratio <= 1.05)) if valid.any() else 0.0,
-                    [float(np.quantile(ratio, q)) for q in (0.01, 0.5, 0.99)])
-
-        frac, ratio_q = conv(res_np)
-        frac_plain, ratio_q_plain = conv(res_plain_np) if plain_s else (None, None)
+        learned_s = res_np[idx]
+        conv = chi2_agreement(learned_s, ref_res)
+        conv_plain = chi2_agreement(res_plain_np[idx], ref_res) if plain_s else None
+        parity = None
+        if args.parity:
+            arms = {"plain_fp32": res_plain_np[idx] if plain_s else None,
+                    "plain_fp64": res_fp64_sample}
+            parity = {"tolerance": TOLERANCE,
+                      "rule": "median <= max(tol, 1.1 x ref spread median) and p99 <= max(tol, "
+                              "1.1 x ref spread p99); chi2 within 1.05 share >= ref spread "
+                              "share - 0.02; ref spread = the reference against itself with "
+                              "another restart seed and with a one-ulp input change, same "
+                              "pixels",
+                      "ref_self_spread": spread,
+                      "arms": {k: parity_vs_reference(r, ref_res, spread)
+                               for k, r in arms.items() if r is not None}}
+            # the learned start is judged by chi^2 and truth recovery: it
+            # finds lower minima than the reference's restarts on most pixels
+            miss = valid & (learned_s[:, 9] > 1.05 * ref_res[:, 9])
+            b_miss = valid & (ref_b[:, 9] > 1.05 * ref_res[:, 9])
+            parity["arms"]["learned"] = {
+                "chi2": conv,
+                "misses": int(miss.sum()),
+                "misses_where_ref_other_seed_also_misses": int((miss & b_miss).sum()),
+                "misses_within_1.05_of_ref_other_seed": int(
+                    (miss & (learned_s[:, 9] <= 1.05 * ref_b[:, 9])).sum()),
+                "truth_recovery": truth_recovery(learned_s, ref_res, par_true[idx]),
+                "err_vs_ref_median_p99": param_errors(learned_s[valid], ref_res[valid])}
+            parity["arms"]["learned"]["all_pass"] = bool(
+                conv["within_1.05"] >= spread["other_restart_seed"]["chi2"]["within_1.05"] - 0.02
+                and all(p["pass"] for p in parity["arms"]["learned"]["truth_recovery"].values()))
+            parity["all_pass"] = bool(all(a["all_pass"] for a in parity["arms"].values()))
         fc = json.load(open(os.path.join(ROOT, "tests", "golden", "flop_counts.json")))[name]
         peak = fp32_peak_tflops(torch)
-        kr = kernel_rooflines(prof_stats, fc, nl, peak)
+        peak64 = fp64_peak_tflops(torch)
+        kr = kernel_rooflines(prof_stats, fc, nl, peak, peak64)
         top = max(kr, key=lambda k: kr[k]["ms"])
         alg_step = sum(event_flops(fc, nl, last["jacobians"], last["trials"]).values())
-        out = {"frac": frac, "ratio_q": ratio_q, "frac_plain": frac_plain,
-               "ratio_q_plain": ratio_q_plain, "cpu_value": nb / base_dt, "nb": nb,
-               "base_kind": base_kind, "cores": cores, "kernels": kr, "top": top,
+        out = {"conv": conv, "conv_plain": conv_plain, "parity": parity,
+               "cpu_value": nb / base_dt, "base_kind": pool.kind, "kernels": kr, "top": top,
                "alg_step": alg_step, "step_tflops": alg_step / (kernel_ms / 1e3) / 1e12,
-               "clk": clk.summary(), "peak": peak,
-               "err_vs_ref": param_errors(res_np[idx][valid], ref_res[valid]),
+               "clk": clk.summary(), "peak": peak, "peak64": peak64,
+               "err_vs_ref": param_errors(learned_s[valid], ref_res[valid]),
                "err_vs_truth": param_errors(res_np, par_true),
                "err_vs_truth_ref": param_errors(ref_res[valid], par_true[idx][valid])}
+        pool.close()
+
+    # ---- the other configurations (one GPU only; after the headline)
+    others = {}
+    if rank == 0 and world == 1 and args.other_workloads:
+        t_other = time.perf_counter()
+        del res, res_plain
+        torch.cuda.empty_cache()
+        for key in [k.strip() for k in args.other_workloads.split(",") if k.strip()]:
+            if time.perf_counter() - t_other > args.other_budget_s:
+                others[key] = {"skipped": f"wall-time budget of {args.other_budget_s} s spent"}
+                continue
+            try:
+                label, o = other_workload(torch, me_b200, args, key, stream, cores, init)
+                others[label] = o
+            except Exception as exc:  # report, do not lose the headline line
+                others[key] = {"error": f"{type(exc).__name__}: {exc}"}
 
     if dist:
         dist.barrier()
     if rank == 0:
         pix_per_s = npix * world / step_s
-        value = pix_per_s * out["frac"]
+        frac = out["conv"]["within_1.05"]
+        value = pix_per_s * frac
         plain_cfg = None
+        plain_conv = None
         if plain_s:
             plain_raw = npix * world / plain_s
-            plain_cfg = {"converged_pixels_per_s": plain_raw * out["frac_plain"],
+            plain_conv = plain_raw * out["conv_plain"]["within_1.05"]
+            plain_cfg = {"converged_pixels_per_s": plain_conv,
                          "raw_pixels_per_s": plain_raw, "ms_per_step": plain_s * 1e3,
-                         "converged_fraction": out["frac_plain"],
-                         "chi2_ratio_q01_q50_q99": out["ratio_q_plain"],
+                         "converged_fraction": out["conv_plain"]["within_1.05"],
+                         "chi2_ratio_q01_q50_q99": out["conv_plain"]["ratio_q01_q50_q99"],
                          "runs_per_pixel": plain_last["runs"] / max(1, plain_last["valid"]),
                          "steps": plain_steps, "warmup": 1}
+        learned_vs_plain = value / plain_conv if plain_conv else None
+        parity = out["parity"]
+        config = arm_config(name, widen, npix, nb)
+        config.update({
+            "converged_fraction": frac,
+            "raw_pixels_per_s": pix_per_s,
+            "plain_converged_pixels_per_s": plain_conv,
+            "learned_vs_plain": learned_vs_plain,
+            "parity_all_pass": parity["all_pass"] if parity else None,
+            "ref_seed_to_seed_within_1.05": (parity["ref_self_spread"]["other_restart_seed"]
+                                             ["chi2"]["within_1.05"] if parity else None),
+            "precision": args.precision,
+            "parallelism": f"pixel shards x{world}",
+            "l2": "inputs larger than L2 (2 GB of profiles per GPU)",
+            "fallback_rate": 1.0 - last["learned_done"] / max(1, last["valid"]),
+            "runs_per_pixel": last["runs"] / max(1, last["valid"]),
+            "init_ms_per_step": init_ms,
+            "init": "learned (MLP 240-256-256-256-10 GELU), then the reference's "
+                    "restarts for pixels above chisq_criteria",
+            "train": {"samples": args.train_samples, "epochs": args.train_epochs,
+                      "batch": 4096, "lr": 1e-3, "seconds": train_s,
+                      "final_loss": init.final_loss},
+            "converged_sample": f"{nb} seeded pixels vs the {out['base_kind']} FP64 chi^2",
+            "chi2_ratio_q01_q50_q99": out["conv"]["ratio_q01_q50_q99"],
+            "ended_after_learned_start": last["learned_done"] / max(1, last["valid"]),
+            "profile_stream": {
+                "bytes_per_pixel": 4 * nl * 8 + 10 * 8,
+                "gb_per_s": npix * (4 * nl * 8 + 10 * 8) / step_s / 1e9,
+                "note": "profiles read once and results written once per step "
+                        "(HBM), far below the measured HBM bandwidth: the path is "
+                        "compute bound"},
+            "initialiser_gemm": mlp_cmp,
+            "autotuned": {"learned": tuned, "plain": tuned_plain},
+            "histograms": {"learned": work_histograms(counts_learned),
+                           "plain": work_histograms(counts_plain)},
+            "fp32_vs_fp64_plain": fp_cmp,
+            "plain_lm": plain_cfg,
+            "param_err_vs_fp64_ref_median_p99": out["err_vs_ref"],
+            "param_err_vs_truth_median_p99": out["err_vs_truth"],
+            "ref_param_err_vs_truth_median_p99": out["err_vs_truth_ref"]})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64 (MLP bf16)" if args.precision == "FP32" else "f64 (MLP bf16)",
             "data": "synthetic (seeded draws of the workload's parameter distributions, "
-                    "GPU FP64 synthesis + Gaussian noise)",
-            "config": {"workload": name, "bounds": "widened" if widen else "workload's own",
-                       "pixels_per_gpu": npix,
-                       "nl": nl, "num_run": int(w["ctl"].get("num_run", 4)),
-                       "chisq_criteria": float(w["ctl"].get("chisq_criteria", 1.0)),
-                       "precision": args.precision,
-                       "init": "learned (MLP 240-256-256-256-10 GELU), then the reference's "
-                               "restarts for pixels above chisq_criteria",
-                       "train": {"samples": args.train_samples, "epochs": args.train_epochs,
-                                 "batch": 4096, "lr": 1e-3, "seconds": train_s,
-                                 "final_loss": init.final_loss},
-                       "parallelism": f"pixel shards x{world}",
-                       "l2": "inputs larger than L2 (2 GB of profiles per GPU)",
-                       "raw_pixels_per_s": pix_per_s,
-                       "converged_fraction": out["frac"],
-                       "converged_sample": f"{out['nb']} seeded pixels vs the "
-                                           f"{out['base_kind']} FP64 chi^2",
-                       "chi2_ratio_q01_q50_q99": out["ratio_q"],
-                       "runs_per_pixel": last["runs"] / max(1, last["valid"]),
-                       "ended_after_learned_start": last["learned_done"] / max(1, last["valid"]),
-                       "fallback_rate": 1.0 - last["learned_done"] / max(1, last["valid"]),
-                       "profile_stream": {
-                           "bytes_per_pixel": 4 * nl * 8 + 10 * 8,
-                           "gb_per_s": npix * (4 * nl * 8 + 10 * 8) / step_s / 1e9,
-                           "note": "profiles read once and results written once per step "
-                                   "(HBM), far below the measured HBM bandwidth: the path is "
-                                   "compute bound"},
-                       "init_ms_per_step": init_ms,
-                       "initialiser_gemm": mlp_cmp,
-                       "autotuned": {"learned": tuned, "plain": tuned_plain},
-                       "histograms": {"learned": work_histograms(counts_learned),
-                                      "plain": work_histograms(counts_plain)},
-                       "fp32_vs_fp64_plain": fp_cmp,
-                       "plain_lm": plain_cfg,
-                       "learned_vs_plain": (value / plain_cfg["converged_pixels_per_s"]
-                                            if plain_cfg else None),
-                       "param_err_vs_fp64_ref_median_p99": out["err_vs_ref"],
-                       "param_err_vs_truth_median_p99": out["err_vs_truth"],
-                       "ref_param_err_vs_truth_median_p99": out["err_vs_truth_ref"]},
+                    "GPU FP64 synthesis + Gaussian noise; the sample pixels synthesised by "
+                    "the reference core on the host)",
+            "config": config,
+            "plain_converged_pixels_per_s": plain_conv,
+            "learned_vs_plain": learned_vs_plain,
+            "parity_all_pass": parity["all_pass"] if parity else None,
             "gpu_launches": int(sum(s["launches"] for s in stats)),
             "e2e": None, "clocks": out["clk"],
             "roofline": {"bound": "fp32", "kernel": out["top"],
@@ -638,20 +968,24 @@ def main():
                                  "reference algorithm for the events it ran (counted with a "
                                  "counting scalar type) / its time; peak = FP32 FFMA rate "
                                  "measured in this run with cuBLAS SGEMM, TF32 off "
-                                 "(MEASURED_PEAKS.json has no FP32 figure)",
+                                 "(MEASURED_PEAKS.json has no FP32 figure); the SVD solve is "
+                                 "also given against the FP64 DGEMM rate measured in this run",
+                         "fp64_peak": out["peak64"],
                          "kernels": out["kernels"],
                          "step_algorithmic_tflops": out["step_tflops"],
                          "algorithmic_flop_per_step": out["alg_step"]},
-            "cpu_baseline": {"value": out["cpu_value"], "unit": UNIT, "cores": out["cores"],
+            "cpu_baseline": {"value": out["cpu_value"], "unit": UNIT, "cores": cores,
                              "kind": out["base_kind"],
-                             "sample": f"{out['nb']} seeded pixels of the map, "
-                                       f"{out['cores']} processes of the reference core"},
+                             "sample": f"{nb} seeded pixels of the map, "
+                                       f"{cores} processes of the reference core"},
+            "parity": parity,
+            "other_workloads": others or None,
             "stats": {k: last[k] for k in ("valid", "runs", "iterations", "trials", "accepted",
                                            "jacobians", "redo_pixels", "launches",
                                            "learned_done")},
         }
         if e2e:
-            line["e2e"] = {"value": npix * world / e2e["seconds"] * out["frac"], "unit": UNIT,
+            line["e2e"] = {"value": npix * world / e2e["seconds"] * frac, "unit": UNIT,
                            "h2d_bytes_per_step": npix * 4 * nl * 8,
                            "d2h_bytes_per_step": npix * 10 * 8,
                            "h2d_ms": e2e["h2d_ms"], "d2h_ms": e2e["d2h_ms"]}
@@ -670,23 +1004,33 @@ def fp32_peak_tflops(torch):
     old = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
     try:
-        n = 8192
-        a = torch.randn(n, n, device="cuda")
-        b = torch.randn(n, n, device="cuda")
-        for _ in range(2):
-            torch.mm(a, b)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        best = 0.0
-        for _ in range(3):
-            e0.record()
-            torch.mm(a, b)
-            e1.record()
-            torch.cuda.synchronize()
-            best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12)
-        return best
+        return _gemm_peak(torch, torch.float32)
     finally:
         torch.backends.cuda.matmul.allow_tf32 = old
+
+
+def fp64_peak_tflops(torch):
+    """FP64 throughput of this GPU: cuBLAS DGEMM."""
+    return _gemm_peak(torch, torch.float64)
+
+
+def _gemm_peak(torch, dtype):
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=dtype)
+    b = torch.randn(n, n, device="cuda", dtype=dtype)
+    for _ in range(2):
+        torch.mm(a, b)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(3):
+        e0.record()
+        torch.mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12)
+    del a, b
+    return best
 
 
 if __name__ == "__main__":

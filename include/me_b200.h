@@ -205,6 +205,12 @@ void me_plan_set_max_group(me_plan *plan, int lanes);
  * or 8); more lanes cut the decomposition's latency, fewer keep more of them
  * in flight.  Default 1. */
 int me_plan_svd_lanes(const me_plan *plan);
+/* With all nine parameters free, the one-thread-per-pixel SVD solves keep
+ * their 9x9 matrix in registers (default, 1) or in shared memory (0).  Same
+ * operations in the same order; the register form has no shared-memory
+ * round trips and interleaves the independent row and column updates. */
+int me_plan_svd_registers(const me_plan *plan);
+void me_plan_set_svd_registers(me_plan *plan, int on);
 /* The LM rounds between two checks of the queue go to the GPU as one CUDA
  * graph, captured once per batch for each lane-group size (default on; off:
  * one launch per kernel).  Profiling (me_plan_set_profiling) launches
@@ -302,23 +308,27 @@ int me_svd_device(const double *d_a, long nmat, int n, double *d_u, double *d_w,
 int me_synthesize_jacobian_device(me_plan *plan, const double *d_par, long npix, double step7,
                                   double *d_prof, double *d_jac, void *stream);
 
-/* me_invert_batch_device without any device allocation, for callers that
- * cannot allocate while they invert: code running while a CUDA graph is being
- * captured, pipelines that give their whole GPU memory to their own pool up
- * front, real-time loops that must not block in the allocator.  No reference
- * counterpart: it replaces the same INVERSION_MULTI (Src/LM_FIT.c:746-811) as
- * me_invert_batch_device, with the control file and the wavelength grid
- * (host arrays) instead of a plan.
+/* me_invert_batch_device without any device allocation.  No counterpart in
+ * the reference: an addition of this library, for callers that cannot
+ * allocate device memory while they invert -- data-reduction pipelines and
+ * frameworks that reserve the GPU's memory for their own pool when they start
+ * (an allocation of ours would fail or take memory their pool counts on), and
+ * real-time loops at the instrument, where cudaMalloc / cudaFree can
+ * synchronise the device and stall the loop.  It takes the control file and
+ * the wavelength grid (host arrays) instead of a plan and runs the same round
+ * kernels as me_invert_batch_device.
  *
  * All of its scratch lives in one static device array of fixed size (about
  * 12.4 MB, held on every GPU the library is loaded on until the process
  * exits): at most ME_NOALLOC_MAX_PIXELS pixels per call, ME_NOALLOC_SLOTS of
  * them in flight; a larger npix is rejected with ME_ERR_ARG -- invert large
  * maps in chunks, passing *carry_chisq (the LM chi^2 carried from pixel to
- * pixel, 0 at the start of a map) from one call to the next.  d_prof
+ * pixel, 0 at the start of a map) from one call to the next.  Control files
+ * with an instrument filter are rejected (ME_ERR_CONFIG).  d_prof
  * [npix][4][nl] and d_res [npix][10] are device buffers of the caller; the
  * work is ordered on `stream` (a cudaStream_t, NULL = legacy default stream)
- * and complete when the call returns.
+ * and complete when the call returns.  Rounds beyond the LM step bound end
+ * the call with ME_ERR_TIMEOUT.
  *
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) and the kernels' occupancy with that device current;

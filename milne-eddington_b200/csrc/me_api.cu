@@ -196,6 +196,7 @@ int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P
     P.regul_weight[i] = cfg->regul_weight[i];
   }
   if (P.npar == 0) return fail(ME_ERR_CONFIG, "all nine parameters are fixed");
+  P.svd_regs = 1;
   P.ncut = nl / 5;
   const double c = 299792458.0;
   double t = (lambda[P.ncut] - lam0) * c / 1e3;  // the reference omits /lambda0 here
@@ -480,6 +481,10 @@ extern "C" void me_plan_set_graphs(me_plan *p, int on) {
 }
 
 extern "C" int me_plan_svd_lanes(const me_plan *p) { return p ? p->svd_lanes : 0; }
+extern "C" int me_plan_svd_registers(const me_plan *p) { return p ? p->P.svd_regs : 0; }
+extern "C" void me_plan_set_svd_registers(me_plan *p, int on) {
+  if (p) p->P.svd_regs = on ? 1 : 0;
+}
 extern "C" void me_plan_set_svd_lanes(me_plan *p, int lanes) {
   if (p) p->svd_lanes = lanes >= 8 ? 8 : lanes >= 4 ? 4 : lanes >= 2 ? 2 : 1;
 }

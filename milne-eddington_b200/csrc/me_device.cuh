@@ -38,6 +38,9 @@ struct DevPlan {
   int niter, nruns, hmi_ref, regul_any;
   int fixed[9], regul[9];
   int free_idx[9];  // reduced index -> full parameter index
+  // SVD solves of the one-thread-per-slot rounds with all nine parameters
+  // free: 1 = matrix in registers (svd9_kernel), 0 = in shared memory
+  int svd_regs;
   double lambda0, bshift;
   double limits[9][2];
   double step[9];
@@ -1570,6 +1573,232 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
   return hit;
 #undef GSYNC
 #undef A_
+}
+
+// gr_svd_u for a full 9x9 matrix held in registers (no parameter fixed, the
+// common case).  Once the loops over the column i (Householder, left-hand
+// accumulation) and over the block end k (QR sweeps) are unrolled, every index
+// is a compile-time constant, so the 81 elements, w and rv1 stay in registers
+// and the independent row and column updates of each step interleave.  The
+// two per-matrix indices of the QR phase -- the start l of the unreduced block
+// and the cancelled column l - 1 -- select among unrolled cases (predicated
+// on j >= l, or one case per value of l).  The operations and their order are
+// gr_svd_u's (SVD_TEMPLATE.h:84-344 without V).  A NaN matrix, for which no
+// negligible entry is found, is left unrotated (the reference's loop would
+// index below the matrix there).
+__device__ __forceinline__ int gr_svd_u9(double (&A)[9][9], double (&w)[9]) {
+  constexpr int n = 9, m = 9;
+  double rv1[9];
+  double anorm = 0., g = 0., scale = 0.;
+  int hit = 0;
+#pragma unroll
+  for (int i = 0; i < n; i++) {
+    const int l = i + 1;
+    rv1[i] = scale * g;
+    double s = 0.0;
+    g = scale = 0.0;
+#pragma unroll
+    for (int k = i; k < m; k++) scale += fabs(A[k][i]);
+    if (scale) {
+      const double is = 1.0 / scale;
+#pragma unroll
+      for (int k = i; k < m; k++) {
+        const double t = A[k][i] * is;
+        A[k][i] = t;
+        s += t * t;
+      }
+      const double f = A[i][i];
+      g = f >= 0 ? -sqrt(s) : sqrt(s);
+      const double h = f * g - s;
+      A[i][i] = f - g;
+      const double ih = 1.0 / h;
+#pragma unroll
+      for (int j = l; j < n; j++) {
+        double sj = 0.0;
+#pragma unroll
+        for (int k = i; k < m; k++) sj += A[k][i] * A[k][j];
+        const double fj = sj * ih;
+#pragma unroll
+        for (int k = i; k < m; k++) A[k][j] += fj * A[k][i];
+      }
+#pragma unroll
+      for (int k = i; k < m; k++) A[k][i] *= scale;
+    }
+    w[i] = scale * g;
+    s = 0.0;
+    g = scale = 0.0;
+    if (i != n - 1) {
+#pragma unroll
+      for (int k = l; k < n; k++) scale += fabs(A[i][k]);
+      if (scale) {
+        const double is = 1.0 / scale;
+#pragma unroll
+        for (int k = l; k < n; k++) {
+          const double t = A[i][k] * is;
+          A[i][k] = t;
+          s += t * t;
+        }
+        const double f = A[i][l];
+        g = f >= 0 ? -sqrt(s) : sqrt(s);
+        const double h = f * g - s;
+        A[i][l] = f - g;
+        const double ih = 1.0 / h;
+#pragma unroll
+        for (int k = l; k < n; k++) rv1[k] = A[i][k] * ih;
+#pragma unroll
+        for (int j = l; j < m; j++) {
+          double sj = 0.0;
+#pragma unroll
+          for (int k = l; k < n; k++) sj += A[j][k] * A[i][k];
+#pragma unroll
+          for (int k = l; k < n; k++) A[j][k] += sj * rv1[k];
+        }
+#pragma unroll
+        for (int k = l; k < n; k++) A[i][k] *= scale;
+      }
+    }
+    const double t = fabs(w[i]) + fabs(rv1[i]);
+    if (anorm < t) anorm = t;
+  }
+  // accumulation of the left-hand transformations into U
+#pragma unroll
+  for (int i = n - 1; i >= 0; i--) {
+    const int l = i + 1;
+    double gi = w[i];
+#pragma unroll
+    for (int j = l; j < n; j++) A[i][j] = 0.0;
+    if (gi != 0.0) {
+      gi = 1.0 / gi;
+      const double iaii = 1.0 / A[i][i];
+#pragma unroll
+      for (int j = l; j < n; j++) {
+        double sj = 0.0;
+#pragma unroll
+        for (int k = l; k < m; k++) sj += A[k][i] * A[k][j];
+        const double fj = (sj * iaii) * gi;
+#pragma unroll
+        for (int k = i; k < m; k++) A[k][j] += fj * A[k][i];
+      }
+#pragma unroll
+      for (int j = i; j < m; j++) A[j][i] *= gi;
+    } else {
+#pragma unroll
+      for (int j = i; j < m; j++) A[j][i] = 0.0;
+    }
+    A[i][i] += 1.0;
+  }
+  // implicit-shift QR sweeps on the bidiagonal, block end k
+#pragma unroll
+  for (int k = n - 1; k >= 0; k--) {
+    for (int its = 0; its < 50; its++) {
+      // l: start of the unreduced block; cancel: w[l - 1] is negligible
+      int l = 0;
+      bool found = false, cancel = false;
+#pragma unroll
+      for (int ll = k; ll >= 0; ll--) {
+        if (!found) {
+          if ((fabs(rv1[ll]) + anorm) == anorm) {
+            l = ll;
+            found = true;
+          } else if (ll >= 1 && (fabs(w[ll - 1]) + anorm) == anorm) {
+            l = ll;
+            found = true;
+            cancel = true;
+          }
+        }
+      }
+      if (cancel) {
+        double c = 0.0, s = 1.0;
+#pragma unroll
+        for (int lc = 1; lc <= k; lc++) {
+          if (lc == l) {
+            bool stop = false;
+#pragma unroll
+            for (int i = lc; i <= k; i++) {
+              if (!stop) {
+                const double f = s * rv1[i];
+                rv1[i] = c * rv1[i];
+                if ((fabs(f) + anorm) == anorm) {
+                  stop = true;
+                } else {
+                  const double gg = w[i];
+                  double h = pythag_d(f, gg);
+                  w[i] = h;
+                  h = 1.0 / h;
+                  c = gg * h;
+                  s = -f * h;
+#pragma unroll
+                  for (int j = 0; j < m; j++) {
+                    const double y = A[j][lc - 1], z = A[j][i];
+                    A[j][lc - 1] = y * c + z * s;
+                    A[j][i] = z * c - y * s;
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+      const double zk = w[k];
+      if (l == k) {
+        if (zk < 0.0) w[k] = -zk;
+        break;
+      }
+      if (its == 49) hit = 1;
+      double x = 0.0;
+#pragma unroll
+      for (int q = 0; q < k; q++)
+        if (q == l) x = w[q];
+      double y = w[k - 1];
+      double gq = rv1[k - 1];
+      double h = rv1[k];
+      double z = zk;
+      double f = ((y - z) * (y + z) + (gq - h) * (gq + h)) / (2.0 * h * y);
+      gq = pythag_d(f, 1.0);
+      f = ((x - z) * (x + z) + h * (y / (f + (f >= 0.0 ? gq : -gq)) - h)) / x;
+      double c = 1.0, s = 1.0;
+#pragma unroll
+      for (int j = 0; j < k; j++) {
+        if (j >= l) {
+          const int i = j + 1;
+          gq = rv1[i];
+          y = w[i];
+          h = s * gq;
+          gq *= c;
+          z = pythag_d(f, h);
+          rv1[j] = z;
+          const double iz = 1.0 / z;
+          c = f * iz;
+          s = h * iz;
+          f = x * c + gq * s;
+          gq = gq * c - x * s;
+          h = y * s;
+          y *= c;
+          z = pythag_d(f, h);
+          w[j] = z;
+          if (z) {
+            z = 1.0 / z;
+            c = f * z;
+            s = h * z;
+          }
+          f = c * gq + s * y;
+          x = c * y - s * gq;
+#pragma unroll
+          for (int jj = 0; jj < m; jj++) {
+            const double yy = A[jj][j], zz = A[jj][i];
+            A[jj][j] = yy * c + zz * s;
+            A[jj][i] = zz * c - yy * s;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < k; q++)
+        if (q == l) rv1[q] = 0.0;
+      rv1[k] = f;
+      w[k] = x;
+    }
+  }
+  return hit;
 }
 
 // x = V diag(1/w) U^T b, skipping w <= 1e-50 (svbksb, SVD_TEMPLATE.h:348-406).

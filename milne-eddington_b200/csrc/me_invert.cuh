@@ -384,6 +384,104 @@ __device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int 
   return hits;
 }
 
+// solve_slot for a plan with all nine parameters free, one thread per slot,
+// the matrix in registers (gr_svd_u9): the same trial steps and ladder.
+// Trial 1 decomposes H; trial 2 uses the factor trial 1 stored; trial
+// k >= 3 decomposes the factor trial k - 1 left (see solve_slot).
+__device__ __forceinline__ void trial_params9(const DevPlan &P, const Slots &S, int s,
+                                              const double x[9]) {
+  const int W = S.W;
+  double ptmp[9];
+  load9(S.par, W, s, ptmp);
+#pragma unroll
+  for (int q = 0; q < 9; q++) ptmp[q] += x[q] * (q == 7 ? S.sc[SC_STEP7 * W + s] : P.step[q]);
+  bounds_fold(ptmp, P, S.sc[SC_L70 * W + s], S.sc[SC_L71 * W + s]);
+  store9(S.ptmp, W, s, ptmp);
+}
+
+__device__ __forceinline__ int solve_slot9(const DevPlan &P, const Slots &S, int s) {
+  const int W = S.W;
+  const int tk = S.tk[s];
+  double x[9];
+  if (tk == 2) {  // U^T g with the stored factor, clamped
+    double g[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) g[k] = S.jvec[(size_t)k * W + s];
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int i = 0; i < 9; i++) acc += S.hess[(size_t)(i * 9 + j) * W + s] * g[i];
+      x[j] = acc > 0.5 ? 0.5 : (acc < -0.5 ? -0.5 : acc);
+    }
+    trial_params9(P, S, s, x);
+    return 0;
+  }
+  double A[9][9], w[9];
+#pragma unroll
+  for (int r = 0; r < 9; r++)
+#pragma unroll
+    for (int c = 0; c < 9; c++) A[r][c] = S.hess[(size_t)(r * 9 + c) * W + s];
+  const int hits = gr_svd_u9(A, w);
+#pragma unroll
+  for (int r = 0; r < 9; r++)
+#pragma unroll
+    for (int c = 0; c < 9; c++) S.hess[(size_t)(r * 9 + c) * W + s] = A[r][c];
+  double ug[9];  // U^T g
+  {
+    double g[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) g[k] = S.jvec[(size_t)k * W + s];
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int i = 0; i < 9; i++) acc += A[i][j] * g[i];
+      ug[j] = acc;
+    }
+  }
+  if (tk == 1) {
+    double wmax = w[0];
+#pragma unroll
+    for (int i = 1; i < 9; i++) wmax = fmax(wmax, w[i]);
+    double thr = P.svd_thr;
+    while (true) {
+      const double wthr = wmax * thr;
+      double tj[9];
+#pragma unroll
+      for (int j = 0; j < 9; j++) {
+        double wj = w[j];
+        if (wj < wthr) {
+          wj = 0.0;
+          w[j] = 0.0;
+        }
+        tj[j] = wj > 1e-50 ? ug[j] / wj : 0.0;
+      }
+      bool inside = true;
+#pragma unroll
+      for (int i = 0; i < 9; i++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 9; j++) acc += A[i][j] * tj[j];
+        x[i] = acc;
+        if (acc > 0.5 || acc < -0.5) inside = false;
+      }
+      if (inside) break;
+      if (thr > 2e-3) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) x[i] = x[i] > 0.5 ? 0.5 : (x[i] < -0.5 ? -0.5 : x[i]);
+        break;
+      }
+      thr *= 5.;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 9; j++) x[j] = ug[j] > 0.5 ? 0.5 : (ug[j] < -0.5 ? -0.5 : ug[j]);
+  }
+  trial_params9(P, S, s, x);
+  return hits;
+}
+
 // After a trial synthesis (chi_new, when the slot is in SL_TRIAL) or at a run
 // that ended without one (SL_RUN_END): the accept / reject / convergence logic
 // (Src/LM_FIT.c:588-646), the end-of-run restart policy (INVERSION,
@@ -598,6 +696,24 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_cons
     const int s = list[i];
     if (S.state[s] != SL_TRIAL) continue;
     tl.svdlim += solve_slot<kSvdBlock, 1>(P, S, s, a, w, rv1, 0, 0u);
+  }
+  tl.flush(A, S);
+}
+
+// svd_kernel for plans with all nine parameters free: each thread's matrix in
+// its registers (solve_slot9), no shared memory.
+static __global__ void __launch_bounds__(kSvdBlock) svd9_kernel(const __grid_constant__ DevPlan P,
+                                                                const __grid_constant__ InvertArgs A,
+                                                                const __grid_constant__ Slots S,
+                                                                int parity, int which) {
+  const int W = S.W;
+  Tally tl;
+  const int *list = which == 0 ? S.jlist + parity * W : S.rlist + parity * W;
+  const int count = which == 0 ? S.jcount[parity] : S.rcount[parity];
+  for (int i = blockIdx.x * kSvdBlock + threadIdx.x; i < count; i += gridDim.x * kSvdBlock) {
+    const int s = list[i];
+    if (S.state[s] != SL_TRIAL) continue;
+    tl.svdlim += solve_slot9(P, S, s);
   }
   tl.flush(A, S);
 }
@@ -1066,8 +1182,13 @@ int round_grid_impl(int which, int device) {
   } else if (which == 3) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finish_kernel<T, FILT>, kBlock, 0);
   } else {
+    // the larger of the two SVD kernels' resident grids (a grid beyond one
+    // kernel's residency only queues blocks)
     cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSvdSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, svd_kernel, kSvdBlock, kSvdSmem);
+    int per_sm9 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm9, svd9_kernel, kSvdBlock, 0);
+    if (per_sm9 > per_sm) per_sm = per_sm9;
   }
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
@@ -1084,7 +1205,12 @@ static inline void launch_svd_lanes(int lanes, const DevPlan &P, const InvertArg
     case 2: svd_grp_kernel<2><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
     case 4: svd_grp_kernel<4><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
     case 8: svd_grp_kernel<8><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
-    default: svd_kernel<<<grid, kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, which); break;
+    default:
+      if (P.npar == 9 && P.svd_regs)
+        svd9_kernel<<<grid, kSvdBlock, 0, st>>>(P, A, S, parity, which);
+      else
+        svd_kernel<<<grid, kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, which);
+      break;
   }
 }
 

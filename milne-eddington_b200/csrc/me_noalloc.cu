@@ -1,9 +1,13 @@
-// me_noalloc.cu -- the inversion entry point that allocates nothing.
+// me_invert_batch_device_noalloc -- the inversion entry point that allocates
+// nothing.  It has no counterpart in the reference; it is an addition of this
+// library.
 //
 // Some callers cannot allocate device memory when they run the inversion:
-// code that runs while a CUDA graph is being captured elsewhere in the
-// process, pipelines that hand every byte of the GPU to their own pool up
-// front, or hosts whose real-time loop must never block in the allocator.
+// data-reduction pipelines and frameworks that reserve the GPU's memory for
+// their own pool when they start (a cudaMalloc of ours would then fail, or
+// take memory their pool counts on), and real-time loops at the instrument,
+// where cudaMalloc and cudaFree can synchronise the device and stall the
+// loop for an unbounded time.
 // For them me_invert_batch_device_noalloc() does the work of
 // me_invert_batch_device() with all of its scratch -- the in-flight pixel
 // slots, the per-pixel bookkeeping of the carried LM chi^2, the wavelength
@@ -142,17 +146,28 @@ int setup(int prec, DeviceSetup **out) {
   return ME_OK;
 }
 
-// Rounds until the queue of A is exhausted and every slot is empty.
+// Rounds until the queue of A is exhausted and every slot is empty.  A pixel
+// ends within slot_step_cap(P) LM steps, and while the queue feeds the slots
+// every round advances each of the W slots by one step, so the queue empties
+// within about ceil(count / W) x cap rounds and the last pixels end within cap
+// more (the bound me_invert_batch_device uses); rounds beyond it (a
+// non-finite damping value, say) end the call with ME_ERR_TIMEOUT.
 int run_rounds(int prec, const me::DevPlan &P, const me::InvertArgs &A, const me::Slots &S,
                const int grids[3], cudaStream_t st, Small *d_small) {
   NA_CK(cudaMemsetAsync(S.state, 0, sizeof(int) * (size_t)S.W, st));  // SL_EMPTY
   NA_CK(cudaMemsetAsync(d_small, 0, offsetof(Small, totals), st));  // lists, busy, next
+  const double round_cap =
+      (double)me::slot_step_cap(P) * (double)((A.count + S.W - 1) / S.W + 1);
+  long long rounds = 0;
   int parity = 0;
   while (true) {
+    if ((double)rounds > round_cap)
+      return set_err(ME_ERR_TIMEOUT, "inversion rounds exceeded their bound");
     for (int r = 0; r < 8; r++) {
       NA_CK(me::launch_round(prec, P, A, S, parity, grids, st));
       parity ^= 1;
     }
+    rounds += 8;
     unsigned long long next = 0;
     int busy = 0;
     NA_CK(cudaMemcpyAsync(&next, &d_small->next, sizeof(next), cudaMemcpyDeviceToHost, st));
@@ -174,7 +189,7 @@ extern "C" int me_invert_batch_device_noalloc(const me_config *cfg, const double
     return set_err(ME_ERR_ARG, "npix exceeds ME_NOALLOC_MAX_PIXELS (65536): split the map");
   me::DevPlan P;
   int rc = me::build_devplan(cfg, lambda, nl, P);
-  if (rc) return set_err(rc, "invalid control file or wavelength grid");
+  if (rc) return rc;  // build_devplan recorded the cause
   // the sub-wavelength grid of an instrument filter would need scratch of its
   // own: filtered plans go through me_invert_batch_device
   if (P.nsub > 1) return set_err(ME_ERR_CONFIG, "no instrument filter without allocation");
@@ -252,8 +267,11 @@ extern "C" int me_invert_batch_device_noalloc(const me_config *cfg, const double
   if (rc) return rc;
 
   // the LM chi^2 carried from pixel to pixel: re-run the pixels whose first
-  // ratio test it flips, until none is left (as me_invert_batch_device)
-  for (int pass = 0;; pass++) {
+  // ratio test it flips, until none is left (as me_invert_batch_device).  A
+  // pass settles at least the first flipped pixel for good (only later pixels
+  // depend on it), so npix + 1 passes bound the loop.
+  for (long pass = 0;; pass++) {
+    if (pass > npix) return set_err(ME_ERR_TIMEOUT, "carried chi^2 passes exceeded their bound");
     carry_scan_kernel<<<1, 1, 0, st>>>(npix, *carry_chisq, P.regul_any, pass);
     NA_CK(cudaGetLastError());
     long long redo = 0;

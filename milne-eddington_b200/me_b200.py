@@ -144,6 +144,7 @@ EXPORTED = [
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
     "me_plan_svd_lanes", "me_plan_set_svd_lanes", "me_plan_set_graphs",
+    "me_plan_svd_registers", "me_plan_set_svd_registers",
     "me_plan_autotune", "me_plan_last_counters", "me_plan_set_overlap",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
@@ -271,6 +272,9 @@ def lib() -> ctypes.CDLL:
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
         L.me_plan_set_svd_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_svd_lanes.restype = None
+        L.me_plan_svd_registers.argtypes = [ctypes.c_void_p]
+        L.me_plan_set_svd_registers.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_svd_registers.restype = None
         L.me_invert_batch.argtypes = [ctypes.c_void_p, _D, ctypes.c_long, _D, _D,
                                       ctypes.POINTER(MeStats)]
         L.me_invert_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
@@ -460,6 +464,15 @@ class Plan:
     @svd_lanes.setter
     def svd_lanes(self, lanes: int):
         lib().me_plan_set_svd_lanes(self._h, int(lanes))
+
+    @property
+    def svd_registers(self) -> bool:
+        """SVD solves with the 9x9 matrix in registers (all nine parameters free)."""
+        return bool(lib().me_plan_svd_registers(self._h))
+
+    @svd_registers.setter
+    def svd_registers(self, on: bool):
+        lib().me_plan_set_svd_registers(self._h, int(bool(on)))
 
     def set_filter(self, offsets_mA, weights):
         """Instrument filter: offsets [mA] and weights of each observed wavelength's

@@ -147,3 +147,18 @@ def train_prior(name: str) -> dict:
 def add_noise(prof: np.ndarray, sigma: float, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed + 7919)
     return prof + rng.normal(0.0, sigma, prof.shape)
+
+
+def sample_indices(npix: int, nsample: int, seed: int = 7) -> np.ndarray:
+    """Sorted indices of a seeded sample of a map's pixels (the pixels whose
+    chi^2 is compared with the reference's, and the reference arm's input)."""
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(npix, size=min(nsample, npix), replace=False))
+
+
+def sample_noise(name: str, nsample: int, map_seed: int) -> np.ndarray:
+    """Gaussian noise [nsample][4][nl] of a map's sample pixels, drawn on the
+    host so that every process that builds the sample gets the same values."""
+    w = WORKLOADS[name]
+    rng = np.random.default_rng(map_seed + 104729)
+    return rng.normal(0.0, w["noise"], (nsample, 4, w["nl"]))

@@ -21,6 +21,8 @@
  *   meref_bounds    bounds_check (Src/ME_SOLVER.c:370).
  *   meref_rng_gauss RNG_GAUSS (Src/RANDOM_NUMBER.c:137) from the fixed seed.
  *   meref_get/set_lm_chisq  the LM->chisq value carried between pixels.
+ *   meref_reseed    the RNG state of meref_setup for another seed, carried
+ *                   LM->chisq zeroed (a fresh map in the same process).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -125,6 +127,49 @@ int meref_plan_facts(int *ints, double *limits) {
   }
   return 0;
 }
+
+/* Puts the RNG back in the state meref_setup leaves for `seed` and zeroes the
+ * LM chi^2 carried from pixel to pixel, so that a process set up once can
+ * invert a map afresh with another restart stream. */
+int meref_reseed(int seed) {
+  if (!g_ready) return -1;
+  g_lm.RNG.idum = -(int32_t)(seed & 0x7FFFFFFF);
+  g_lm.RNG.iy = 0;
+  g_lm.RNG.iset = true;
+  g_lm.chisq = 0;
+  return 0;
+}
+
+#ifdef ME_WITH_SHIM
+/* The same buffers and structures through the GPU adapter that replaces
+ * INVERSION_MULTI (milne-eddington_b200/shim/me_inversion_multi.c), for the
+ * test that runs both on one set-up.  Built into _ref/libmeshim.so only. */
+#include "me_inversion_multi.h"
+
+int meref_invert_shim(const double *prof, long npix, double *res, double *fit,
+                      int precision) {
+  if (!g_ready) return -1;
+  if (npix < 1 || npix > g_nbuf) return -2;
+  const long n = 4L * g_stk.nw;
+  memcpy(g_input.profbuff, prof, sizeof(double) * n * npix);
+  g_subset.nProf = (int)npix;
+  me_inversion_multi_set_precision(precision);
+  const int st = me_inversion_multi(&g_input, &g_stk, &g_para, &g_lm, &g_subset);
+  if (st != 0) return st;
+  memcpy(res, g_input.resbuff, sizeof(double) * 10 * npix);
+  if (fit) {
+    if (!g_input.output_fit) return -3;
+    memcpy(fit, g_input.fitbuff, sizeof(double) * n * npix);
+  }
+  return 0;
+}
+
+/* me_config of the parsed control file, as the adapter builds it. */
+int meref_shim_config(me_config *cfg) {
+  if (!g_ready) return -1;
+  return me_inversion_multi_config(&g_input, &g_stk, &g_para, &g_lm, cfg);
+}
+#endif
 
 double meref_get_lm_chisq(void) { return g_lm.chisq; }
 void meref_set_lm_chisq(double v) { g_lm.chisq = v; }

@@ -20,7 +20,6 @@ PKG = os.path.join(ROOT, "milne-eddington_b200")
 if PKG not in sys.path:
     sys.path.insert(0, PKG)
 
-import me_b200  # noqa: E402
 
 ORACLE_SO = os.path.join(ROOT, "oracle", "libme_oracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libmeref.so")
@@ -44,6 +43,10 @@ _olib = None
 def oracle_lib():
     global _olib
     if _olib is None:
+        # the oracle shares the product's control-file structure (me_config);
+        # only the Oracle class needs it, so the Reference class below loads
+        # nothing of the product
+        import me_b200
         L = ctypes.CDLL(ORACLE_SO)
         L.meo_plan_create.argtypes = [ctypes.POINTER(me_b200.MeConfig), _D, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_void_p)]
@@ -67,7 +70,7 @@ def oracle_lib():
 
 
 class Oracle:
-    def __init__(self, cfg: me_b200.MeConfig, wavelengths):
+    def __init__(self, cfg: "me_b200.MeConfig", wavelengths):
         self.cfg = cfg
         self.lam = np.ascontiguousarray(wavelengths, dtype=np.float64)
         self.nl = self.lam.size
@@ -96,6 +99,7 @@ class Oracle:
             pass
 
     def facts(self):
+        import me_b200
         f = me_b200.MePlanFacts()
         oracle_lib().meo_plan_facts(self.h, ctypes.byref(f))
         return {"nl": f.nl, "ncut": f.ncut, "ic": f.ic, "i0": f.i0, "i1": f.i1, "npar": f.npar,
@@ -202,6 +206,7 @@ def ref_lib():
         L.meref_init_guess.argtypes = [_D, _D, _D]
         L.meref_bounds.argtypes = [_D, _D]
         L.meref_rng_gauss.argtypes = [ctypes.c_int, ctypes.c_long, _D]
+        L.meref_reseed.argtypes = [ctypes.c_int]
         _rlib = L
     return _rlib
 
@@ -232,6 +237,11 @@ class Reference:
                                         _p(fit[s:e]) if want_fit else None)
             assert st == 0, st
         return (res, fit) if want_fit else res
+
+    def reseed(self, seed: int):
+        """The RNG state of a fresh set-up with `seed`, carried LM chi^2 zeroed."""
+        st = ref_lib().meref_reseed(int(seed))
+        assert st == 0, st
 
     @property
     def lm_chisq(self):
@@ -286,3 +296,121 @@ def ref_rng_gauss(seed, n):
     out = np.zeros(n)
     ref_lib().meref_rng_gauss(seed, n, _p(out))
     return out
+
+
+# ---------------------------------------------------------------------------
+# the oracle over host cores: contiguous chunks of a map in spawned processes
+# ---------------------------------------------------------------------------
+_PW = {}
+
+
+def _pool_init(ctl_text, lam):
+    for p in (PKG, os.path.dirname(os.path.abspath(__file__))):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import me_b200
+    _PW["orc"] = Oracle(me_b200.parse_config_text(ctl_text), lam)
+
+
+def _pool_invert(job):
+    prof, offset, rng_mode, nr_seed = job
+    orc = _PW["orc"]
+    orc.carry[0] = 0.0
+    return orc.invert(prof, pixel_offset=offset, rng_mode=rng_mode, nr_seed=nr_seed)
+
+
+def oracle_invert_chunks(ctl_text, lam, prof, chunk, procs=None, rng_mode=MEO_RNG_COUNTER,
+                         nr_seed=0):
+    """The oracle on prof [n][4][nl] in contiguous chunks of `chunk` pixels,
+    each chunk a fresh run (carried LM chi^2 0 at its first pixel, as a new
+    reference process starts; per-pixel restart draws keyed by the pixel's
+    index in the whole map), the chunks spread over `procs` spawned
+    processes.  Compare with a GPU plan inverting the same chunks with its
+    carried chi^2 reset to 0 before each."""
+    import multiprocessing as mp
+    n = prof.shape[0]
+    jobs = [(np.ascontiguousarray(prof[s:s + chunk]), s, rng_mode, nr_seed)
+            for s in range(0, n, chunk)]
+    procs = procs or min(len(jobs), os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(procs, initializer=_pool_init,
+                                      initargs=(ctl_text, np.asarray(lam))) as pool:
+        return np.concatenate(pool.map(_pool_invert, jobs))
+
+
+# ---------------------------------------------------------------------------
+# the reference's core and the GPU adapter that replaces its INVERSION_MULTI
+# (milne-eddington_b200/shim/me_inversion_multi.c) on one set-up
+# ---------------------------------------------------------------------------
+SHIM_SO = os.path.join(ROOT, "oracle", "_ref", "libmeshim.so")
+_slib = None
+
+
+def shim_available() -> bool:
+    return os.path.exists(SHIM_SO)
+
+
+def shim_lib():
+    global _slib
+    if _slib is None:
+        import me_b200  # the adapter links the product library
+        L = ctypes.CDLL(SHIM_SO)
+        L.meref_setup.argtypes = [ctypes.c_char_p, _D, ctypes.c_int, ctypes.c_long, ctypes.c_int,
+                                  ctypes.c_char_p]
+        L.meref_invert.argtypes = [_D, ctypes.c_long, _D, _D]
+        L.meref_invert_shim.argtypes = [_D, ctypes.c_long, _D, _D, ctypes.c_int]
+        L.meref_shim_config.argtypes = [ctypes.POINTER(me_b200.MeConfig)]
+        L.meref_get_lm_chisq.restype = ctypes.c_double
+        L.meref_set_lm_chisq.argtypes = [ctypes.c_double]
+        L.meref_set_lm_chisq.restype = None
+        _slib = L
+    return _slib
+
+
+class ShimHarness:
+    """RDINPUT + INIT_INV of the reference once per process (in libmeshim.so),
+    then the same structures through the reference's INVERSION_MULTI or
+    through me_inversion_multi (the GPU)."""
+
+    def __init__(self, ctl_text: str, wavelengths, npix_max: int, seed: int = 12345):
+        self.dir = tempfile.mkdtemp(prefix="meshim_")
+        self.ctl = os.path.join(self.dir, "input")
+        with open(self.ctl, "w") as f:
+            f.write(ctl_text.replace("./input", self.ctl))
+        self.lam = np.ascontiguousarray(wavelengths, dtype=np.float64)
+        self.nl = self.lam.size
+        self.npix_max = npix_max
+        st = shim_lib().meref_setup(self.ctl.encode(), _p(self.lam), self.nl, npix_max, seed,
+                                    self.dir.encode())
+        assert st == 0, f"meref_setup: {st}"
+
+    def _run(self, prof, shim, precision):
+        prof = np.ascontiguousarray(prof, dtype=np.float64)
+        n = prof.shape[0]
+        assert n <= self.npix_max
+        res = np.zeros((n, 10))
+        if shim:
+            st = shim_lib().meref_invert_shim(_p(prof), n, _p(res), None, precision)
+        else:
+            st = shim_lib().meref_invert(_p(prof), n, _p(res), None)
+        assert st == 0, st
+        return res
+
+    def invert_reference(self, prof):
+        return self._run(prof, False, 0)
+
+    def invert_shim(self, prof, precision):
+        return self._run(prof, True, precision)
+
+    def config(self):
+        import me_b200
+        cfg = me_b200.MeConfig()
+        assert shim_lib().meref_shim_config(ctypes.byref(cfg)) == 0
+        return cfg
+
+    @property
+    def lm_chisq(self):
+        return shim_lib().meref_get_lm_chisq()
+
+    @lm_chisq.setter
+    def lm_chisq(self, v):
+        shim_lib().meref_set_lm_chisq(float(v))

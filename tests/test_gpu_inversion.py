@@ -5,14 +5,19 @@ large share of pixels to another trajectory (tests/test_oracle_vs_reference.py
 shows it on the reference itself).  The CUDA path rounds differently (FMA,
 CUDA libm, summation order), so per-pixel equality cannot hold for those
 pixels.  Parity is therefore judged against the reference's own ulp
-sensitivity, measured in the same test: the oracle on the same input versus
-the oracle on the input perturbed by one ulp.  The GPU must be no further
-from the oracle than that, within a stated margin:
+sensitivity, measured in the same test on the same 8192 pixels: the oracle on
+the same input versus the oracle on the input perturbed by one ulp.  The GPU
+must be no further from the oracle than that, within a margin of about three
+standard errors of the difference of two shares on 8192 pixels (a share near
+0.75 has a standard error of 0.005 there):
   * identical pixels (all 10 outputs within 1e-6 relative): FP64 at least the
-    self-perturbation share minus 0.10;
+    self-perturbation share minus 0.03;
   * chi^2 <= 1.05 x the oracle's chi^2: at least the self-perturbation share
-    minus 0.05 (FP64 and FP32);
+    minus 0.02 (FP64 and FP32);
   * the median chi^2 ratio within 1e-3 of 1.
+The map is inverted in chunks of 1024 pixels, each a fresh run (carried LM
+chi^2 0 at its first pixel) on both sides, so that the oracle can run the
+chunks in parallel on the host cores.
 """
 import numpy as np
 import pytest
@@ -22,6 +27,8 @@ import me_maps
 import oracle_bind as ob
 
 pytestmark = pytest.mark.gpu
+
+CHUNK = 1024
 
 
 def ulp_perturb(prof, seed=5):
@@ -37,20 +44,31 @@ def agreement(res, base):
     return same.mean(), np.mean(ratio[valid] <= 1.05), np.median(ratio[valid])
 
 
+def invert_chunks(plan, prof):
+    """plan.invert over contiguous chunks of CHUNK pixels, the carried LM
+    chi^2 reset to 0 before each (the oracle side's chunking)."""
+    out, stats = [], []
+    for s in range(0, prof.shape[0], CHUNK):
+        plan.carry_chisq = 0.0
+        r, st = plan.invert(prof[s:s + CHUNK])
+        out.append(r)
+        stats.append(st)
+    return np.concatenate(out), stats
+
+
 @pytest.fixture(scope="module")
 def cfg0_map():
     name = "fe15648_64x64"
     lam = me_maps.wavelengths(name)
-    cfg = me_b200.parse_config_text(me_maps.control_text(name, precision="FP64"))
+    ctl = me_maps.control_text(name, precision="FP64")
+    cfg = me_b200.parse_config_text(ctl)
     orc = ob.Oracle(cfg, lam)
-    npix = 2048
+    npix = 8192
     par = me_maps.draw_parameters(name, npix, 21)
     prof = me_maps.add_noise(orc.synth_many(par), 1e-3, 21)
-    base = orc.invert(prof)
-    orc2 = ob.Oracle(cfg, lam)
-    pert = orc2.invert(ulp_perturb(prof))
-    return dict(name=name, lam=lam, prof=prof, base=base, carry=orc.carry[0],
-                self=agreement(pert, base))
+    base = ob.oracle_invert_chunks(ctl, lam, prof, CHUNK)
+    pert = ob.oracle_invert_chunks(ctl, lam, ulp_perturb(prof), CHUNK)
+    return dict(name=name, lam=lam, prof=prof, base=base, self=agreement(pert, base))
 
 
 # (max_group, tail_slots, svd_lanes): one thread per pixel throughout;
@@ -67,23 +85,48 @@ def test_inversion_parity_vs_oracle(cfg0_map, prec, mode):
     cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
     with me_b200.Plan(cfg, m["lam"]) as plan:
         plan.max_group, plan.tail_slots, plan.svd_lanes = MODES[mode]
-        res, st = plan.invert(m["prof"])
-    tail_launches = st["launches"] - 4 * st["rounds"]
-    assert tail_launches == (0 if MODES[mode][1] == 0 else 1)
+        res, stats = invert_chunks(plan, m["prof"])
+    for st in stats:
+        tail_launches = st["launches"] - 4 * st["rounds"]
+        assert tail_launches == (0 if MODES[mode][1] == 0 else 1)
     same, within, med = agreement(res, m["base"])
     s_same, s_within, _ = m["self"]
     print(f"{prec} {mode}: identical {same:.3f} (self {s_same:.3f}), chi2<=1.05x "
-          f"{within:.3f} (self {s_within:.3f}), median ratio {med:.6f}, rounds {st['rounds']}")
-    assert st["valid"] == np.sum(m["base"][:, 9] > 0)
+          f"{within:.3f} (self {s_within:.3f}), median ratio {med:.6f}")
+    assert sum(st["valid"] for st in stats) == np.sum(m["base"][:, 9] > 0)
     assert abs(med - 1) < 1e-3
-    assert within >= s_within - 0.05
+    assert within >= s_within - 0.02
     if prec == "FP64":
-        assert same >= s_same - 0.10
+        assert same >= s_same - 0.03
     # skipped pixels are zeros exactly where the oracle's are
     np.testing.assert_array_equal(res[:, 9] == 0, m["base"][:, 9] == 0)
     # parameters stay inside the bounds / folds
     v = res[:, 9] > 0
     assert np.all((res[v, 1] >= 0) & (res[v, 1] <= np.pi) & (res[v, 2] >= 0) & (res[v, 2] < np.pi))
+
+
+@pytest.mark.parametrize("prec", ["FP64", "FP32"])
+def test_svd_registers_vs_shared_memory(cfg0_map, prec):
+    """The SVD solve with the 9x9 matrix in registers (svd9_kernel) runs the
+    shared-memory kernel's operations in the same order: with one thread per
+    pixel throughout, the two give the same results for (nearly) every
+    pixel; the few the compiler's multiply-add contraction may separate
+    still meet the oracle bar."""
+    m = cfg0_map
+    cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
+    out = {}
+    for regs in (True, False):
+        with me_b200.Plan(cfg, m["lam"]) as plan:
+            plan.max_group, plan.tail_slots, plan.svd_lanes = 1, 0, 1
+            plan.svd_registers = regs
+            assert plan.svd_registers == regs
+            out[regs], _ = invert_chunks(plan, m["prof"])
+    same = np.mean(np.all(out[True] == out[False], axis=1))
+    _, within, med = agreement(out[True], m["base"])
+    print(f"{prec}: registers vs shared memory bitwise identical {same:.4f}; "
+          f"vs oracle within 1.05 {within:.3f}, median ratio {med:.6f}")
+    assert same >= 0.95
+    assert abs(med - 1) < 1e-3 and within >= m["self"][1] - 0.02
 
 
 def test_restarts_counter_rng_vs_oracle():
