@@ -38,8 +38,8 @@ distributions, other seeds than the map's, 20 epochs of Adam, lr 1e-3, batch
 A step is one inversion of the whole map.  The map (2 GB of FP64 profiles,
 larger than L2) is resident in HBM when the timed region starts; `e2e` times
 the same step through the host entry point me_invert_batch with the profiles
-in pinned host memory (host->device copy, inference, inversion, device->host
-copy of the results).
+and the results in pinned host memory (host->device copy, inference,
+inversion, device->host copy of the results).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     torchrun --nproc-per-node N bench.py --gpus N ...   (one rank per GPU)
@@ -796,14 +796,16 @@ def main():
         h_prof = torch.empty((npix, 4, nl), dtype=torch.float64, pin_memory=True)
         h_prof.copy_(prof)
         h_prof_np = h_prof.numpy()
+        h_res = torch.empty((npix, 10), dtype=torch.float64, pin_memory=True)
+        h_res_np = h_res.numpy()
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            _, st_e2e = plan.invert(h_prof_np)
+            _, st_e2e = plan.invert(h_prof_np, out=h_res_np)
         e2e_s = me_ranks.max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, dist, "cuda")
         e2e = {"seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"], "d2h_ms": st_e2e["d2h_ms"]}
-        del h_prof, h_prof_np
+        del h_prof, h_prof_np, h_res, h_res_np
 
     res_np = res.cpu().numpy()
     res_plain_np = res_plain.cpu().numpy()

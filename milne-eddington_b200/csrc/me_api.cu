@@ -141,7 +141,19 @@ struct me_plan {
   // start (me_plan_set_queue_order): keys, histograms and the order
   bool queue_order = true;
   DevBuf d_okey, d_ohist, d_order;
+  // the host entry point's chunked copy of a map in page-locked memory,
+  // overlapped with the inversion (me_plan_set_feed): the copy stream, the
+  // stream that makes each chunk's learned guesses and queue order, the
+  // device count of queue positions that have arrived and its host values
+  bool feed = true;
+  cudaStream_t copy_stream = nullptr, prep_stream = nullptr;
+  DevBuf d_avail;
+  unsigned long long *h_feed = nullptr;  // pinned, kMaxFeedChunks
+  std::vector<cudaEvent_t> feed_events;
 };
+
+// chunks of the host entry point's overlapped copy (at most)
+constexpr int kMaxFeedChunks = 64;
 
 extern "C" const char *me_version(void) { return "me_b200 0.1 (sm_100a)"; }
 
@@ -322,6 +334,15 @@ extern "C" int me_plan_set_filter(me_plan *p, const double *offsets_mA, const do
   return set_filter_grid(p, offsets_mA, weights, k);
 }
 
+// a non-blocking stream at the device's highest priority (returns nonzero on
+// failure, like the CUDA calls it sits among)
+static cudaError_t create_priority_stream(cudaStream_t *s) {
+  int lo = 0, hi = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  if (e != cudaSuccess) return e;
+  return cudaStreamCreateWithPriority(s, cudaStreamNonBlocking, hi);
+}
+
 extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl, int device,
                               me_plan **out) {
   if (!cfg || !lambda || !out) return fail(ME_ERR_ARG, "null argument");
@@ -346,6 +367,8 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
       p->d_next.ensure(sizeof(unsigned long long)) ||
       cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) ||
       cudaStreamCreateWithFlags(&p->stream2, cudaStreamNonBlocking) ||
+      cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking) ||
+      create_priority_stream(&p->prep_stream) ||
       cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) ||
       cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) ||
       cudaEventCreate(&p->ev0) || cudaEventCreate(&p->ev1) ||
@@ -371,7 +394,9 @@ extern "C" int me_plan_create(const me_config *cfg, const double *lambda, int nl
   p->grid_svd = me::round_grid(p->precision, 2, device);
   p->grid_fin = me::round_grid(p->precision, 3, device);
   p->grid = p->grid_trial;
-  if (cudaMallocHost((void **)&p->h_poll, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+  if (cudaMallocHost((void **)&p->h_poll, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMallocHost((void **)&p->h_feed, kMaxFeedChunks * sizeof(unsigned long long)) !=
+          cudaSuccess) {
     me_plan_destroy(p);
     return fail(ME_ERR_CUDA, "pinned allocation failed");
   }
@@ -399,9 +424,14 @@ extern "C" void me_plan_destroy(me_plan *p) {
                     &p->d_list,   &p->d_slot_pix, &p->d_slot_i32, &p->d_slot_cnt,
                     &p->d_slot_u8, &p->d_slot_sc, &p->d_slot_vec, &p->d_slot_hess,
                     &p->d_slot_list, &p->d_slot_small, &p->d_fitpar, &p->d_init,
-                    &p->d_flambda, &p->d_fdlambda, &p->d_okey, &p->d_ohist, &p->d_order};
+                    &p->d_flambda, &p->d_fdlambda, &p->d_okey, &p->d_ohist, &p->d_order,
+                    &p->d_avail};
   for (DevBuf *b : bufs) b->release();
   if (p->h_poll) cudaFreeHost(p->h_poll);
+  if (p->h_feed) cudaFreeHost(p->h_feed);
+  for (cudaEvent_t e : p->feed_events) cudaEventDestroy(e);
+  if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+  if (p->prep_stream) cudaStreamDestroy(p->prep_stream);
   if (p->ev0) cudaEventDestroy(p->ev0);
   if (p->ev1) cudaEventDestroy(p->ev1);
   for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
@@ -584,7 +614,8 @@ cudaEvent_t *take_events(me_plan *p, size_t n) {
 // svd_kernel and trial_kernel on the plan's slots while the queue feeds them,
 // then, once it is empty and at most tail_slots pixels remain, finish_kernel
 // (one warp per pixel, no per-round launches) for the rest.
-int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &rounds) {
+int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &rounds,
+              cudaEvent_t feed_done = nullptr) {
   const long long cap = p->window > 0 ? p->window : 131072;
   const int W = (int)(A.count < cap ? A.count : cap);
   if (W <= 0) return ME_OK;
@@ -636,9 +667,25 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
   rounds = 0;
   // every slot step is one round: a bound no valid batch reaches
   const double round_cap = (double)me::slot_step_cap(p->P) * (double)((A.count + W - 1) / W + 1);
+  // with a feed (A.avail), slots may hold queue positions that have not
+  // arrived (SL_WAIT); the queue counts as drained only after a batch of full
+  // rounds that started once the last position had arrived (its trial
+  // kernels took every held position up)
+  bool fed = feed_done == nullptr;
   while (true) {
     if ((double)rounds > round_cap)
       return fail(ME_ERR_TIMEOUT, "inversion rounds exceeded their bound");
+    bool fed_before = fed;
+    if (!fed_before) {
+      const cudaError_t q = cudaEventQuery(feed_done);
+      if (q == cudaSuccess) {
+        fed_before = true;
+      } else if (q == cudaErrorNotReady) {
+        cudaGetLastError();  // not an error: clear it
+      } else {
+        return fail(ME_ERR_CUDA, std::string("feed: ") + cudaGetErrorString(q));
+      }
+    }
     // the rounds between two polls: one CUDA graph per lane-group size,
     // captured once per queue on the plan's stream (an even number of rounds
     // starts every batch at parity 0), or direct launches when profiling
@@ -699,7 +746,8 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     CK(cudaMemcpyAsync(p->h_poll + 1, S.busy, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     const int busy = *reinterpret_cast<int *>(p->h_poll + 1);
-    const bool drained = p->h_poll[0] >= (unsigned long long)A.count;
+    if (fed_before) fed = true;
+    const bool drained = p->h_poll[0] >= (unsigned long long)A.count && fed;
     if (drained && busy == 0) break;
     if (drained && p->max_group > 1) {
       // the queue is empty: give each slot in flight as many lanes as fill
@@ -745,11 +793,21 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
 
 }  // namespace
 
-extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npix, double *d_res,
-                                      double *d_fit, void *stream, me_stats *stats) {
-  if (!p || !d_prof || !d_res || npix < 0) return fail(ME_ERR_ARG, "null argument");
-  CK(cudaSetDevice(p->device));
-  cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+namespace {
+
+// A map that the host entry point is still copying in (me_invert_batch): the
+// queue positions below *avail are on the device; `done` is recorded once
+// the last has arrived.  With a learned start the feed also made each chunk's
+// guesses (plan d_init) and, with the queue order, its order (plan d_order,
+// sorted within the chunk); init_ms is their device time.
+struct Feed {
+  const unsigned long long *avail;
+  cudaEvent_t done;
+  float init_ms;
+};
+
+int invert_impl(me_plan *p, const double *d_prof, long npix, double *d_res, double *d_fit,
+                cudaStream_t st, me_stats *stats, const Feed *feed) {
   if (stats) memset(stats, 0, sizeof(*stats));
   if (npix == 0) return ME_OK;
   const size_t n = (size_t)npix;
@@ -779,8 +837,13 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   A.stale = nullptr;
   A.carry = p->carry;
   A.first_pixel = 0;
+  A.avail = feed ? feed->avail : nullptr;
   float init_ms = 0.f;
-  if (p->init) {
+  if (p->init && feed) {
+    // guesses and order came with the chunks (me_invert_batch)
+    A.init_par = p->d_init.as<double>();
+    if (p->queue_order) A.list = p->d_order.as<long long>();
+  } else if (p->init) {
     CK(p->d_init.ensure(n * 9 * sizeof(double)));
     CK(cudaEventRecord(p->ev0, st));
     const int rc = me_mlp_predict_device(p->init, d_prof, npix, p->d_init.as<double>(), st);
@@ -814,10 +877,15 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   p->ev_marks.clear();
   p->tail_seen = false;
   CK(cudaEventRecord(p->ev0, st));
-  int rc = run_queue(p, A, st, rounds);
+  int rc = run_queue(p, A, st, rounds, feed ? feed->done : nullptr);
   if (rc) return rc;
   CK(cudaEventRecord(p->ev1, st));
   rounds_total += rounds;
+  if (p->init && feed) {
+    const int grc = me::mlp_gemm_status(p->init);
+    if (grc) return grc;
+    init_ms = feed->init_ms;
+  }
 
   // The reference carries LM->chisq from pixel to pixel; it enters only the
   // first regularisation ratio test of each pixel (Src/LM_FIT.c:555-559).  The
@@ -875,6 +943,7 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
     B.list = p->d_list.as<long long>();
     B.count = (long long)m;
     B.stale = p->d_stale.as<double>();
+    B.avail = nullptr;  // the whole map is on the device by now
     CK(cudaEventRecord(p->ev0, st));
     rc = run_queue(p, B, st, rounds);
     if (rc) return rc;
@@ -937,6 +1006,128 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   return ME_OK;
 }
 
+// Pixels per chunk of the overlapped copy of an npix map (0: copy it whole).
+// A multiple of 64 pixels, so that no 128-byte line of the profiles, the
+// guesses or the queue order straddles two chunks.
+long long feed_chunk(long long npix) {
+  constexpr long long kMin = 65536;
+  if (npix < 2 * kMin) return 0;
+  long long c = (npix + 7) / 8;
+  if (c < kMin) c = kMin;
+  c = (c + 63) / 64 * 64;
+  while ((npix + c - 1) / c > kMaxFeedChunks) c += 64;
+  return c;
+}
+
+bool host_page_locked(const void *ptr) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// The copy of the map in chunks on the copy stream, each chunk announced to
+// the rounds by raising *avail once it is on the device -- after, with a
+// learned start, its guesses and its queue order (sorted within the chunk)
+// were made on the priority stream -- so that the inversion starts on the
+// first chunk while the rest is still on its way.  Fills f; the copy's own
+// device time goes to *h2d_ms once the batch is over (events e0, e1).
+int start_feed(me_plan *p, const double *prof, long long npix, long long chunk, Feed &f,
+               cudaEvent_t e0, cudaEvent_t e1) {
+  const long long nl = p->P.nl;
+  const long long nch = (npix + chunk - 1) / chunk;
+  const size_t n = (size_t)npix;
+  const bool learned = p->init != nullptr;
+  CK(p->d_avail.ensure(sizeof(unsigned long long)));
+  if (learned) {
+    CK(p->d_init.ensure(n * 9 * sizeof(double)));
+    if (p->queue_order) {
+      CK(p->d_okey.ensure(n));
+      CK(p->d_ohist.ensure((size_t)me::kOrderBuckets * me::kOrderBlocks * sizeof(int)));
+      CK(p->d_order.ensure(n * sizeof(long long)));
+    }
+  }
+  // events: start, feed done, and per chunk arrival + prep start/end
+  const size_t need = 2 + 3 * (size_t)nch;
+  while (p->feed_events.size() < need) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    p->feed_events.push_back(e);
+  }
+  cudaEvent_t ev_start = p->feed_events[0], ev_done = p->feed_events[1];
+  unsigned long long *d_avail = p->d_avail.as<unsigned long long>();
+  // avail = 0 before the rounds look at it; the feed streams start after that
+  CK(cudaMemsetAsync(d_avail, 0, sizeof(unsigned long long), p->stream));
+  CK(cudaEventRecord(ev_start, p->stream));
+  CK(cudaStreamWaitEvent(p->copy_stream, ev_start, 0));
+  if (learned) CK(cudaStreamWaitEvent(p->prep_stream, ev_start, 0));
+  CK(cudaEventRecord(e0, p->copy_stream));
+  double *d_prof = p->d_prof.as<double>();
+  for (long long k = 0; k < nch; k++) {
+    const long long s0 = k * chunk, s1 = std::min(npix, s0 + chunk);
+    const size_t off = (size_t)s0 * 4 * nl;
+    CK(cudaMemcpyAsync(d_prof + off, prof + off, (size_t)(s1 - s0) * 4 * nl * sizeof(double),
+                       cudaMemcpyHostToDevice, p->copy_stream));
+    p->h_feed[k] = (unsigned long long)s1;
+    if (!learned) {
+      // in order on the copy stream: the count rises after the chunk landed
+      CK(cudaMemcpyAsync(d_avail, p->h_feed + k, sizeof(unsigned long long),
+                         cudaMemcpyHostToDevice, p->copy_stream));
+      continue;
+    }
+    cudaEvent_t arrived = p->feed_events[2 + 3 * k];
+    cudaEvent_t pb = p->feed_events[3 + 3 * k], pe = p->feed_events[4 + 3 * k];
+    CK(cudaEventRecord(arrived, p->copy_stream));
+    CK(cudaStreamWaitEvent(p->prep_stream, arrived, 0));
+    CK(cudaEventRecord(pb, p->prep_stream));
+    double *d_init = p->d_init.as<double>() + (size_t)s0 * 9;
+    const int rc = me_mlp_predict_device(p->init, d_prof + off, s1 - s0, d_init, p->prep_stream);
+    if (rc) return rc;
+    if (p->queue_order)
+      CK(me::launch_start_order(p->precision, p->P, d_prof + off, d_init, s1 - s0,
+                                p->d_okey.as<unsigned char>() + s0, p->d_ohist.as<int>(),
+                                p->d_order.as<long long>() + s0, p->prep_stream, s0));
+    CK(cudaEventRecord(pe, p->prep_stream));
+    CK(cudaMemcpyAsync(d_avail, p->h_feed + k, sizeof(unsigned long long),
+                       cudaMemcpyHostToDevice, p->prep_stream));
+  }
+  CK(cudaEventRecord(e1, p->copy_stream));
+  CK(cudaEventRecord(ev_done, learned ? p->prep_stream : p->copy_stream));
+  f.avail = d_avail;
+  f.done = ev_done;
+  f.init_ms = 0.f;
+  return ME_OK;
+}
+
+// Device time of the feed's learned-start work (after the batch).
+float feed_init_ms(me_plan *p, long long npix, long long chunk) {
+  if (!p->init) return 0.f;
+  float sum = 0.f;
+  const long long nch = (npix + chunk - 1) / chunk;
+  for (long long k = 0; k < nch; k++) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, p->feed_events[3 + 3 * k], p->feed_events[4 + 3 * k]);
+    sum += t;
+  }
+  return sum;
+}
+
+}  // namespace
+
+extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npix, double *d_res,
+                                      double *d_fit, void *stream, me_stats *stats) {
+  if (!p || !d_prof || !d_res || npix < 0) return fail(ME_ERR_ARG, "null argument");
+  CK(cudaSetDevice(p->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+  return invert_impl(p, d_prof, npix, d_res, d_fit, st, stats, nullptr);
+}
+
+extern "C" void me_plan_set_feed(me_plan *p, int on) {
+  if (p) p->feed = on != 0;
+}
+
 extern "C" int me_invert_batch(me_plan *p, const double *prof, long npix, double *res, double *fit,
                                me_stats *stats) {
   if (!p || !prof || !res || npix < 0) return fail(ME_ERR_ARG, "null argument");
@@ -955,11 +1146,32 @@ extern "C" int me_invert_batch(me_plan *p, const double *prof, long npix, double
   cudaEventCreate(&e1);
   cudaEventCreate(&e2);
   cudaEventCreate(&e3);
-  cudaEventRecord(e0, p->stream);
-  CK(cudaMemcpyAsync(p->d_prof.p, prof, pbytes, cudaMemcpyHostToDevice, p->stream));
-  cudaEventRecord(e1, p->stream);
-  int rc = me_invert_batch_device(p, p->d_prof.as<double>(), npix, p->d_res.as<double>(),
-                                  fit ? p->d_fit.as<double>() : nullptr, p->stream, stats);
+  // a map in page-locked memory goes in chunks that the inversion starts on
+  // as they land; from pageable memory a copy cannot run beside the host's
+  // launches, so it goes whole first
+  const long long chunk = p->feed ? feed_chunk(npix) : 0;
+  int rc = ME_OK;
+  if (chunk > 0 && host_page_locked(prof)) {
+    Feed f;
+    rc = start_feed(p, prof, npix, chunk, f, e0, e1);
+    if (rc == ME_OK)
+      rc = invert_impl(p, p->d_prof.as<double>(), npix, p->d_res.as<double>(),
+                       fit ? p->d_fit.as<double>() : nullptr, p->stream, stats, &f);
+    if (rc == ME_OK && stats) {
+      stats->init_ms = feed_init_ms(p, npix, chunk);
+      CK(cudaStreamSynchronize(p->copy_stream));
+    }
+    if (rc != ME_OK) {  // leave no copy running into the plan's buffers
+      cudaStreamSynchronize(p->copy_stream);
+      cudaStreamSynchronize(p->prep_stream);
+    }
+  } else {
+    cudaEventRecord(e0, p->stream);
+    CK(cudaMemcpyAsync(p->d_prof.p, prof, pbytes, cudaMemcpyHostToDevice, p->stream));
+    cudaEventRecord(e1, p->stream);
+    rc = invert_impl(p, p->d_prof.as<double>(), npix, p->d_res.as<double>(),
+                     fit ? p->d_fit.as<double>() : nullptr, p->stream, stats, nullptr);
+  }
   if (rc == ME_OK) {
     cudaEventRecord(e2, p->stream);
     cudaError_t e = cudaMemcpyAsync(res, p->d_res.p, n * 10 * sizeof(double),

@@ -144,15 +144,33 @@ __device__ __forceinline__ void store9(double *a, int W, int s, const double *v)
 
 // Takes pixels from the queue until one is valid (INVERSION_MULTI's gate and
 // Init_Guess, Src/LM_FIT.c:776-789) and sets the slot up for its first run.
-// Skipped pixels get zeros.  Returns false when the queue is exhausted.
-static __device__ bool refill(const DevPlan &P, const InvertArgs &A, const Slots &S, int s,
-                       unsigned long long &t_valid) {
+// Skipped pixels get zeros.  Returns kRefilled, kExhausted when the queue is
+// exhausted, or kWaiting when the queue position drawn is not on the device
+// yet (A.avail): the slot then keeps the position (SL_WAIT, S.pix = the
+// position) and calls again with it (held) in a later round.
+enum RefillResult : int { kExhausted = 0, kRefilled = 1, kWaiting = 2 };
+
+static __device__ int refill(const DevPlan &P, const InvertArgs &A, const Slots &S, int s,
+                             unsigned long long &t_valid, long long held = -1) {
   const int nl = P.nl;
   const int W = S.W;
   while (true) {
-    const unsigned long long k = atomicAdd(A.next, 1ULL);
-    if (k >= (unsigned long long)A.count) return false;
-    const long long pix = A.list ? A.list[k] : (long long)k;
+    unsigned long long k;
+    if (held >= 0) {
+      k = (unsigned long long)held;
+      held = -1;
+    } else {
+      k = atomicAdd(A.next, 1ULL);
+      if (k >= (unsigned long long)A.count) return kExhausted;
+    }
+    if (A.avail && k >= *(volatile const unsigned long long *)A.avail) {
+      S.pix[s] = (long long)k;
+      S.state[s] = SL_WAIT;
+      return kWaiting;
+    }
+    // with a feed (A.avail) the list and the guesses were written while this
+    // kernel may run: read them past the L1 cache
+    const long long pix = A.list ? (A.avail ? __ldcg(A.list + k) : A.list[k]) : (long long)k;
     const double *pp = A.prof + (size_t)pix * 4 * nl;
     PixelInit pin;
     const int bad = init_guess(pp, P, pin, true);
@@ -174,7 +192,8 @@ static __device__ bool refill(const DevPlan &P, const InvertArgs &A, const Slots
       double q[9];
 #pragma unroll
       for (int i = 0; i < 9; i++) {
-        const double v = A.init_par[(size_t)pix * 9 + i];
+        const double v = A.avail ? __ldcg(A.init_par + (size_t)pix * 9 + i)
+                                 : A.init_par[(size_t)pix * 9 + i];
         q[i] = (P.fixed[i] || !isfinite(v)) ? pin.guess[i] : v;
       }
       bounds_fold(q, P, pin.l70, pin.l71);
@@ -200,7 +219,7 @@ static __device__ bool refill(const DevPlan &P, const InvertArgs &A, const Slots
     for (int i = 0; i < 4; i++) S.cnt[i * W + s] = 0;
     S.had_trial[s] = 0;
     S.state[s] = SL_JAC_START;
-    return true;
+    return kRefilled;
   }
 }
 
@@ -623,12 +642,13 @@ __device__ __forceinline__ void trial_transition(const DevPlan &P, const InvertA
         reinterpret_cast<uint4 *>(A.counters)[pix] = c4;
       }
       t.iter += S.cnt[1 * W + s];
-      if (ROUNDS && refill(P, A, S, s, t.valid)) {
+      const int got = ROUNDS ? refill(P, A, S, s, t.valid) : kExhausted;
+      if (got == kRefilled) {
         append_jac(S, next_parity, s);
-      } else {
+      } else if (got == kExhausted) {
         S.state[s] = SL_DONE;
         t.busy_delta--;
-      }
+      }  // kWaiting: the slot holds a queue position (still busy)
     }
   }
 }
@@ -738,12 +758,14 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < W; s += gridDim.x * blockDim.x) {
     const int st = S.state[s];
     if (st == SL_DONE) continue;
-    if (st == SL_EMPTY) {
-      if (refill(P, A, S, s, t.valid)) {
-        t.busy_delta++;
-        append_jac(S, next_parity, s);
-      } else {
+    if (st == SL_EMPTY || st == SL_WAIT) {
+      // a waiting slot counts as busy; it takes up the position it holds
+      const int r = refill(P, A, S, s, t.valid, st == SL_WAIT ? S.pix[s] : -1);
+      if (r == kRefilled) append_jac(S, next_parity, s);
+      if (st == SL_EMPTY && r != kExhausted) t.busy_delta++;
+      if (r == kExhausted) {
         S.state[s] = SL_DONE;
+        if (st == SL_WAIT) t.busy_delta--;
       }
       continue;
     }

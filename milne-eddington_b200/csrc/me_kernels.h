@@ -31,6 +31,8 @@ enum SlotStateCode : int {
   SL_TRIAL = 3,      // normal equations ready: trial steps
   SL_RUN_END = 4,    // run ended without a trial step (num_iter <= 0)
   SL_DONE = 5,       // queue exhausted
+  SL_WAIT = 6,       // holds a queue position whose pixel has not arrived yet
+                     // (S.pix = the position; InvertArgs::avail)
 };
 
 // Per-slot scalars, stored [SC_COUNT][W].
@@ -99,6 +101,10 @@ struct InvertArgs {
   long long first_pixel;
   const double *init_par;      // [npix][9] learned starting parameters (an extra first
                                // run, run -1), or null for the reference's schedule
+  // queue positions below *avail can be taken (their profiles, and with a
+  // learned start their guesses and order, are on the device); the host
+  // raises it while it copies the map in.  null: the whole queue is there.
+  const unsigned long long *avail;
 };
 
 // Plan constants from a control file and a wavelength grid (me_api.cu);
@@ -153,14 +159,16 @@ cudaError_t launch_init_guess(const DevPlan &P, const double *d_prof, long long 
                               double *d_guess, double *d_extra, int *d_status, cudaStream_t st);
 // Queue order of a learned start: pixels by descending misfit of their run -1
 // parameters (kOrderBuckets quarter-octave buckets of chi^2, stable), into
-// d_order [npix].  d_key: npix bytes; d_hist: kOrderBuckets * kOrderBlocks ints.
+// d_order [npix] as base + the index into d_prof.  d_key: npix bytes; d_hist:
+// kOrderBuckets * kOrderBlocks ints.
 constexpr int kOrderBuckets = 128;
 constexpr int kOrderBlocks = 1024;
 cudaError_t launch_start_order(int precision, const DevPlan &P, const double *d_prof,
                                const double *d_init, long long npix, unsigned char *d_key,
-                               int *d_hist, long long *d_order, cudaStream_t st);
+                               int *d_hist, long long *d_order, cudaStream_t st,
+                               long long base = 0);
 // the stable counting sort alone (keys < kOrderBuckets)
 cudaError_t launch_order_by_key(const unsigned char *d_key, long long n, int *d_hist,
-                                long long *d_order, cudaStream_t st);
+                                long long *d_order, cudaStream_t st, long long base = 0);
 
 }  // namespace me

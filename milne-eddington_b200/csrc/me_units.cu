@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(1024) order_scan_kernel(int *hist, int m) {
 
 __global__ void __launch_bounds__(256) order_scatter_kernel(const unsigned char *key, long long n,
                                                             long long chunk, const int *offs,
-                                                            long long *order) {
+                                                            long long *order, long long first) {
   __shared__ int base[kOrderBuckets];
   __shared__ int wcnt[8][kOrderBuckets];
   for (int t = threadIdx.x; t < kOrderBuckets; t += blockDim.x) {
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(const unsigned char 
     if (in) {
       int pos = base[k] + rank;
       for (int w = 0; w < warp; w++) pos += wcnt[w][k];
-      order[pos] = i;
+      order[pos] = first + i;
     }
     __syncthreads();
     if (in && leader) {
@@ -378,19 +378,20 @@ cudaError_t launch_svd(const double *d_a, long long nmat, int n, double *d_u, do
 }
 
 cudaError_t launch_order_by_key(const unsigned char *d_key, long long n, int *d_hist,
-                                long long *d_order, cudaStream_t st) {
+                                long long *d_order, cudaStream_t st, long long base) {
   if (n <= 0) return cudaSuccess;
   const long long chunk = n / kOrderBlocks + 1 > 1024 ? n / kOrderBlocks + 1 : 1024;
   const int nb = (int)((n + chunk - 1) / chunk);
   order_hist_kernel<<<nb, 256, 0, st>>>(d_key, n, chunk, d_hist);
   order_scan_kernel<<<1, 1024, 0, st>>>(d_hist, kOrderBuckets * nb);
-  order_scatter_kernel<<<nb, 256, 0, st>>>(d_key, n, chunk, d_hist, d_order);
+  order_scatter_kernel<<<nb, 256, 0, st>>>(d_key, n, chunk, d_hist, d_order, base);
   return cudaGetLastError();
 }
 
 cudaError_t launch_start_order(int precision, const DevPlan &P, const double *d_prof,
                                const double *d_init, long long npix, unsigned char *d_key,
-                               int *d_hist, long long *d_order, cudaStream_t st) {
+                               int *d_hist, long long *d_order, cudaStream_t st,
+                               long long base) {
   if (npix <= 0) return cudaSuccess;
   const int b = 128;
   const unsigned g = (unsigned)((npix + b - 1) / b);
@@ -407,7 +408,7 @@ cudaError_t launch_start_order(int precision, const DevPlan &P, const double *d_
     else
       start_misfit_kernel<float, false><<<g, b, 0, st>>>(P, d_prof, d_init, npix, stride, d_key);
   }
-  return launch_order_by_key(d_key, npix, d_hist, d_order, st);
+  return launch_order_by_key(d_key, npix, d_hist, d_order, st, base);
 }
 
 cudaError_t launch_init_guess(const DevPlan &P, const double *d_prof, long long npix,

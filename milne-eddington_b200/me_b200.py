@@ -144,7 +144,7 @@ EXPORTED = [
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
     "me_plan_svd_lanes", "me_plan_set_svd_lanes", "me_plan_set_graphs",
-    "me_plan_svd_registers", "me_plan_set_svd_registers",
+    "me_plan_svd_registers", "me_plan_set_svd_registers", "me_plan_set_feed",
     "me_plan_autotune", "me_plan_last_counters", "me_plan_set_overlap",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
@@ -272,6 +272,8 @@ def lib() -> ctypes.CDLL:
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
         L.me_plan_set_svd_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_svd_lanes.restype = None
+        L.me_plan_set_feed.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_feed.restype = None
         L.me_plan_svd_registers.argtypes = [ctypes.c_void_p]
         L.me_plan_set_svd_registers.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_svd_registers.restype = None
@@ -498,6 +500,11 @@ class Plan:
             ctypes.POINTER(ctypes.c_uint)), npix), "me_plan_last_counters")
         return out
 
+    def set_feed(self, on: bool = True):
+        """me_invert_batch from page-locked host memory: copy the map in chunks
+        and start inverting as they land (default on); off: copy it whole first."""
+        lib().me_plan_set_feed(self._h, int(bool(on)))
+
     def set_overlap(self, on: bool = True):
         """Later-trial SVDs on a second stream beside the Jacobian kernel (default on)."""
         lib().me_plan_set_overlap(self._h, int(bool(on)))
@@ -521,12 +528,18 @@ class Plan:
                "me_plan_set_initializer")
         self._init = init
 
-    def invert(self, prof: np.ndarray, want_fit: bool = False):
-        """me_invert_batch on host arrays: prof [npix][4][nl] -> res [npix][10] (+fit)."""
+    def invert(self, prof: np.ndarray, want_fit: bool = False, out: Optional[np.ndarray] = None):
+        """me_invert_batch on host arrays: prof [npix][4][nl] -> res [npix][10] (+fit).
+        out (optional): a C-contiguous float64 [npix][10] array for the results,
+        e.g. a view of pinned host memory."""
         prof = np.ascontiguousarray(prof, dtype=np.float64)
         npix = prof.shape[0]
         assert prof.shape[1:] == (4, self.nl)
-        res = np.zeros((npix, 10))
+        if out is not None:
+            assert out.shape == (npix, 10) and out.dtype == np.float64 and out.flags["C_CONTIGUOUS"]
+            res = out
+        else:
+            res = np.zeros((npix, 10))
         fit = np.zeros((npix, 4, self.nl)) if want_fit else None
         st = MeStats()
         _check(lib().me_invert_batch(self._h, _ptr(prof), npix, _ptr(res), _ptr(fit),
