@@ -205,12 +205,15 @@ void me_plan_set_max_group(me_plan *plan, int lanes);
  * or 8); more lanes cut the decomposition's latency, fewer keep more of them
  * in flight.  Default 1. */
 int me_plan_svd_lanes(const me_plan *plan);
-/* With all nine parameters free, the one-thread-per-pixel SVD solves keep
- * their 9x9 matrix in registers (default, 1) or in shared memory (0).  Same
- * operations in the same order; the register form has no shared-memory
- * round trips and interleaves the independent row and column updates. */
+/* With all nine parameters free, the SVD solves can keep their 9x9 matrix in
+ * registers, one thread per pixel: 0 = shared memory everywhere; 1 (default)
+ * = registers in the one-thread-per-pixel rounds; 2 = registers also in the
+ * lane-split rounds after the queue drains (in place of the lanes' shared
+ * SVD).  Same operations in the same order; the register form has no
+ * shared-memory round trips and interleaves the independent row and column
+ * updates. */
 int me_plan_svd_registers(const me_plan *plan);
-void me_plan_set_svd_registers(me_plan *plan, int on);
+void me_plan_set_svd_registers(me_plan *plan, int mode);
 /* The LM rounds between two checks of the queue go to the GPU as one CUDA
  * graph, captured once per batch for each lane-group size (default on; off:
  * one launch per kernel).  Profiling (me_plan_set_profiling) launches
@@ -247,18 +250,30 @@ void me_plan_set_tail_slots(me_plan *plan, int slots);
  * for skipped pixels.  npix at most the last batch's. */
 int me_plan_last_counters(const me_plan *plan, unsigned int *counters, long npix);
 
+/* Variant of the one-thread-per-pixel Jacobian and trial kernels: 0 (default)
+ * 128 pixels per CTA, the wavelength grid read through the L1 cache, the FP32
+ * Faddeeva (Alg-916) series terms 1 / (a^2 n^2 + y^2) from a per-synthesis
+ * table in shared memory; 1 = 64 and 2 = 256 pixels per CTA; 3 = the grid
+ * staged in shared memory per CTA; 4 = no table, each term's correctly
+ * rounded reciprocal computed where it is used.  All give the same results. */
+int me_plan_kernel_variant(const me_plan *plan);
+void me_plan_set_kernel_variant(me_plan *plan, int variant);
+
 /* Autotuner: times me_invert_batch_device on the caller's batch (device
  * profiles d_prof [npix][4][nl], ideally of the size and kind the plan will
  * invert) for candidate values of the plan's runtime knobs -- pixels in
  * flight (window), lanes per pixel after the queue drains (max_group), the
- * tail kernel's threshold (tail_slots), lanes per SVD (svd_lanes) -- one knob
- * at a time, keeping each improvement, and leaves the best setting on the
- * plan.  The carried LM chi^2 is restored afterwards.  out (may be NULL)
+ * tail kernel's threshold (tail_slots), lanes per SVD (svd_lanes), the
+ * kernel variant (pixels per CTA, grid staging, Faddeeva series reciprocals;
+ * me_plan_set_kernel_variant) and where the SVD keeps its matrix
+ * (me_plan_set_svd_registers) -- one knob at a time, keeping each
+ * improvement, and leaves the best setting on the plan.  The carried LM chi^2 is restored afterwards.  out (may be NULL)
  * receives the choice, its time and the number of timed runs. */
 typedef struct me_tune_result {
   int window, max_group, tail_slots, svd_lanes;
   double ms;    /* device time of the batch with the chosen setting */
   int trials;   /* batches timed */
+  int kernel_variant, svd_registers;  /* me_plan_set_kernel_variant / _svd_registers */
 } me_tune_result;
 int me_plan_autotune(me_plan *plan, const double *d_prof, long npix, void *stream,
                      me_tune_result *out);

@@ -209,6 +209,7 @@ int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P
   }
   if (P.npar == 0) return fail(ME_ERR_CONFIG, "all nine parameters are fixed");
   P.svd_regs = 1;
+  P.kvar = 0;
   P.ncut = nl / 5;
   const double c = 299792458.0;
   double t = (lambda[P.ncut] - lam0) * c / 1e3;  // the reference omits /lambda0 here
@@ -512,8 +513,12 @@ extern "C" void me_plan_set_graphs(me_plan *p, int on) {
 
 extern "C" int me_plan_svd_lanes(const me_plan *p) { return p ? p->svd_lanes : 0; }
 extern "C" int me_plan_svd_registers(const me_plan *p) { return p ? p->P.svd_regs : 0; }
-extern "C" void me_plan_set_svd_registers(me_plan *p, int on) {
-  if (p) p->P.svd_regs = on ? 1 : 0;
+extern "C" int me_plan_kernel_variant(const me_plan *p) { return p ? p->P.kvar : 0; }
+extern "C" void me_plan_set_kernel_variant(me_plan *p, int v) {
+  if (p) p->P.kvar = (v >= 0 && v < me::kKernelVariants) ? v : 0;
+}
+extern "C" void me_plan_set_svd_registers(me_plan *p, int mode) {
+  if (p) p->P.svd_regs = mode <= 0 ? 0 : (mode >= 2 ? 2 : 1);
 }
 extern "C" void me_plan_set_svd_lanes(me_plan *p, int lanes) {
   if (p) p->svd_lanes = lanes >= 8 ? 8 : lanes >= 4 ? 4 : lanes >= 2 ? 2 : 1;
@@ -1387,6 +1392,12 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
        {0, p->grid_fin * (me::kBlock / 32) / 4, -1, p->grid_fin * (me::kBlock / 32),
         p->grid_fin * (me::kBlock / 32) * 2}},
       {&p->svd_lanes, {1, 2}},
+      // the Jacobian / trial kernels' variant: 64, 128 or 256 pixels per CTA,
+      // the wavelength grid staged in shared memory, no reciprocal table
+      {&p->P.kvar, {0, 1, 2, 3, 4}},
+      // the 9x9 SVD in registers in the full rounds (default), also in the
+      // lane-split rounds, or in shared memory throughout
+      {&p->P.svd_regs, {1, 2, 0}},
   };
   for (Knob &k : knobs) {
     if (rc) break;
@@ -1417,6 +1428,8 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
     out->svd_lanes = p->svd_lanes;
     out->ms = best;
     out->trials = trials;
+    out->kernel_variant = p->P.kvar;
+    out->svd_registers = p->P.svd_regs;
   }
   return ME_OK;
 }

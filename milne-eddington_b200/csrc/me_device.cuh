@@ -38,8 +38,12 @@ struct DevPlan {
   int niter, nruns, hmi_ref, regul_any;
   int fixed[9], regul[9];
   int free_idx[9];  // reduced index -> full parameter index
-  // SVD solves of the one-thread-per-slot rounds with all nine parameters
-  // free: 1 = matrix in registers (svd9_kernel), 0 = in shared memory
+  // variant of the one-thread-per-slot Jacobian and trial kernels (pixels
+  // per CTA, grid staging, reciprocal table; me_kernels.h kKernelVariants)
+  int kvar;
+  // SVD solves with all nine parameters free: 0 = matrix in shared memory,
+  // 1 = in registers (svd9_kernel) in the one-thread-per-slot rounds, 2 = in
+  // registers in the lane-split rounds as well
   int svd_regs;
   double lambda0, bshift;
   double limits[9][2];
@@ -310,8 +314,11 @@ __device__ __forceinline__ HL<float> voigt_alg916_f32(float nu, float y, float e
   const float ie2b = __fdividef(1.f, e2b);
   const float e1f = K.ema2 * e1b * ie2b;
   const float e2f = K.em2a2 * ie2b;
+  // 1 / (a^2 n^2 + y^2): from the per-synthesis table, or (no table) the
+  // same correctly rounded reciprocal computed in place
   auto rd = [&](int n) {
-    return n < kRden ? K.rden[n * K.rstride] : __fdividef(1.f, K.aa * float(n * n) + K.yy);
+    if (n < kRden) return K.rden ? K.rden[n * K.rstride] : 1.f / (K.aa * float(n * n) + K.yy);
+    return __fdividef(1.f, K.aa * float(n * n) + K.yy);
   };
   float s1 = 0.f, s2s = 0.f, s3 = 0.f, s4 = 0.f, s5 = 0.f, ep = 1.f;
   for (int n = nf; n <= nf + nmaxf; n++) {
@@ -547,6 +554,9 @@ struct SynthCall {
   T shift_b, vshift;  // Zeeman and Doppler shifts
   T erfcx_y;
   T step[9];
+  // the observed (or, with a filter, sub-) wavelength grid staged in shared
+  // memory as shift_w reads it, or null: read through the L1 cache
+  const T *grid;
 };
 
 template <class T>
@@ -590,6 +600,21 @@ __device__ __forceinline__ void synth_setup(SynthCall<T> &c, const double *mp, c
   c.erfcx_y = erfcx_t<T>(c.p5);
 #pragma unroll
   for (int k = 0; k < 9; k++) c.step[k] = T(step[k]);
+  c.grid = nullptr;
+}
+
+// The grid values shift_w / shift_wf read, for staging: FP32 the offsets from
+// lambda0 converted to float, FP64 the wavelengths; entry i of the filter's
+// sub-grid when it has one.
+template <class T>
+__device__ __forceinline__ T grid_value(const DevPlan &P, int i);
+template <>
+__device__ __forceinline__ float grid_value<float>(const DevPlan &P, int i) {
+  return float(P.nsub > 1 ? P.fdlambda[i] : P.dlambda[i]);
+}
+template <>
+__device__ __forceinline__ double grid_value<double>(const DevPlan &P, int i) {
+  return P.nsub > 1 ? P.flambda[i] : P.lambda[i];
 }
 
 // Reduced wavelength of grid point iw.
@@ -598,12 +623,14 @@ __device__ __forceinline__ T shift_w(const SynthCall<T> &c, const DevPlan &P, in
 template <>
 __device__ __forceinline__ float shift_w<float>(const SynthCall<float> &c, const DevPlan &P,
                                                 int iw) {
-  return (1e3f * float(__ldg(P.dlambda + iw)) - c.vshift) * c.inv_p4;
+  const float d = c.grid ? c.grid[iw] : float(__ldg(P.dlambda + iw));
+  return (1e3f * d - c.vshift) * c.inv_p4;
 }
 template <>
 __device__ __forceinline__ double shift_w<double>(const SynthCall<double> &c, const DevPlan &P,
                                                   int iw) {
-  return 1e3 * __ldg(P.lambda + iw) / c.p4 + c.vshift;
+  const double l = c.grid ? c.grid[iw] : __ldg(P.lambda + iw);
+  return 1e3 * l / c.p4 + c.vshift;
 }
 
 // shift_w at sub-wavelength j of the instrument filter
@@ -612,12 +639,14 @@ __device__ __forceinline__ T shift_wf(const SynthCall<T> &c, const DevPlan &P, i
 template <>
 __device__ __forceinline__ float shift_wf<float>(const SynthCall<float> &c, const DevPlan &P,
                                                  int j) {
-  return (1e3f * float(__ldg(P.fdlambda + j)) - c.vshift) * c.inv_p4;
+  const float d = c.grid ? c.grid[j] : float(__ldg(P.fdlambda + j));
+  return (1e3f * d - c.vshift) * c.inv_p4;
 }
 template <>
 __device__ __forceinline__ double shift_wf<double>(const SynthCall<double> &c, const DevPlan &P,
                                                    int j) {
-  return 1e3 * __ldg(P.flambda + j) / c.p4 + c.vshift;
+  const double l = c.grid ? c.grid[j] : __ldg(P.flambda + j);
+  return 1e3 * l / c.p4 + c.vshift;
 }
 
 // One wavelength of Milne_Eddington_Single.  syn[4] = I, Q, U, V.  With

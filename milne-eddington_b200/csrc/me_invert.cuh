@@ -39,9 +39,10 @@ template <class T, bool FILT>
 __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                              const double *par, const double *step,
                                              const double *prof, const double sw[4], double *H45,
-                                             double *g9) {
+                                             double *g9, const T *sgrid = nullptr) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
+  c.grid = sgrid;
   voigt_prepare<T>(K, c.p5, rden, blockDim.x);
   T h[45], g[9];
 #pragma unroll
@@ -86,9 +87,10 @@ template <class T, bool FILT>
 __device__ __forceinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                             const double *par, const double *step,
                                             const double *prof, const double sw[4],
-                                            double *fit) {
+                                            double *fit, const T *sgrid = nullptr) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
+  c.grid = sgrid;
   voigt_prepare<T>(K, c.p5, rden, blockDim.x);
   const T ones[4] = {T(1), T(1), T(1), T(1)};
   double chi = 0.0;
@@ -660,15 +662,28 @@ using namespace detail;
 // ---------------------------------------------------------------------------
 // Synthesis with Jacobian + normal equations for the slots of jlist[parity].
 // ---------------------------------------------------------------------------
-template <class T, bool FILT>
-__global__ void __launch_bounds__(kBlock, ME_JAC_MINB) jac_kernel(const __grid_constant__ DevPlan P,
-                                                     const __grid_constant__ InvertArgs A,
-                                                     const __grid_constant__ Slots S, int parity) {
+// Kernel variants (pixels per CTA BLOCK, the grid staged in shared memory,
+// the reciprocal table): the same arithmetic, bit for bit.
+template <class T, bool STAGE>
+__device__ __forceinline__ const T *stage_grid(const DevPlan &P, T *s_grid) {
+  if (!STAGE) return nullptr;
+  const int m = P.nl * P.nsub;
+  if (m > kMaxStage) return nullptr;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) s_grid[i] = grid_value<T>(P, i);
+  return s_grid;  // (voigt_block_setup's barrier follows)
+}
+
+template <class T, bool FILT, int BLOCK, bool STAGE, bool TABLE>
+__global__ void __launch_bounds__(BLOCK, ME_JAC_MINB * kBlock / BLOCK)
+    jac_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ InvertArgs A,
+               const __grid_constant__ Slots S, int parity) {
   __shared__ T s_tab[100];
-  __shared__ T s_rden[kRden * kBlock];
+  __shared__ T s_rden[TABLE ? kRden * BLOCK : 1];
+  __shared__ T s_grid[STAGE ? kMaxStage : 1];
+  const T *sgrid = stage_grid<T, STAGE>(P, s_grid);
   VoigtK<T> K;
   voigt_block_setup<T>(K, P, s_tab);
-  T *rden = s_rden + threadIdx.x;
+  T *rden = TABLE ? s_rden + threadIdx.x : nullptr;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     S.jcount[parity ^ 1] = 0;
     S.rcount[parity ^ 1] = 0;
@@ -684,7 +699,7 @@ __global__ void __launch_bounds__(kBlock, ME_JAC_MINB) jac_kernel(const __grid_c
     load9(S.par, W, s, par);
     slot_weights(P, S, s, step, sw);
     double H45[45], g9[9];
-    const double chi0 = deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9);
+    const double chi0 = deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9, sgrid);
     t.jac++;
     jac_store(P, S, s, par, chi0, H45, g9);
   }
@@ -741,16 +756,18 @@ static __global__ void __launch_bounds__(kSvdBlock) svd9_kernel(const __grid_con
 // ---------------------------------------------------------------------------
 // One trial step for every slot; run and pixel transitions; refills.
 // ---------------------------------------------------------------------------
-template <class T, bool FILT>
-__global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ DevPlan P,
-                                                       const __grid_constant__ InvertArgs A,
-                                                       const __grid_constant__ Slots S,
-                                                       int parity) {
+template <class T, bool FILT, int BLOCK, bool STAGE, bool TABLE>
+__global__ void __launch_bounds__(BLOCK) trial_kernel(const __grid_constant__ DevPlan P,
+                                                      const __grid_constant__ InvertArgs A,
+                                                      const __grid_constant__ Slots S,
+                                                      int parity) {
   __shared__ T s_tab[100];
-  __shared__ T s_rden[kRden * kBlock];
+  __shared__ T s_rden[TABLE ? kRden * BLOCK : 1];
+  __shared__ T s_grid[STAGE ? kMaxStage : 1];
+  const T *sgrid = stage_grid<T, STAGE>(P, s_grid);
   VoigtK<T> K;
   voigt_block_setup<T>(K, P, s_tab);
-  T *rden = s_rden + threadIdx.x;
+  T *rden = TABLE ? s_rden + threadIdx.x : nullptr;
   const int W = S.W;
   const int nl = P.nl;
   const int next_parity = parity ^ 1;
@@ -775,7 +792,7 @@ __global__ void __launch_bounds__(kBlock) trial_kernel(const __grid_constant__ D
       load9(S.ptmp, W, s, ptmp);
       slot_weights(P, S, s, step, sw);
       chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl, sw,
-                                nullptr);
+                                      nullptr, sgrid);
     }
     trial_transition<true>(P, A, S, s, st, chi_new, next_parity, t);
   }
@@ -1198,9 +1215,11 @@ int round_grid_impl(int which, int device) {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (which == 0) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jac_kernel<T, FILT>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jac_kernel<T, FILT, kBlock, false, true>,
+                                                  kBlock, 0);
   } else if (which == 1) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trial_kernel<T, FILT>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, trial_kernel<T, FILT, kBlock, false, true>, kBlock, 0);
   } else if (which == 3) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finish_kernel<T, FILT>, kBlock, 0);
   } else {
@@ -1236,6 +1255,35 @@ static inline void launch_svd_lanes(int lanes, const DevPlan &P, const InvertArg
   }
 }
 
+// The Jacobian / trial kernel of the plan's variant (P.kvar, kKernelVariants):
+// `grid` CTAs of kBlock threads, or as many threads in CTAs of another size.
+template <class T, bool FILT>
+void launch_jac_variant(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
+                        int grid, cudaStream_t st) {
+  switch (P.kvar) {
+    case 1: jac_kernel<T, FILT, 64, false, true><<<grid * 2, 64, 0, st>>>(P, A, S, parity); break;
+    case 2:
+      jac_kernel<T, FILT, 256, false, true><<<(grid + 1) / 2, 256, 0, st>>>(P, A, S, parity);
+      break;
+    case 3: jac_kernel<T, FILT, kBlock, true, true><<<grid, kBlock, 0, st>>>(P, A, S, parity); break;
+    case 4: jac_kernel<T, FILT, kBlock, false, false><<<grid, kBlock, 0, st>>>(P, A, S, parity); break;
+    default: jac_kernel<T, FILT, kBlock, false, true><<<grid, kBlock, 0, st>>>(P, A, S, parity);
+  }
+}
+template <class T, bool FILT>
+void launch_trial_variant(const DevPlan &P, const InvertArgs &A, const Slots &S, int parity,
+                          int grid, cudaStream_t st) {
+  switch (P.kvar) {
+    case 1: trial_kernel<T, FILT, 64, false, true><<<grid * 2, 64, 0, st>>>(P, A, S, parity); break;
+    case 2:
+      trial_kernel<T, FILT, 256, false, true><<<(grid + 1) / 2, 256, 0, st>>>(P, A, S, parity);
+      break;
+    case 3: trial_kernel<T, FILT, kBlock, true, true><<<grid, kBlock, 0, st>>>(P, A, S, parity); break;
+    case 4: trial_kernel<T, FILT, kBlock, false, false><<<grid, kBlock, 0, st>>>(P, A, S, parity); break;
+    default: trial_kernel<T, FILT, kBlock, false, true><<<grid, kBlock, 0, st>>>(P, A, S, parity);
+  }
+}
+
 // grids: jac_kernel, trial_kernel, svd; svd_lanes: lanes per matrix of the
 // SVD launches (1: svd_kernel, one thread each; 2, 4, 8: svd_grp_kernel).
 template <class T, bool FILT>
@@ -1249,7 +1297,7 @@ cudaError_t launch_round_impl(const DevPlan &P, const InvertArgs &A, const Slots
     cudaEventRecord(ov->join, ov->aux);
   }
   if (ev) cudaEventRecord(ev[0], st);
-  jac_kernel<T, FILT><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
+  launch_jac_variant<T, FILT>(P, A, S, parity, grids[0], st);
   if (ev) cudaEventRecord(ev[1], st);
   launch_svd_lanes(svd_lanes, P, A, S, parity, 0, grids[2], st);
   if (ev) cudaEventRecord(ev[2], st);
@@ -1258,9 +1306,22 @@ cudaError_t launch_round_impl(const DevPlan &P, const InvertArgs &A, const Slots
   else
     launch_svd_lanes(svd_lanes, P, A, S, parity, 1, grids[2], st);
   if (ev) cudaEventRecord(ev[3], st);
-  trial_kernel<T, FILT><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
+  launch_trial_variant<T, FILT>(P, A, S, parity, grids[1], st);
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
+}
+
+// The SVD launches of a lane-split round: G lanes per matrix in shared memory
+// (svd_grp_kernel), or, with P.svd_regs == 2 and all nine parameters free,
+// one thread per matrix in registers (svd9_kernel; the grid of G-lane groups
+// has at least one thread per slot).
+template <int G>
+static inline void launch_svd_grp(const DevPlan &P, const InvertArgs &A, const Slots &S,
+                                  int parity, int which, int grid, cudaStream_t st) {
+  if (P.npar == 9 && P.svd_regs == 2)
+    svd9_kernel<<<grid * (kBlock / kSvdBlock), kSvdBlock, 0, st>>>(P, A, S, parity, which);
+  else
+    svd_grp_kernel<G><<<grid, kBlock, 0, st>>>(P, A, S, parity, which);
 }
 
 template <class T, int G, bool FILT>
@@ -1269,18 +1330,18 @@ void launch_grp(const DevPlan &P, const InvertArgs &A, const Slots &S, int parit
   if (ov) {
     cudaEventRecord(ov->fork, st);
     cudaStreamWaitEvent(ov->aux, ov->fork, 0);
-    svd_grp_kernel<G><<<grids[2], kBlock, 0, ov->aux>>>(P, A, S, parity, 1);
+    launch_svd_grp<G>(P, A, S, parity, 1, grids[2], ov->aux);
     cudaEventRecord(ov->join, ov->aux);
   }
   if (ev) cudaEventRecord(ev[0], st);
   jac_grp_kernel<T, G, FILT><<<grids[0], kBlock, 0, st>>>(P, A, S, parity);
   if (ev) cudaEventRecord(ev[1], st);
-  svd_grp_kernel<G><<<grids[2], kBlock, 0, st>>>(P, A, S, parity, 0);
+  launch_svd_grp<G>(P, A, S, parity, 0, grids[2], st);
   if (ev) cudaEventRecord(ev[2], st);
   if (ov)
     cudaStreamWaitEvent(st, ov->join, 0);
   else
-    svd_grp_kernel<G><<<grids[2], kBlock, 0, st>>>(P, A, S, parity, 1);
+    launch_svd_grp<G>(P, A, S, parity, 1, grids[2], st);
   if (ev) cudaEventRecord(ev[3], st);
   trial_grp_kernel<T, G, FILT><<<grids[1], kBlock, 0, st>>>(P, A, S, parity);
   if (ev) cudaEventRecord(ev[4], st);

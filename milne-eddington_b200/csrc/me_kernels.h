@@ -15,6 +15,16 @@ constexpr int kBlock = 128;
 #define ME_JAC_MINB 2
 #endif
 constexpr int kSvdBlock = 64;  // threads of svd_kernel; each holds its matrix in shared memory
+// Variants of the one-thread-per-slot Jacobian and trial kernels, chosen per
+// plan (DevPlan::kvar, me_plan_set_kernel_variant, the autotuner):
+//   0  128 pixels per CTA, grid through the L1 cache, FP32 reciprocal table
+//   1   64 pixels per CTA     2  256 pixels per CTA
+//   3  the wavelength grid staged in shared memory (up to kMaxStage points)
+//   4  no reciprocal table: each Alg-916 series term's correctly rounded
+//      reciprocal computed in place (the table holds the same values)
+// All give the same arithmetic.
+constexpr int kKernelVariants = 5;
+constexpr int kMaxStage = 1024;
 constexpr int kSvdSmem = (81 + 18) * kSvdBlock * 8;
 // learned initialiser inference: rows per chunk, kernel launches per chunk
 constexpr int kMlpPredChunk = 65536;

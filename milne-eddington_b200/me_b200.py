@@ -145,6 +145,7 @@ EXPORTED = [
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
     "me_plan_svd_lanes", "me_plan_set_svd_lanes", "me_plan_set_graphs",
     "me_plan_svd_registers", "me_plan_set_svd_registers", "me_plan_set_feed",
+    "me_plan_kernel_variant", "me_plan_set_kernel_variant",
     "me_plan_autotune", "me_plan_last_counters", "me_plan_set_overlap",
     "me_mlp_train_params_default", "me_mlp_train", "me_mlp_destroy", "me_mlp_save",
     "me_mlp_load", "me_mlp_predict", "me_mlp_predict_device", "me_plan_set_initializer",
@@ -159,7 +160,8 @@ EXPORTED = [
 class MeTuneResult(ctypes.Structure):
     _fields_ = [("window", ctypes.c_int), ("max_group", ctypes.c_int),
                 ("tail_slots", ctypes.c_int), ("svd_lanes", ctypes.c_int),
-                ("ms", ctypes.c_double), ("trials", ctypes.c_int)]
+                ("ms", ctypes.c_double), ("trials", ctypes.c_int),
+                ("kernel_variant", ctypes.c_int), ("svd_registers", ctypes.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -272,6 +274,9 @@ def lib() -> ctypes.CDLL:
         L.me_plan_svd_lanes.argtypes = [ctypes.c_void_p]
         L.me_plan_set_svd_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_svd_lanes.restype = None
+        L.me_plan_kernel_variant.argtypes = [ctypes.c_void_p]
+        L.me_plan_set_kernel_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_kernel_variant.restype = None
         L.me_plan_set_feed.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_feed.restype = None
         L.me_plan_svd_registers.argtypes = [ctypes.c_void_p]
@@ -468,13 +473,14 @@ class Plan:
         lib().me_plan_set_svd_lanes(self._h, int(lanes))
 
     @property
-    def svd_registers(self) -> bool:
-        """SVD solves with the 9x9 matrix in registers (all nine parameters free)."""
-        return bool(lib().me_plan_svd_registers(self._h))
+    def svd_registers(self) -> int:
+        """SVD solves with the 9x9 matrix in registers (all nine parameters free):
+        0 shared memory, 1 registers in the full rounds, 2 also after the drain."""
+        return lib().me_plan_svd_registers(self._h)
 
     @svd_registers.setter
-    def svd_registers(self, on: bool):
-        lib().me_plan_set_svd_registers(self._h, int(bool(on)))
+    def svd_registers(self, mode: int):
+        lib().me_plan_set_svd_registers(self._h, int(mode))
 
     def set_filter(self, offsets_mA, weights):
         """Instrument filter: offsets [mA] and weights of each observed wavelength's
@@ -499,6 +505,16 @@ class Plan:
         _check(lib().me_plan_last_counters(self._h, out.ctypes.data_as(
             ctypes.POINTER(ctypes.c_uint)), npix), "me_plan_last_counters")
         return out
+
+    @property
+    def kernel_variant(self) -> int:
+        """Jacobian / trial kernel variant: 0 default, 1 / 2 = 64 / 256 pixels per
+        CTA, 3 = grid staged in shared memory, 4 = no Faddeeva reciprocal table."""
+        return lib().me_plan_kernel_variant(self._h)
+
+    @kernel_variant.setter
+    def kernel_variant(self, v: int):
+        lib().me_plan_set_kernel_variant(self._h, int(v))
 
     def set_feed(self, on: bool = True):
         """me_invert_batch from page-locked host memory: copy the map in chunks

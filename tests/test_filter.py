@@ -144,6 +144,23 @@ def test_filtered_inversion_parity_vs_oracle(filt_map, prec):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["FP64", "FP32"])
+def test_filtered_kernel_variants_agree(filt_map, prec):
+    """The sub-wavelength grid (6 x 21 points) staged in shared memory, and
+    the other kernel variants, give the default variant's results."""
+    m = filt_map
+    out = {}
+    with me_b200.Plan(cfg_of(prec, m["extra"]), m["lam"]) as plan:
+        plan.max_group, plan.tail_slots = 1, 0
+        for v in (0, 3, 4, 1):
+            plan.kernel_variant = v
+            plan.carry_chisq = 0.0
+            out[v], _ = plan.invert(m["prof"])
+    for v in (3, 4, 1):
+        assert np.mean(np.all(out[v] == out[0], axis=1)) >= 0.99, v
+
+
+@pytest.mark.gpu
 def test_learned_start_with_queue_order_on_the_filtered_grid():
     """The learned start on the filtered grid, queue order on and off (the
     start-misfit kernel's filtered variant): the same pixels inverted, chi^2

@@ -71,11 +71,13 @@ def cfg0_map():
     return dict(name=name, lam=lam, prof=prof, base=base, self=agreement(pert, base))
 
 
-# (max_group, tail_slots, svd_lanes): one thread per pixel throughout;
-# lane-split rounds once the queue is empty, with 4 lanes per SVD in the full
-# rounds; the warp-per-pixel tail kernel (for a batch this small the last two
-# run most of the LM steps)
-MODES = {"threads": (1, 0, 1), "lane_split": (32, 0, 4), "tail_kernel": (1, -1, 1)}
+# (max_group, tail_slots, svd_lanes, svd_registers): one thread per pixel
+# throughout; lane-split rounds once the queue is empty, with 4 lanes per SVD
+# in the full rounds; the same with the register SVD in the lane-split
+# rounds; the warp-per-pixel tail kernel (for a batch this small the last
+# three run most of the LM steps)
+MODES = {"threads": (1, 0, 1, 1), "lane_split": (32, 0, 4, 1),
+         "lane_split_svd_regs": (32, 0, 1, 2), "tail_kernel": (1, -1, 1, 1)}
 
 
 @pytest.mark.parametrize("mode", list(MODES))
@@ -84,7 +86,7 @@ def test_inversion_parity_vs_oracle(cfg0_map, prec, mode):
     m = cfg0_map
     cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
     with me_b200.Plan(cfg, m["lam"]) as plan:
-        plan.max_group, plan.tail_slots, plan.svd_lanes = MODES[mode]
+        plan.max_group, plan.tail_slots, plan.svd_lanes, plan.svd_registers = MODES[mode]
         res, stats = invert_chunks(plan, m["prof"])
     for st in stats:
         tail_launches = st["launches"] - 4 * st["rounds"]
@@ -115,18 +117,40 @@ def test_svd_registers_vs_shared_memory(cfg0_map, prec):
     m = cfg0_map
     cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
     out = {}
-    for regs in (True, False):
+    for regs in (1, 0):
         with me_b200.Plan(cfg, m["lam"]) as plan:
             plan.max_group, plan.tail_slots, plan.svd_lanes = 1, 0, 1
             plan.svd_registers = regs
             assert plan.svd_registers == regs
             out[regs], _ = invert_chunks(plan, m["prof"])
-    same = np.mean(np.all(out[True] == out[False], axis=1))
-    _, within, med = agreement(out[True], m["base"])
+    same = np.mean(np.all(out[1] == out[0], axis=1))
+    _, within, med = agreement(out[1], m["base"])
     print(f"{prec}: registers vs shared memory bitwise identical {same:.4f}; "
           f"vs oracle within 1.05 {within:.3f}, median ratio {med:.6f}")
     assert same >= 0.95
     assert abs(med - 1) < 1e-3 and within >= m["self"][1] - 0.02
+
+
+@pytest.mark.parametrize("prec", ["FP32", "FP64"])
+def test_kernel_variants_agree(cfg0_map, prec):
+    """The autotuner's Jacobian / trial kernel variants (64 / 128 / 256 pixels
+    per CTA, the grid staged in shared memory, no Faddeeva reciprocal table)
+    run the same arithmetic: the same results, pixel for pixel."""
+    m = cfg0_map
+    cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
+    prof = m["prof"][:4096]
+    out = {}
+    with me_b200.Plan(cfg, m["lam"]) as plan:
+        plan.max_group, plan.tail_slots = 1, 0
+        for v in range(5):
+            plan.kernel_variant = v
+            assert plan.kernel_variant == v
+            plan.carry_chisq = 0.0
+            out[v], _ = plan.invert(prof)
+    for v in range(1, 5):
+        same = np.mean(np.all(out[v] == out[0], axis=1))
+        print(f"{prec} variant {v}: identical to variant 0 for {same:.4f}")
+        assert same >= 0.99, v
 
 
 def test_restarts_counter_rng_vs_oracle():
