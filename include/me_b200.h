@@ -255,7 +255,9 @@ int me_plan_last_counters(const me_plan *plan, unsigned int *counters, long npix
  * Faddeeva (Alg-916) series terms 1 / (a^2 n^2 + y^2) from a per-synthesis
  * table in shared memory; 1 = 64 and 2 = 256 pixels per CTA; 3 = the grid
  * staged in shared memory per CTA; 4 = no table, each term's correctly
- * rounded reciprocal computed where it is used.  All give the same results. */
+ * rounded reciprocal computed where it is used; 5 = the Jacobian kernel's
+ * normal-equation sums in shared memory, 3 CTAs of 128 per SM (FP32 plans;
+ * FP64 plans run 0).  All give the same results. */
 int me_plan_kernel_variant(const me_plan *plan);
 void me_plan_set_kernel_variant(me_plan *plan, int variant);
 

@@ -1393,8 +1393,9 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
         p->grid_fin * (me::kBlock / 32) * 2}},
       {&p->svd_lanes, {1, 2}},
       // the Jacobian / trial kernels' variant: 64, 128 or 256 pixels per CTA,
-      // the wavelength grid staged in shared memory, no reciprocal table
-      {&p->P.kvar, {0, 1, 2, 3, 4}},
+      // the wavelength grid staged in shared memory, no reciprocal table, the
+      // normal-equation sums in shared memory
+      {&p->P.kvar, {0, 1, 2, 3, 4, 5}},
       // the 9x9 SVD in registers in the full rounds (default), also in the
       // lane-split rounds, or in shared memory throughout
       {&p->P.svd_regs, {1, 2, 0}},

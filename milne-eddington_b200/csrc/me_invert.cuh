@@ -81,6 +81,55 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *
   return chi / (4.0 * nl);
 }
 
+// deriv_pass with the 45 + 9 sums of the normal equations in shared memory
+// (acc[k * BLOCK], this thread's column) instead of registers: the same
+// additions in the same order, fewer live registers across the wavelength
+// loop (the kernel then fits more CTAs per SM).
+template <class T, bool FILT, int BLOCK>
+__device__ __forceinline__ double deriv_pass_sacc(const DevPlan &P, VoigtK<T> &K, T *rden,
+                                                  const double *par, const double *step,
+                                                  const double *prof, const double sw[4],
+                                                  double *H45, double *g9, const T *sgrid,
+                                                  T *acc) {
+  SynthCall<T> c;
+  synth_setup<T>(c, par, P, step);
+  c.grid = sgrid;
+  voigt_prepare<T>(K, c.p5, rden, blockDim.x);
+#pragma unroll
+  for (int i = 0; i < 54; i++) acc[i * BLOCK] = T(0);
+  double chi = 0.0;
+  const int nl = P.nl;
+  const T tsw[4] = {T(sw[0]), T(sw[1]), T(sw[2]), T(sw[3])};
+#pragma unroll 1
+  for (int iw = 0; iw < nl; iw++) {
+    T syn[4], J[4][9];
+    channel_point<T, true, FILT>(c, P, K, tsw, iw, syn, J);
+    T r[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+      chi += rd * rd;
+      r[s] = T(rd);
+    }
+    int idx = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+#pragma unroll
+      for (int j = i; j < 9; j++) {
+        acc[idx * BLOCK] += J[0][i] * J[0][j] + J[1][i] * J[1][j] + J[2][i] * J[2][j] +
+                            J[3][i] * J[3][j];
+        idx++;
+      }
+      acc[(45 + i) * BLOCK] -= J[0][i] * r[0] + J[1][i] * r[1] + J[2][i] * r[2] + J[3][i] * r[3];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 45; i++) H45[i] = (double)acc[i * BLOCK];
+#pragma unroll
+  for (int i = 0; i < 9; i++) g9[i] = (double)acc[(45 + i) * BLOCK];
+  return chi / (4.0 * nl);
+}
+
 // Forward synthesis + chi^2 (Trial_Synthesis's synthesis and Loss_Function);
 // residuals and their squares in FP64.  fit (nullable) receives the profile.
 template <class T, bool FILT>
@@ -673,13 +722,16 @@ __device__ __forceinline__ const T *stage_grid(const DevPlan &P, T *s_grid) {
   return s_grid;  // (voigt_block_setup's barrier follows)
 }
 
-template <class T, bool FILT, int BLOCK, bool STAGE, bool TABLE>
-__global__ void __launch_bounds__(BLOCK, ME_JAC_MINB * kBlock / BLOCK)
+// SACC: the normal-equation sums in shared memory (deriv_pass_sacc), compiled
+// for 3 CTAs of 128 per SM instead of 2
+template <class T, bool FILT, int BLOCK, bool STAGE, bool TABLE, bool SACC = false>
+__global__ void __launch_bounds__(BLOCK, SACC ? 3 : ME_JAC_MINB * kBlock / BLOCK)
     jac_kernel(const __grid_constant__ DevPlan P, const __grid_constant__ InvertArgs A,
                const __grid_constant__ Slots S, int parity) {
   __shared__ T s_tab[100];
   __shared__ T s_rden[TABLE ? kRden * BLOCK : 1];
   __shared__ T s_grid[STAGE ? kMaxStage : 1];
+  __shared__ T s_acc[SACC ? 54 * BLOCK : 1];
   const T *sgrid = stage_grid<T, STAGE>(P, s_grid);
   VoigtK<T> K;
   voigt_block_setup<T>(K, P, s_tab);
@@ -699,7 +751,10 @@ __global__ void __launch_bounds__(BLOCK, ME_JAC_MINB * kBlock / BLOCK)
     load9(S.par, W, s, par);
     slot_weights(P, S, s, step, sw);
     double H45[45], g9[9];
-    const double chi0 = deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9, sgrid);
+    const double chi0 =
+        SACC ? deriv_pass_sacc<T, FILT, BLOCK>(P, K, rden, par, step, pp, sw, H45, g9, sgrid,
+                                               s_acc + threadIdx.x)
+             : deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9, sgrid);
     t.jac++;
     jac_store(P, S, s, par, chi0, H45, g9);
   }
@@ -1267,6 +1322,14 @@ void launch_jac_variant(const DevPlan &P, const InvertArgs &A, const Slots &S, i
       break;
     case 3: jac_kernel<T, FILT, kBlock, true, true><<<grid, kBlock, 0, st>>>(P, A, S, parity); break;
     case 4: jac_kernel<T, FILT, kBlock, false, false><<<grid, kBlock, 0, st>>>(P, A, S, parity); break;
+    case 5:
+      // FP32 only (FP64 sums would not fit in a CTA's static shared memory)
+      if constexpr (sizeof(T) == sizeof(float)) {
+        jac_kernel<T, FILT, kBlock, false, true, true><<<grid * 3 / 2, kBlock, 0, st>>>(P, A, S,
+                                                                                     parity);
+        break;
+      }
+      [[fallthrough]];
     default: jac_kernel<T, FILT, kBlock, false, true><<<grid, kBlock, 0, st>>>(P, A, S, parity);
   }
 }

@@ -22,8 +22,11 @@ constexpr int kSvdBlock = 64;  // threads of svd_kernel; each holds its matrix i
 //   3  the wavelength grid staged in shared memory (up to kMaxStage points)
 //   4  no reciprocal table: each Alg-916 series term's correctly rounded
 //      reciprocal computed in place (the table holds the same values)
+//   5  the Jacobian kernel's normal-equation sums in shared memory, 3 CTAs
+//      of 128 per SM (the trial kernel as 0; FP32 synthesis only, FP64 plans
+//      run variant 0)
 // All give the same arithmetic.
-constexpr int kKernelVariants = 5;
+constexpr int kKernelVariants = 6;
 constexpr int kMaxStage = 1024;
 constexpr int kSvdSmem = (81 + 18) * kSvdBlock * 8;
 // learned initialiser inference: rows per chunk, kernel launches per chunk

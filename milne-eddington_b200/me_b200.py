@@ -509,7 +509,8 @@ class Plan:
     @property
     def kernel_variant(self) -> int:
         """Jacobian / trial kernel variant: 0 default, 1 / 2 = 64 / 256 pixels per
-        CTA, 3 = grid staged in shared memory, 4 = no Faddeeva reciprocal table."""
+        CTA, 3 = grid staged in shared memory, 4 = no Faddeeva reciprocal table,
+        5 = normal-equation sums in shared memory (FP32)."""
         return lib().me_plan_kernel_variant(self._h)
 
     @kernel_variant.setter

@@ -152,11 +152,11 @@ def test_filtered_kernel_variants_agree(filt_map, prec):
     out = {}
     with me_b200.Plan(cfg_of(prec, m["extra"]), m["lam"]) as plan:
         plan.max_group, plan.tail_slots = 1, 0
-        for v in (0, 3, 4, 1):
+        for v in (0, 3, 4, 1, 5):
             plan.kernel_variant = v
             plan.carry_chisq = 0.0
             out[v], _ = plan.invert(m["prof"])
-    for v in (3, 4, 1):
+    for v in (3, 4, 1, 5):
         assert np.mean(np.all(out[v] == out[0], axis=1)) >= 0.99, v
 
 

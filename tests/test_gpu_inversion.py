@@ -134,20 +134,21 @@ def test_svd_registers_vs_shared_memory(cfg0_map, prec):
 @pytest.mark.parametrize("prec", ["FP32", "FP64"])
 def test_kernel_variants_agree(cfg0_map, prec):
     """The autotuner's Jacobian / trial kernel variants (64 / 128 / 256 pixels
-    per CTA, the grid staged in shared memory, no Faddeeva reciprocal table)
-    run the same arithmetic: the same results, pixel for pixel."""
+    per CTA, the grid staged in shared memory, no Faddeeva reciprocal table,
+    the normal-equation sums in shared memory) run the same arithmetic: the
+    same results, pixel for pixel."""
     m = cfg0_map
     cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
     prof = m["prof"][:4096]
     out = {}
     with me_b200.Plan(cfg, m["lam"]) as plan:
         plan.max_group, plan.tail_slots = 1, 0
-        for v in range(5):
+        for v in range(6):
             plan.kernel_variant = v
             assert plan.kernel_variant == v
             plan.carry_chisq = 0.0
             out[v], _ = plan.invert(prof)
-    for v in range(1, 5):
+    for v in range(1, 6):
         same = np.mean(np.all(out[v] == out[0], axis=1))
         print(f"{prec} variant {v}: identical to variant 0 for {same:.4f}")
         assert same >= 0.99, v
