@@ -206,12 +206,13 @@ void me_plan_set_max_group(me_plan *plan, int lanes);
  * in flight.  Default 1. */
 int me_plan_svd_lanes(const me_plan *plan);
 /* With all nine parameters free, the SVD solves can keep their 9x9 matrix in
- * registers, one thread per pixel: 0 = shared memory everywhere; 1 (default)
- * = registers in the one-thread-per-pixel rounds; 2 = registers also in the
+ * registers, one thread per pixel: 0 (default) = shared memory everywhere;
+ * 1 = registers in the one-thread-per-pixel rounds; 2 = registers also in the
  * lane-split rounds after the queue drains (in place of the lanes' shared
- * SVD).  Same operations in the same order; the register form has no
- * shared-memory round trips and interleaves the independent row and column
- * updates. */
+ * SVD).  Same operations in the same order (results agree to rounding: the
+ * compiler fuses multiply-adds differently); the register form has no
+ * shared-memory round trips, the shared-memory form a smaller code.  Which is
+ * faster depends on the batch (me_plan_autotune tries them). */
 int me_plan_svd_registers(const me_plan *plan);
 void me_plan_set_svd_registers(me_plan *plan, int mode);
 /* The LM rounds between two checks of the queue go to the GPU as one CUDA
@@ -250,14 +251,15 @@ void me_plan_set_tail_slots(me_plan *plan, int slots);
  * for skipped pixels.  npix at most the last batch's. */
 int me_plan_last_counters(const me_plan *plan, unsigned int *counters, long npix);
 
-/* Variant of the one-thread-per-pixel Jacobian and trial kernels: 0 (default)
- * 128 pixels per CTA, the wavelength grid read through the L1 cache, the FP32
- * Faddeeva (Alg-916) series terms 1 / (a^2 n^2 + y^2) from a per-synthesis
- * table in shared memory; 1 = 64 and 2 = 256 pixels per CTA; 3 = the grid
+/* Variant of the one-thread-per-pixel Jacobian and trial kernels (default:
+ * 5 on FP32 plans, 0 on FP64 plans): 0 = 128 pixels per CTA, the wavelength
+ * grid read through the L1 cache, the FP32 Faddeeva (Alg-916) series terms
+ * 1 / (a^2 n^2 + y^2) from a per-synthesis table in shared memory; 1 = 64 and 2 = 256 pixels per CTA; 3 = the grid
  * staged in shared memory per CTA; 4 = no table, each term's correctly
  * rounded reciprocal computed where it is used; 5 = the Jacobian kernel's
  * normal-equation sums in shared memory, 3 CTAs of 128 per SM (FP32 plans;
- * FP64 plans run 0).  All give the same results. */
+ * FP64 plans run 0).  All run the same arithmetic; each variant is compiled
+ * on its own, so results agree to rounding. */
 int me_plan_kernel_variant(const me_plan *plan);
 void me_plan_set_kernel_variant(me_plan *plan, int variant);
 

@@ -208,8 +208,11 @@ int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P
     P.regul_weight[i] = cfg->regul_weight[i];
   }
   if (P.npar == 0) return fail(ME_ERR_CONFIG, "all nine parameters are fixed");
-  P.svd_regs = 1;
-  P.kvar = 0;
+  // measured defaults on a B200 (the autotuner may choose others): the
+  // shared-memory SVD; on the FP32 path the Jacobian kernel with its sums in
+  // shared memory
+  P.svd_regs = 0;
+  P.kvar = cfg->precision == ME_PREC_FP64 ? 0 : 5;
   P.ncut = nl / 5;
   const double c = 299792458.0;
   double t = (lambda[P.ncut] - lam0) * c / 1e3;  // the reference omits /lambda0 here
