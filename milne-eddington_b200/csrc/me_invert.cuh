@@ -163,6 +163,7 @@ __device__ __forceinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T
 // Get_Regul's penalty (Src/LM_FIT.c:354-396).
 __device__ __forceinline__ double penalty_of(const DevPlan &P, const double *par) {
   double pen = 0.0;
+#pragma unroll
   for (int i = 0; i < 9; i++) {
     if (P.fixed[i] || !P.regul[i]) continue;
     const double r = par[i] - P.regul_value[i];
@@ -311,6 +312,11 @@ __device__ __forceinline__ void slot_weights(const DevPlan &P, const Slots &S, i
 // normal matrix with Get_Regul's diagonal and gradient terms
 // (Hessian_Compute + Get_Regul, Src/LM_FIT.c:240-396), and the move to the
 // first trial (or the run's end when num_iter <= 0).  One thread per slot.
+// UNROLL: the loops below over all nine parameters with compile-time indices
+// (the sums stay in registers: the FP32 kernels); otherwise over the free
+// parameters through P.free_idx (the sums in local memory: the FP64 kernels,
+// whose 54 double sums would not fit in registers beside the loop state).
+template <bool UNROLL = false>
 __device__ __forceinline__ void jac_store(const DevPlan &P, const Slots &S, int s,
                                           const double *par, double chi0, const double *H45,
                                           const double *g9) {
@@ -331,20 +337,49 @@ __device__ __forceinline__ void jac_store(const DevPlan &P, const Slots &S, int 
       return;
     }
   }
-  double g[9];
-  for (int a = 0; a < n; a++) {
-    const int ia = P.free_idx[a];
-    for (int b = a; b < n; b++) {
-      const int ib = P.free_idx[b];
+  if constexpr (!UNROLL) {
+    double g[9];
+    for (int a = 0; a < n; a++) {
+      const int ia = P.free_idx[a];
+      for (int b = a; b < n; b++) {
+        const int ib = P.free_idx[b];
+        double h = H45[ia * 9 - ia * (ia + 1) / 2 + ib];
+        if (a == b && P.regul_any && P.regul[ia]) h += P.regul_weight[ia] * ratio;
+        S.hess[(size_t)(a * n + b) * W + s] = h;
+        S.hess[(size_t)(b * n + a) * W + s] = h;
+      }
+      g[a] = g9[ia];
+      if (P.regul_any && P.regul[ia])
+        g[a] -= (par[ia] - P.regul_value[ia]) * P.regul_weight[ia] * ratio;
+    }
+    for (int a = 0; a < n; a++) S.jvec[(size_t)a * W + s] = g[a];
+    S.cnt[1 * W + s]++;
+    S.sc[SC_DAMP * W + s] = P.damp;
+    S.tk[s] = 1;
+    S.state[s] = SL_TRIAL;
+    return;
+  }
+  // all nine parameters with compile-time indices into H45 / g9, skipping
+  // the fixed ones; a and b count the free parameters before ia and ib
+  int a = 0;
+#pragma unroll
+  for (int ia = 0; ia < 9; ia++) {
+    if (P.fixed[ia]) continue;
+    int b = a;
+#pragma unroll
+    for (int ib = ia; ib < 9; ib++) {
+      if (P.fixed[ib]) continue;
       double h = H45[ia * 9 - ia * (ia + 1) / 2 + ib];
-      if (a == b && P.regul_any && P.regul[ia]) h += P.regul_weight[ia] * ratio;
+      if (ib == ia && P.regul_any && P.regul[ia]) h += P.regul_weight[ia] * ratio;
       S.hess[(size_t)(a * n + b) * W + s] = h;
       S.hess[(size_t)(b * n + a) * W + s] = h;
+      b++;
     }
-    g[a] = g9[ia];
-    if (P.regul_any && P.regul[ia]) g[a] -= (par[ia] - P.regul_value[ia]) * P.regul_weight[ia] * ratio;
+    double gv = g9[ia];
+    if (P.regul_any && P.regul[ia]) gv -= (par[ia] - P.regul_value[ia]) * P.regul_weight[ia] * ratio;
+    S.jvec[(size_t)a * W + s] = gv;
+    a++;
   }
-  for (int a = 0; a < n; a++) S.jvec[(size_t)a * W + s] = g[a];
   S.cnt[1 * W + s]++;
   S.sc[SC_DAMP * W + s] = P.damp;
   S.tk[s] = 1;
@@ -756,7 +791,7 @@ __global__ void __launch_bounds__(BLOCK, SACC ? 3 : ME_JAC_MINB * kBlock / BLOCK
                                                s_acc + threadIdx.x)
              : deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9, sgrid);
     t.jac++;
-    jac_store(P, S, s, par, chi0, H45, g9);
+    jac_store<sizeof(T) == sizeof(float)>(P, S, s, par, chi0, H45, g9);
   }
   t.flush(A, S);
 }
