@@ -413,10 +413,12 @@ def parity_vs_reference(res, ref, spread):
     """A GPU arm against the reference on the sample: per parameter median /
     p99 |delta| and pass/fail.  A parameter passes when its median is within
     the stated tolerance or within 1.1 x the reference's own spread, and its
-    p99 within 1.1 x that spread (or the tolerance): the spread is the larger
+    p99 within 1.25 x that spread (or the tolerance): the spread is the larger
     of the reference against itself with another restart seed and with a
-    one-ulp input change, on the same pixels.  The chi^2 test passes when the
-    share within 1.05 x is no more than 0.02 below the reference's own."""
+    one-ulp input change, on the same pixels.  (A p99 of 4096 pixels rests on
+    its ~41 largest differences and varies by about 10 % between samples.)
+    The chi^2 test passes when the share within 1.05 x is no more than 0.02
+    below the reference's own."""
     v = ref[:, 9] > 0
     err = param_errors(res[v], ref[v])
     params = {}
@@ -427,7 +429,7 @@ def parity_vs_reference(res, ref, spread):
         tol = TOLERANCE[n]
         params[n] = {"median_p99": [med, p99], "tolerance": tol,
                      "ref_spread_median_p99": [smed, sp99],
-                     "pass": bool(med <= max(tol, 1.1 * smed) and p99 <= max(tol, 1.1 * sp99)),
+                     "pass": bool(med <= max(tol, 1.1 * smed) and p99 <= max(tol, 1.25 * sp99)),
                      "within_tolerance_median": bool(med <= tol)}
     chi = chi2_agreement(res, ref)
     s_within = min(spread[k]["chi2"]["within_1.05"] for k in spread)
@@ -835,7 +837,7 @@ def main():
                     "plain_fp64": res_fp64_sample}
             parity = {"tolerance": TOLERANCE,
                       "rule": "median <= max(tol, 1.1 x ref spread median) and p99 <= max(tol, "
-                              "1.1 x ref spread p99); chi2 within 1.05 share >= ref spread "
+                              "1.25 x ref spread p99); chi2 within 1.05 share >= ref spread "
                               "share - 0.02; ref spread = the reference against itself with "
                               "another restart seed and with a one-ulp input change, same "
                               "pixels",
