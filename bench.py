@@ -268,6 +268,12 @@ def parse():
                     help="comma list of further workloads measured after the headline "
                          "(N = 1 only; 'literal' = the headline map with the literal bounds); "
                          "empty: none")
+    ap.add_argument("--svd-registers", type=int, default=-1,
+                    help="me_plan_set_svd_registers for both arms after any autotuning "
+                         "(-1: leave the default / the autotuner's choice)")
+    ap.add_argument("--kernel-variant", type=int, default=-1,
+                    help="me_plan_set_kernel_variant for both arms after any autotuning "
+                         "(-1: leave the default / the autotuner's choice)")
     ap.add_argument("--other-budget-s", type=float, default=480.0,
                     help="wall-time budget of the further workloads; one that would start "
                          "past it is skipped")
@@ -705,6 +711,11 @@ def main():
     tuned, tuned_plain = None, None
     if args.autotune:
         tuned = plan.autotune(prof.data_ptr(), npix, stream.cuda_stream)
+    for pl in (plan, plain):
+        if args.svd_registers >= 0:
+            pl.svd_registers = args.svd_registers
+        if args.kernel_variant >= 0:
+            pl.kernel_variant = args.kernel_variant
 
     def step():
         return plan.invert_device(prof.data_ptr(), npix, res.data_ptr(), 0, stream.cuda_stream)
@@ -752,6 +763,10 @@ def main():
     if plain_steps > 0:
         if args.autotune:
             tuned_plain = plain.autotune(prof.data_ptr(), npix, stream.cuda_stream)
+            if args.svd_registers >= 0:
+                plain.svd_registers = args.svd_registers
+            if args.kernel_variant >= 0:
+                plain.kernel_variant = args.kernel_variant
         step_plain()  # warm-up (slot buffers, caches)
         nvtx.range_push("plain")
         el, pst = timed_steps(torch, step_plain, plain_steps, stream, dist)
