@@ -521,7 +521,7 @@ extern "C" void me_plan_set_kernel_variant(me_plan *p, int v) {
   if (p) p->P.kvar = (v >= 0 && v < me::kKernelVariants) ? v : 0;
 }
 extern "C" void me_plan_set_svd_registers(me_plan *p, int mode) {
-  if (p) p->P.svd_regs = mode <= 0 ? 0 : (mode >= 3 ? 3 : mode);
+  if (p) p->P.svd_regs = mode <= 0 ? 0 : (mode >= 2 ? 2 : 1);
 }
 extern "C" void me_plan_set_svd_lanes(me_plan *p, int lanes) {
   if (p) p->svd_lanes = lanes >= 8 ? 8 : lanes >= 4 ? 4 : lanes >= 2 ? 2 : 1;
@@ -1401,7 +1401,7 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
       {&p->P.kvar, {0, 1, 2, 3, 4, 5}},
       // the 9x9 SVD in registers in the full rounds (default), also in the
       // lane-split rounds, or in shared memory throughout
-      {&p->P.svd_regs, {1, 2, 3, 0}},
+      {&p->P.svd_regs, {1, 2, 0}},
   };
   for (Knob &k : knobs) {
     if (rc) break;

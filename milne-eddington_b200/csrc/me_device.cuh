@@ -43,8 +43,7 @@ struct DevPlan {
   int kvar;
   // SVD solves with all nine parameters free: 0 = matrix in shared memory,
   // 1 = in registers (svd9_kernel) in the one-thread-per-slot rounds, 2 = in
-  // registers in the lane-split rounds as well, 3 = in shared memory with the
-  // size fixed at 9 (unrolled rotations)
+  // registers in the lane-split rounds as well
   int svd_regs;
   double lambda0, bshift;
   double limits[9][2];
@@ -1243,12 +1242,8 @@ static __device__ __noinline__ int gr_svd(double *a, int n, double *w, double *v
 // scalars that are reassigned before their next use), so U and w come out
 // identical.  Matrix element (i, j) lives at a[(i * n + j) * STR], w[i] at
 // w[i * STR], so one thread's matrix can sit in a column of shared memory.
-// N > 0: the matrix size fixed at compile time (n is then N), so the row loops
-// of the QR rotations, whose trip count is the size, unroll into independent
-// updates; the rest of the code keeps its loops (a compact kernel).
-template <int STR, int N = 0>
-__device__ __noinline__ int gr_svd_u(double *a, int n_arg, double *w, double *rv1) {
-  const int n = N > 0 ? N : n_arg;
+template <int STR>
+__device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
 #define A_(i, j) a[((i) * n + (j)) * STR]
 #define W_(i) w[(i) * STR]
 #define R_(i) rv1[(i) * STR]
@@ -1352,7 +1347,6 @@ __device__ __noinline__ int gr_svd_u(double *a, int n_arg, double *w, double *rv
           h = 1.0 / h;
           c = g * h;
           s = -f * h;
-#pragma unroll
           for (int j = 0; j < m; j++) {
             y = A_(j, nm);
             z = A_(j, i);
@@ -1400,7 +1394,6 @@ __device__ __noinline__ int gr_svd_u(double *a, int n_arg, double *w, double *rv
         }
         f = c * g + s * y;
         x = c * y - s * g;
-#pragma unroll
         for (int jj = 0; jj < m; jj++) {
           y = A_(jj, j);
           z = A_(jj, i);

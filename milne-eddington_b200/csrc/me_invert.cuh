@@ -408,7 +408,7 @@ __device__ __forceinline__ void jac_store(const DevPlan &P, const Slots &S, int 
 // decomposition is gr_svd_u_grp, the rest runs redundantly in every lane and
 // lane 0 stores).  Returns the number of decompositions that hit the 50-sweep
 // limit.
-template <int STR, int G, int N = 0>
+template <int STR, int G>
 __device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int s, double *a,
                                           double *w, double *rv1, int lane, unsigned mask) {
   constexpr bool WARP = G > 1;
@@ -425,7 +425,7 @@ __device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int 
     if constexpr (WARP)
       return gr_svd_u_grp<G>(a, n, w, lane, mask);
     else
-      return gr_svd_u<STR, N>(a, n, w, rv1);
+      return gr_svd_u<STR>(a, n, w, rv1);
   };
   if (tk == 1) {
     hits += decompose();
@@ -820,10 +820,7 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_cons
   for (int i = blockIdx.x * kSvdBlock + t; i < count; i += gridDim.x * kSvdBlock) {
     const int s = list[i];
     if (S.state[s] != SL_TRIAL) continue;
-    // mode 3 with all nine parameters free: the n = 9 specialisation
-    tl.svdlim += (P.svd_regs == 3 && P.npar == 9)
-                     ? solve_slot<kSvdBlock, 1, 9>(P, S, s, a, w, rv1, 0, 0u)
-                     : solve_slot<kSvdBlock, 1>(P, S, s, a, w, rv1, 0, 0u);
+    tl.svdlim += solve_slot<kSvdBlock, 1>(P, S, s, a, w, rv1, 0, 0u);
   }
   tl.flush(A, S);
 }

@@ -110,15 +110,14 @@ def test_inversion_parity_vs_oracle(cfg0_map, prec, mode):
 @pytest.mark.parametrize("prec", ["FP64", "FP32"])
 def test_svd_registers_vs_shared_memory(cfg0_map, prec):
     """The SVD solve with the 9x9 matrix in registers (svd9_kernel, in the
-    full rounds and, mode 2, in the lane-split rounds too) or in shared memory
-    with the size fixed at 9 (mode 3) runs the shared-memory kernel's
-    operations in the same order; the compiler fuses
+    full rounds and, mode 2, in the lane-split rounds too) runs the
+    shared-memory kernel's operations in the same order; the compiler fuses
     multiply-adds differently in the two, so they agree to rounding, and each
     meets the oracle bar (the reference's own one-ulp spread)."""
     m = cfg0_map
     cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
     s_same, s_within, _ = m["self"]
-    for regs, group in ((0, 1), (1, 1), (2, 32), (3, 1)):
+    for regs, group in ((0, 1), (1, 1), (2, 32)):
         with me_b200.Plan(cfg, m["lam"]) as plan:
             plan.max_group, plan.tail_slots, plan.svd_lanes = group, 0, 1
             plan.svd_registers = regs
