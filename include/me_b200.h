@@ -292,10 +292,12 @@ int me_invert_batch(me_plan *plan, const double *prof, long npix, double *res,
  * and at least 131072 pixels, me_invert_batch copies the map in chunks of about
  * an eighth and starts inverting the first chunk while the others are on
  * their way; with a learned start each chunk's guesses and queue order
- * (sorted within the chunk) are made as it lands.  Results agree with the
- * whole-map copy to rounding (the order in which pixels meet the kernels
- * changes).  Default on; 0: copy the map whole first. */
-void me_plan_set_feed(me_plan *plan, int on);
+ * (sorted within the chunk) are made as it lands, and once the last chunk
+ * has landed the part of the queue not yet taken is re-sorted into the global
+ * order.  Results agree with the whole-map copy to rounding (the order in
+ * which pixels meet the kernels changes).  1 (default): on; 2: on, without
+ * the global re-sort; 0: copy the map whole first. */
+void me_plan_set_feed(me_plan *plan, int mode);
 
 /* Same on device buffers (d_prof, d_res, d_fit device pointers; d_fit may be
  * NULL); work is ordered on `stream` (a cudaStream_t, NULL = the plan's). */

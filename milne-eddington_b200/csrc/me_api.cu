@@ -150,6 +150,12 @@ struct me_plan {
   DevBuf d_avail;
   unsigned long long *h_feed = nullptr;  // pinned, kMaxFeedChunks
   std::vector<cudaEvent_t> feed_events;
+  // with a learned start and the queue order, the queue's untaken part is
+  // re-sorted globally once the whole map has arrived (me_plan_set_feed 2:
+  // chunk order only); its scratch
+  bool feed_resort = true;
+  bool resort_pending = false;
+  DevBuf d_tkey, d_tval, d_perm;
 };
 
 // chunks of the host entry point's overlapped copy (at most)
@@ -429,7 +435,7 @@ extern "C" void me_plan_destroy(me_plan *p) {
                     &p->d_slot_u8, &p->d_slot_sc, &p->d_slot_vec, &p->d_slot_hess,
                     &p->d_slot_list, &p->d_slot_small, &p->d_fitpar, &p->d_init,
                     &p->d_flambda, &p->d_fdlambda, &p->d_okey, &p->d_ohist, &p->d_order,
-                    &p->d_avail};
+                    &p->d_avail, &p->d_tkey, &p->d_tval, &p->d_perm};
   for (DevBuf *b : bufs) b->release();
   if (p->h_poll) cudaFreeHost(p->h_poll);
   if (p->h_feed) cudaFreeHost(p->h_feed);
@@ -755,6 +761,17 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     CK(cudaStreamSynchronize(st));
     const int busy = *reinterpret_cast<int *>(p->h_poll + 1);
     if (fed_before) fed = true;
+    if (fed && p->resort_pending) {
+      // the whole map is on the device and the stream is idle: the queue
+      // positions not taken yet go into the global misfit order
+      p->resort_pending = false;
+      const long long first = (long long)p->h_poll[0];
+      if (first < A.count && A.list)
+        CK(me::launch_resort_tail(const_cast<long long *>(A.list), first, A.count - first,
+                                  p->d_okey.as<unsigned char>(), p->d_tkey.as<unsigned char>(),
+                                  p->d_tval.as<long long>(), p->d_ohist.as<int>(),
+                                  p->d_perm.as<long long>(), st));
+    }
     const bool drained = p->h_poll[0] >= (unsigned long long)A.count && fed;
     if (drained && busy == 0) break;
     if (drained && p->max_group > 1) {
@@ -1049,12 +1066,19 @@ int start_feed(me_plan *p, const double *prof, long long npix, long long chunk, 
   const size_t n = (size_t)npix;
   const bool learned = p->init != nullptr;
   CK(p->d_avail.ensure(sizeof(unsigned long long)));
+  p->resort_pending = false;
   if (learned) {
     CK(p->d_init.ensure(n * 9 * sizeof(double)));
     if (p->queue_order) {
       CK(p->d_okey.ensure(n));
       CK(p->d_ohist.ensure((size_t)me::kOrderBuckets * me::kOrderBlocks * sizeof(int)));
       CK(p->d_order.ensure(n * sizeof(long long)));
+      if (p->feed_resort) {
+        CK(p->d_tkey.ensure(n));
+        CK(p->d_tval.ensure(n * sizeof(long long)));
+        CK(p->d_perm.ensure(n * sizeof(long long)));
+        p->resort_pending = true;
+      }
     }
   }
   // events: start, feed done, and per chunk arrival + prep start/end
@@ -1132,8 +1156,10 @@ extern "C" int me_invert_batch_device(me_plan *p, const double *d_prof, long npi
   return invert_impl(p, d_prof, npix, d_res, d_fit, st, stats, nullptr);
 }
 
-extern "C" void me_plan_set_feed(me_plan *p, int on) {
-  if (p) p->feed = on != 0;
+extern "C" void me_plan_set_feed(me_plan *p, int mode) {
+  if (!p) return;
+  p->feed = mode != 0;
+  p->feed_resort = mode != 2;
 }
 
 extern "C" int me_invert_batch(me_plan *p, const double *prof, long npix, double *res, double *fit,

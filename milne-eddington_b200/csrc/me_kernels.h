@@ -180,6 +180,12 @@ cudaError_t launch_start_order(int precision, const DevPlan &P, const double *d_
                                const double *d_init, long long npix, unsigned char *d_key,
                                int *d_hist, long long *d_order, cudaStream_t st,
                                long long base = 0);
+// queue positions [first, first + n) of d_list re-sorted by the per-pixel
+// keys d_key (stable); d_tkey (n bytes), d_tval, d_perm (n each): scratch
+cudaError_t launch_resort_tail(long long *d_list, long long first, long long n,
+                               const unsigned char *d_key, unsigned char *d_tkey,
+                               long long *d_tval, int *d_hist, long long *d_perm,
+                               cudaStream_t st);
 // the stable counting sort alone (keys < kOrderBuckets)
 cudaError_t launch_order_by_key(const unsigned char *d_key, long long n, int *d_hist,
                                 long long *d_order, cudaStream_t st, long long base = 0);

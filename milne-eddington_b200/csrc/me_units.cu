@@ -388,6 +388,40 @@ cudaError_t launch_order_by_key(const unsigned char *d_key, long long n, int *d_
   return cudaGetLastError();
 }
 
+// Re-sort of the queue positions [first, first + n) of `list` by the pixels'
+// misfit keys, stable (the streamed host entry point: once the whole map has
+// arrived, the part of the queue not yet taken goes into one global order).
+__global__ void tail_gather_kernel(const long long *list, long long first, long long n,
+                                   const unsigned char *key, unsigned char *tkey,
+                                   long long *tval) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long pix = list[first + i];
+  tval[i] = pix;
+  tkey[i] = key[pix];
+}
+
+__global__ void tail_scatter_kernel(long long *list, long long first, long long n,
+                                    const long long *perm, const long long *tval) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  list[first + i] = tval[perm[i]];
+}
+
+cudaError_t launch_resort_tail(long long *d_list, long long first, long long n,
+                               const unsigned char *d_key, unsigned char *d_tkey,
+                               long long *d_tval, int *d_hist, long long *d_perm,
+                               cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int b = 256;
+  const unsigned g = (unsigned)((n + b - 1) / b);
+  tail_gather_kernel<<<g, b, 0, st>>>(d_list, first, n, d_key, d_tkey, d_tval);
+  cudaError_t e = launch_order_by_key(d_tkey, n, d_hist, d_perm, st, 0);
+  if (e != cudaSuccess) return e;
+  tail_scatter_kernel<<<g, b, 0, st>>>(d_list, first, n, d_perm, d_tval);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_start_order(int precision, const DevPlan &P, const double *d_prof,
                                const double *d_init, long long npix, unsigned char *d_key,
                                int *d_hist, long long *d_order, cudaStream_t st,

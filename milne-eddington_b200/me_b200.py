@@ -517,10 +517,11 @@ class Plan:
     def kernel_variant(self, v: int):
         lib().me_plan_set_kernel_variant(self._h, int(v))
 
-    def set_feed(self, on: bool = True):
+    def set_feed(self, mode=True):
         """me_invert_batch from page-locked host memory: copy the map in chunks
-        and start inverting as they land (default on); off: copy it whole first."""
-        lib().me_plan_set_feed(self._h, int(bool(on)))
+        and start inverting as they land (True / 1, default); 2: the same without
+        the global re-sort of the queue's untaken part; False / 0: copy it whole."""
+        lib().me_plan_set_feed(self._h, int(mode))
 
     def set_overlap(self, on: bool = True):
         """Later-trial SVDs on a second stream beside the Jacobian kernel (default on)."""
