@@ -255,6 +255,8 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--plain-steps", type=int, default=-1, help="timed plain-LM steps (-1: K)")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-warmup", type=int, default=1,
+                    help="untimed calls of the host entry point before its timed steps")
     ap.add_argument("--fp64-sample", type=int, default=16384,
                     help="pixels of the FP32-vs-FP64 comparison of the plain algorithm (0: off)")
     ap.add_argument("--autotune", type=int, default=1,
@@ -815,13 +817,16 @@ def main():
         h_prof_np = h_prof.numpy()
         h_res = torch.empty((npix, 10), dtype=torch.float64, pin_memory=True)
         h_res_np = h_res.numpy()
+        for _ in range(args.e2e_warmup):  # first-call set-up of the streamed copy
+            plan.invert(h_prof_np, out=h_res_np)
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             _, st_e2e = plan.invert(h_prof_np, out=h_res_np)
         e2e_s = me_ranks.max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, dist, "cuda")
-        e2e = {"seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"], "d2h_ms": st_e2e["d2h_ms"]}
+        e2e = {"seconds": e2e_s, "h2d_ms": st_e2e["h2d_ms"], "d2h_ms": st_e2e["d2h_ms"],
+               "steps": args.e2e_steps, "warmup": args.e2e_warmup}
         del h_prof, h_prof_np, h_res, h_res_np
 
     res_np = res.cpu().numpy()
@@ -1007,7 +1012,9 @@ def main():
             line["e2e"] = {"value": npix * world / e2e["seconds"] * frac, "unit": UNIT,
                            "h2d_bytes_per_step": npix * 4 * nl * 8,
                            "d2h_bytes_per_step": npix * 10 * 8,
-                           "h2d_ms": e2e["h2d_ms"], "d2h_ms": e2e["d2h_ms"]}
+                           "h2d_ms": e2e["h2d_ms"], "d2h_ms": e2e["d2h_ms"],
+                           "steps": e2e["steps"], "warmup": e2e["warmup"],
+                           "host_buffers": "page-locked (profiles streamed in chunks)"}
         print(json.dumps(line), flush=True)
     init.close()
     plan.close()
