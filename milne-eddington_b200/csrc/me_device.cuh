@@ -142,8 +142,11 @@ __device__ __forceinline__ T erfcx_t(T a) {
 }
 
 // Dawson's integral by Rybicki's method (FADDEEVA.c:29-79); only reached for a == 0.
+// Out of line, like the two evaluators below that the default accuracy row
+// (Nfigures 6, damping below 1) never reaches: the synthesis kernels' hot code
+// stays smaller, and their instruction fetch stalls less.
 template <class T>
-__device__ T dawson_t(T x) {
+__device__ __noinline__ T dawson_t(T x) {
   const T H = T(0.4);
   T ax = m_abs(x);
   if (ax < T(0.2)) {
@@ -170,7 +173,7 @@ __device__ T dawson_t(T x) {
 
 // Hui, Armstrong & Wray (1978) 6-pole rational approximation (FADDEEVA.c:112-163).
 template <class T>
-__device__ __forceinline__ HL<T> voigt_hui6(T nu, T y) {
+__device__ __noinline__ HL<T> voigt_hui6(T nu, T y) {
   const T A[7] = {T(122.607931777104326), T(214.382388694706425), T(181.928533092181549),
                   T(93.155580458138441),  T(30.180142196210589),  T(5.912626209773153),
                   T(0.564189583562615)};
@@ -196,7 +199,7 @@ __device__ __forceinline__ HL<T> voigt_hui6(T nu, T y) {
 
 // Humlicek (1982) W4 (FADDEEVA.c:167-281).  Reached only for Nfigures <= 5.
 template <class T>
-__device__ HL<T> voigt_humlicek_w4(T nu, T y) {
+__device__ __noinline__ HL<T> voigt_humlicek_w4(T nu, T y) {
   T H, L;
   const T anu = m_abs(nu);
   const T s = anu + y;

@@ -1025,8 +1025,10 @@ __device__ double forward_warp(const DevPlan &P, VoigtK<T> &K, T *rden, const do
 
 }  // namespace detail
 
+// (compiled for one CTA per SM at least: 230 registers and no spill on the FP32
+// path, where the default budget spilled; the kernel runs a few warps per SM)
 template <class T, bool FILT>
-__global__ void __launch_bounds__(kBlock) finish_kernel(const __grid_constant__ DevPlan P,
+__global__ void __launch_bounds__(kBlock, 1) finish_kernel(const __grid_constant__ DevPlan P,
                                                         const __grid_constant__ InvertArgs A,
                                                         const __grid_constant__ Slots S,
                                                         int *cursor) {
