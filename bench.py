@@ -569,9 +569,10 @@ def gpu_map(torch, me_b200, name, npix, seed, device):
 # ---------------------------------------------------------------------------
 def other_workload(torch, me_b200, args, key, stream, cores, init_headline):
     """One further workload: learned start (1 warm-up + 2 timed steps) and
-    plain LM (1 timed step after a warm-up on a part of the map), the
-    converged share of each against the reference core (the port with the
-    filter) on a seeded sample, iteration histograms, fallback rate."""
+    plain LM (1 timed step after a warm-up on a part of the map), each arm
+    autotuned first on the map's first 262144 pixels, the converged share of
+    each against the reference core (the port with the filter) on a seeded
+    sample, iteration histograms, fallback rate."""
     if key == "literal":
         name, widen, label = args.workload, False, f"{args.workload}_literal_bounds"
     else:
@@ -605,6 +606,11 @@ def other_workload(torch, me_b200, args, key, stream, cores, init_headline):
                 torch.cuda.synchronize()
                 out["train_s"] = time.perf_counter() - t0
             plan.set_initializer(init)
+            # the autotuner on a part of the map (its time stays bounded), per arm
+            tune_pix = min(npix, 262144)
+            tuned_l = tuned_p = None
+            if args.autotune:
+                tuned_l = plan.autotune(prof.data_ptr(), tune_pix, stream.cuda_stream)
 
             def step():
                 return plan.invert_device(prof.data_ptr(), npix, res.data_ptr(), 0,
@@ -618,6 +624,8 @@ def other_workload(torch, me_b200, args, key, stream, cores, init_headline):
             plan.set_initializer(None)
             if key != "literal":
                 init.close()
+            if args.autotune:
+                tuned_p = plan.autotune(prof.data_ptr(), tune_pix, stream.cuda_stream)
             # plain LM: warm-up on the first eighth of the map, one timed step
             part = max(1, npix // 8)
             plan.invert_device(prof.data_ptr(), part, res.data_ptr(), 0, stream.cuda_stream)
@@ -648,6 +656,8 @@ def other_workload(torch, me_b200, args, key, stream, cores, init_headline):
         "runs_per_pixel": last["runs"] / max(1, last["valid"]),
         "plain_runs_per_pixel": st_p[-1]["runs"] / max(1, st_p[-1]["valid"]),
         "histograms": {"learned": work_histograms(counts), "plain": work_histograms(counts_p)},
+        "autotuned": {"learned": tuned_l, "plain": tuned_p,
+                      "on_pixels": min(npix, 262144)},
         "converged_sample": f"{nb} seeded pixels vs the {pool.kind} FP64 chi^2",
         "cpu_pixels_per_s": nb / ref_dt,
         "param_err_vs_truth_median_p99": param_errors(res_l, par_true),
