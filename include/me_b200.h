@@ -245,6 +245,29 @@ void me_plan_set_svd_lanes(me_plan *plan, int lanes);
  * device time in me_stats (off by default; costs a little host time). */
 void me_plan_set_profiling(me_plan *plan, int on);
 void me_plan_set_tail_slots(me_plan *plan, int slots);
+/* The rounds after the queue drains: each pixel in flight gets the most lanes
+ * (a power of two, at most max_group) for which pixels x lanes stay within
+ * group_fill (1..8) half waves of the Jacobian kernel -- more lanes cut each
+ * round's latency, fewer keep each round's work compact -- and the host checks
+ * the pixels in flight every poll_rounds rounds (even, 2..64), which is how
+ * often the lanes adapt and when the tail kernel can take over.  Defaults 4
+ * (two waves) and 4. */
+void me_plan_set_drain(me_plan *plan, int group_fill, int poll_rounds);
+void me_plan_get_drain(const me_plan *plan, int *group_fill, int *poll_rounds);
+
+/* The host's checks of the queue during the plan's last batch, one record per
+ * check: host time since the batch's rounds began (ms; the check waits for
+ * the rounds launched before it, so this is when they ended), LM rounds so
+ * far, queue position, pixels in flight and lanes per pixel of the rounds
+ * before it (1 = one thread per pixel; 0 marks the tail kernel's launch,
+ * -1 the end of the batch's first pass).  Writes at most cap records to out
+ * (may be NULL) and returns how many the batch made. */
+typedef struct me_poll_record {
+  double ms;
+  long long rounds, next;
+  int busy, group;
+} me_poll_record;
+int me_plan_poll_trace(const me_plan *plan, me_poll_record *out, int cap);
 
 /* Per-pixel counters of the plan's last batch: [npix][4] = LM runs,
  * iterations (syntheses with Jacobian), trial steps, accepted steps; zeros
@@ -269,8 +292,9 @@ void me_plan_set_kernel_variant(me_plan *plan, int variant);
  * flight (window), lanes per pixel after the queue drains (max_group), the
  * tail kernel's threshold (tail_slots), lanes per SVD (svd_lanes), the
  * kernel variant (pixels per CTA, grid staging, Faddeeva series reciprocals;
- * me_plan_set_kernel_variant) and where the SVD keeps its matrix
- * (me_plan_set_svd_registers) -- one knob at a time, keeping each
+ * me_plan_set_kernel_variant), where the SVD keeps its matrix
+ * (me_plan_set_svd_registers) and the lanes and check interval after the
+ * queue drains (me_plan_set_drain) -- one knob at a time, keeping each
  * improvement, and leaves the best setting on the plan.  The carried LM chi^2 is restored afterwards.  out (may be NULL)
  * receives the choice, its time and the number of timed runs. */
 typedef struct me_tune_result {
@@ -278,6 +302,7 @@ typedef struct me_tune_result {
   double ms;    /* device time of the batch with the chosen setting */
   int trials;   /* batches timed */
   int kernel_variant, svd_registers;  /* me_plan_set_kernel_variant / _svd_registers */
+  int group_fill, drain_poll;         /* me_plan_set_drain */
 } me_tune_result;
 int me_plan_autotune(me_plan *plan, const double *d_prof, long npix, void *stream,
                      me_tune_result *out);

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <string>
 #include <functional>
 #include <vector>
@@ -130,6 +131,12 @@ struct me_plan {
   unsigned long long tail_start_totals[8] = {};
   bool tail_seen = false;
   int poll_rounds = 8;     // rounds launched between checks of the queue
+  // once the queue is empty: rounds between checks, and how many lanes each
+  // pixel in flight gets -- the most (a power of two, at most max_group) for
+  // which pixels x lanes stay within group_fill half waves of the Jacobian
+  // kernel (me_plan_set_drain)
+  int drain_poll = 4;
+  int group_fill = 4;
   unsigned long long *h_poll = nullptr;  // pinned: next, busy
   long long rounds_last = 0;
   std::vector<unsigned char> h_flags;
@@ -156,6 +163,9 @@ struct me_plan {
   bool feed_resort = true;
   bool resort_pending = false;
   DevBuf d_tkey, d_tval, d_perm;
+  // the queue checks of the last batch (me_plan_poll_trace) and its start
+  std::vector<me_poll_record> trace;
+  std::chrono::steady_clock::time_point trace_t0;
 };
 
 // chunks of the host entry point's overlapped copy (at most)
@@ -520,6 +530,14 @@ extern "C" void me_plan_set_graphs(me_plan *p, int on) {
   if (p) p->use_graphs = on != 0;
 }
 
+extern "C" int me_plan_poll_trace(const me_plan *p, me_poll_record *out, int cap) {
+  if (!p) return 0;
+  const int n = (int)p->trace.size();
+  if (out)
+    for (int i = 0; i < n && i < cap; i++) out[i] = p->trace[i];
+  return n;
+}
+
 extern "C" int me_plan_svd_lanes(const me_plan *p) { return p ? p->svd_lanes : 0; }
 extern "C" int me_plan_svd_registers(const me_plan *p) { return p ? p->P.svd_regs : 0; }
 extern "C" int me_plan_kernel_variant(const me_plan *p) { return p ? p->P.kvar : 0; }
@@ -539,6 +557,17 @@ extern "C" void me_plan_set_max_group(me_plan *p, int lanes) {
   int g = 1;
   while (g * 2 <= lanes && g < 32) g *= 2;
   p->max_group = g;
+}
+
+extern "C" void me_plan_set_drain(me_plan *p, int group_fill, int poll_rounds) {
+  if (!p) return;
+  p->group_fill = group_fill < 1 ? 1 : (group_fill > 8 ? 8 : group_fill);
+  const int r = poll_rounds < 2 ? 2 : (poll_rounds > 64 ? 64 : poll_rounds);
+  p->drain_poll = r & ~1;  // even: a captured batch of rounds starts at parity 0
+}
+extern "C" void me_plan_get_drain(const me_plan *p, int *group_fill, int *poll_rounds) {
+  if (group_fill) *group_fill = p ? p->group_fill : 0;
+  if (poll_rounds) *poll_rounds = p ? p->drain_poll : 0;
 }
 
 extern "C" int me_plan_tail_slots(const me_plan *p) { return p ? p->tail_slots : 0; }
@@ -624,6 +653,12 @@ cudaEvent_t *take_events(me_plan *p, size_t n) {
   return ev;
 }
 
+void trace_poll(me_plan *p, long long rounds, long long next, int busy, int group) {
+  const std::chrono::duration<double, std::milli> t =
+      std::chrono::steady_clock::now() - p->trace_t0;
+  p->trace.push_back({t.count(), rounds, next, busy, group});
+}
+
 // Runs one queue (A.count items) to completion: rounds of jac_kernel,
 // svd_kernel and trial_kernel on the plan's slots while the queue feeds them,
 // then, once it is empty and at most tail_slots pixels remain, finish_kernel
@@ -706,8 +741,9 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     me::Overlap ov_storage{p->stream2, p->ev_fork, p->ev_join};
     const me::Overlap *ov = (p->overlap && !p->profile) ? &ov_storage : nullptr;
     const int gi = group_index(group);
+    const int nr = group > 1 ? p->drain_poll : p->poll_rounds;
     cudaGraphExec_t *gx =
-        (graphs_ok && ran_direct[gi] && p->use_graphs && !p->profile && p->poll_rounds % 2 == 0)
+        (graphs_ok && ran_direct[gi] && p->use_graphs && !p->profile && nr % 2 == 0)
             ? &graphs[gi]
             : nullptr;
     ran_direct[gi] = true;
@@ -715,7 +751,7 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
       cudaError_t e = cudaSuccess;
-      for (int r = 0; r < p->poll_rounds && e == cudaSuccess; r++)
+      for (int r = 0; r < nr && e == cudaSuccess; r++)
         e = group > 1 ? me::launch_round_grp(p->precision, group, p->P, A, S, r & 1, ggrids,
                                              p->stream, nullptr, ov)
                       : me::launch_round(p->precision, p->P, A, S, r & 1, grids, p->stream,
@@ -738,9 +774,9 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
         release_graphs();
         return fail(ME_ERR_CUDA, std::string("round graph launch: ") + cudaGetErrorString(e));
       }
-      rounds += p->poll_rounds;
+      rounds += nr;
     } else {
-      for (int r = 0; r < p->poll_rounds; r++) {
+      for (int r = 0; r < nr; r++) {
         cudaEvent_t *ev = nullptr;
         if (p->profile) {
           const size_t first = p->ev_used;
@@ -760,6 +796,7 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     CK(cudaMemcpyAsync(p->h_poll + 1, S.busy, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     const int busy = *reinterpret_cast<int *>(p->h_poll + 1);
+    trace_poll(p, rounds, (long long)p->h_poll[0], busy, group);
     if (fed_before) fed = true;
     if (fed && p->resort_pending) {
       // the whole map is on the device and the stream is idle: the queue
@@ -776,10 +813,10 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
     if (drained && busy == 0) break;
     if (drained && p->max_group > 1) {
       // the queue is empty: give each slot in flight as many lanes as fill
-      // about one wave of the Jacobian kernel on the whole device
+      // group_fill half waves of the Jacobian kernel on the whole device
       const long long wave = (long long)p->grid_jac * me::kBlock;
       int g = 1;
-      while (g < p->max_group && (long long)busy * g * 2 <= wave) g *= 2;
+      while (g < p->max_group && (long long)busy * g * 2 <= wave * p->group_fill) g *= 2;
       group = g;
       const long long need = ((long long)W * g + me::kBlock - 1) / me::kBlock;
       ggrids[0] = (int)std::min<long long>(p->grid_jac, need);
@@ -809,6 +846,7 @@ int run_queue(me_plan *p, const me::InvertArgs &A, cudaStream_t st, long long &r
       }
       CK(me::launch_finish(p->precision, p->P, A, S, cursor, std::max(g, 1), st));
       if (ev) CK(cudaEventRecord(ev[1], st));
+      trace_poll(p, rounds, (long long)p->h_poll[0], busy, 0);
       p->finish_launches++;
       break;
     }
@@ -901,6 +939,8 @@ int invert_impl(me_plan *p, const double *d_prof, long npix, double *d_res, doub
   p->ev_used = 0;
   p->ev_marks.clear();
   p->tail_seen = false;
+  p->trace.clear();
+  p->trace_t0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(p->ev0, st));
   int rc = run_queue(p, A, st, rounds, feed ? feed->done : nullptr);
   if (rc) return rc;
@@ -928,6 +968,7 @@ int invert_impl(me_plan *p, const double *d_prof, long npix, double *d_res, doub
     CK(cudaMemcpyAsync(p->h_pen0.data(), A.penalty0, n * sizeof(double), cudaMemcpyDeviceToHost,
                        st));
   CK(cudaStreamSynchronize(st));
+  trace_poll(p, rounds, npix, 0, -1);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, p->ev0, p->ev1);
   double kernel_ms = ms;
@@ -1425,9 +1466,13 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
       // the wavelength grid staged in shared memory, no reciprocal table, the
       // normal-equation sums in shared memory
       {&p->P.kvar, {0, 1, 2, 3, 4, 5}},
-      // the 9x9 SVD in registers in the full rounds (default), also in the
-      // lane-split rounds, or in shared memory throughout
+      // the 9x9 SVD in registers in the full rounds, also in the lane-split
+      // rounds, or in shared memory throughout (the default)
       {&p->P.svd_regs, {1, 2, 0}},
+      // after the queue drains: lanes per pixel in flight (half a wave to four
+      // waves of the Jacobian kernel) and rounds between checks
+      {&p->group_fill, {1, 2, 4, 8}},
+      {&p->drain_poll, {8, 4, 2}},
   };
   for (Knob &k : knobs) {
     if (rc) break;
@@ -1460,6 +1505,8 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
     out->trials = trials;
     out->kernel_variant = p->P.kvar;
     out->svd_registers = p->P.svd_regs;
+    out->group_fill = p->group_fill;
+    out->drain_poll = p->drain_poll;
   }
   return ME_OK;
 }

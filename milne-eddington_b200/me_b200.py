@@ -153,15 +153,21 @@ EXPORTED = [
     "me_fits_image_info", "me_fits_read", "me_fits_create", "me_fits_write",
     "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
     "me_mlp_set_gemm", "me_mlp_gemm_launches", "me_gemm_bf16", "me_plan_set_queue_order",
-    "me_order_by_key",
+    "me_order_by_key", "me_plan_poll_trace", "me_plan_set_drain", "me_plan_get_drain",
 ]
+
+
+class MePollRecord(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double), ("rounds", ctypes.c_longlong),
+                ("next", ctypes.c_longlong), ("busy", ctypes.c_int), ("group", ctypes.c_int)]
 
 
 class MeTuneResult(ctypes.Structure):
     _fields_ = [("window", ctypes.c_int), ("max_group", ctypes.c_int),
                 ("tail_slots", ctypes.c_int), ("svd_lanes", ctypes.c_int),
                 ("ms", ctypes.c_double), ("trials", ctypes.c_int),
-                ("kernel_variant", ctypes.c_int), ("svd_registers", ctypes.c_int)]
+                ("kernel_variant", ctypes.c_int), ("svd_registers", ctypes.c_int),
+                ("group_fill", ctypes.c_int), ("drain_poll", ctypes.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -263,6 +269,13 @@ def lib() -> ctypes.CDLL:
                                        ctypes.c_void_p, ctypes.POINTER(MeTuneResult)]
         L.me_plan_last_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint),
                                             ctypes.c_long]
+        L.me_plan_set_drain.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.me_plan_set_drain.restype = None
+        L.me_plan_get_drain.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]
+        L.me_plan_get_drain.restype = None
+        L.me_plan_poll_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_poll_trace.restype = ctypes.c_int
         L.me_plan_set_overlap.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.me_plan_set_overlap.restype = None
         L.me_plan_set_queue_order.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -498,6 +511,27 @@ class Plan:
                                       ctypes.c_void_p(stream) if stream else None,
                                       ctypes.byref(r)), "me_plan_autotune")
         return r.as_dict()
+
+    @property
+    def drain(self) -> tuple:
+        """(group_fill, poll_rounds) of the rounds after the queue drains."""
+        f, r = ctypes.c_int(), ctypes.c_int()
+        lib().me_plan_get_drain(self._h, ctypes.byref(f), ctypes.byref(r))
+        return f.value, r.value
+
+    @drain.setter
+    def drain(self, v):
+        lib().me_plan_set_drain(self._h, int(v[0]), int(v[1]))
+
+    def poll_trace(self) -> list:
+        """The queue checks of the last batch: dicts of ms (host time since its
+        rounds began), rounds, next (queue position), busy (pixels in flight)
+        and group (lanes per pixel; 0 = tail kernel launched, -1 = first pass
+        ended)."""
+        n = lib().me_plan_poll_trace(self._h, None, 0)
+        buf = (MePollRecord * max(n, 1))()
+        n = lib().me_plan_poll_trace(self._h, buf, n)
+        return [{k: getattr(buf[i], k) for k, _ in MePollRecord._fields_} for i in range(n)]
 
     def last_counters(self, npix: int) -> np.ndarray:
         """[npix][4] runs, iterations, trials, accepted of the last batch."""

@@ -77,7 +77,11 @@ def cfg0_map():
 # rounds; the warp-per-pixel tail kernel (for a batch this small the last
 # three run most of the LM steps)
 MODES = {"threads": (1, 0, 1, 1), "lane_split": (32, 0, 4, 1),
-         "lane_split_svd_regs": (32, 0, 1, 2), "tail_kernel": (1, -1, 1, 1)}
+         "lane_split_svd_regs": (32, 0, 1, 2), "tail_kernel": (1, -1, 1, 1),
+         "lane_split_half_wave": (32, -1, 1, 1)}
+# lanes and check interval after the queue drains (me_plan_set_drain), where
+# a mode sets them: half a wave and checks every 8 rounds
+DRAIN = {"lane_split_half_wave": (1, 8)}
 
 
 @pytest.mark.parametrize("mode", list(MODES))
@@ -87,6 +91,9 @@ def test_inversion_parity_vs_oracle(cfg0_map, prec, mode):
     cfg = me_b200.parse_config_text(me_maps.control_text(m["name"], precision=prec))
     with me_b200.Plan(cfg, m["lam"]) as plan:
         plan.max_group, plan.tail_slots, plan.svd_lanes, plan.svd_registers = MODES[mode]
+        if mode in DRAIN:
+            plan.drain = DRAIN[mode]
+            assert plan.drain == DRAIN[mode]
         res, stats = invert_chunks(plan, m["prof"])
     for st in stats:
         tail_launches = st["launches"] - 4 * st["rounds"]
@@ -280,5 +287,36 @@ def test_autotune_picks_a_setting_and_keeps_results_valid():
         assert r["svd_lanes"] in (1, 2)
         assert (plan.window, plan.max_group, plan.tail_slots, plan.svd_lanes) == \
             (r["window"], r["max_group"], r["tail_slots"], r["svd_lanes"])
+        assert r["group_fill"] in (1, 2, 4, 8) and r["drain_poll"] in (2, 4, 8)
+        assert plan.drain == (r["group_fill"], r["drain_poll"])
         res, st = plan.invert(prof)
         assert st["valid"] == prof.shape[0] and (res[:, 9] > 0).all()
+
+
+def test_poll_trace_records_the_batch():
+    """me_plan_poll_trace: one record per check of the queue, in time order,
+    the lanes growing as the queue drains, the tail kernel's launch marked 0
+    and the end of the first pass -1."""
+    name = "fe15648_64x64"
+    lam = me_maps.wavelengths(name)
+    cfg = me_b200.parse_config_text(me_maps.control_text(name, precision="FP32"))
+    with me_b200.Plan(cfg, lam) as plan:
+        par = me_maps.draw_parameters(name, 4096, 62)
+        prof = me_maps.add_noise(plan.synthesize(par), 1e-3, 62)
+        plan.window, plan.max_group, plan.tail_slots = 1024, 32, 64
+        plan.drain = (2, 2)
+        plan.invert(prof)
+        tr = plan.poll_trace()
+    # the first pass (passes that re-run pixels for the carried chi^2 follow)
+    tr = tr[:[r["group"] for r in tr].index(-1) + 1]
+    assert len(tr) >= 3
+    assert all(b["ms"] >= a["ms"] for a, b in zip(tr, tr[1:]))
+    assert tr[-1]["group"] == -1 and tr[-1]["busy"] == 0 and tr[-1]["next"] == 4096
+    rounds = [r["rounds"] for r in tr[:-1]]
+    assert rounds == sorted(rounds)
+    groups = [r["group"] for r in tr[:-1] if r["group"] > 0]
+    assert groups[0] == 1 and groups == sorted(groups) and max(groups) > 1
+    assert sum(r["group"] == 0 for r in tr) == 1  # one tail kernel launch
+    # checks in the lane-split phase come every 2 rounds
+    steps = {b["rounds"] - a["rounds"] for a, b in zip(tr, tr[1:-1]) if a["group"] > 1 and b["group"] > 1}
+    assert steps <= {2}
