@@ -286,6 +286,22 @@ int me_plan_last_counters(const me_plan *plan, unsigned int *counters, long npix
 int me_plan_kernel_variant(const me_plan *plan);
 void me_plan_set_kernel_variant(me_plan *plan, int variant);
 
+/* How an FP32 plan's syntheses evaluate the Faddeeva function w(z) (Voigt and
+ * Faraday-Voigt profiles): 0 = the reference's |z| regions with their rational
+ * approximations and Alg-916 (Faddeeva, Src/FADDEEVA.c:440-590) in FP32;
+ * 1 (default) = Weideman's 16-term rational series (SIAM J. Numer. Anal. 31,
+ * 1994), one formula for every z with Im z >= 0, within 6e-7 of w in FP32, with
+ * no branch -- a different method at least as accurate as mode 0 in FP32, so
+ * results agree with mode 0 to that accuracy, not bit for bit.  FP64 plans
+ * always use 0, the reference's method. */
+int me_plan_faddeeva(const me_plan *plan);
+void me_plan_set_faddeeva(me_plan *plan, int mode);
+/* The coefficients c_0..c_15 and the scale L of that series, for checking. */
+void me_weideman16(float *coef, float *L);
+/* w(nu + i a) by that series in FP32 on the device: H = Re w, L = Im w. */
+int me_faddeeva_weideman(const double *nu, const double *a, long n, double *H, double *L,
+                         int device);
+
 /* Autotuner: times me_invert_batch_device on the caller's batch (device
  * profiles d_prof [npix][4][nl], ideally of the size and kind the plan will
  * invert) for candidate values of the plan's runtime knobs -- pixels in
@@ -293,8 +309,9 @@ void me_plan_set_kernel_variant(me_plan *plan, int variant);
  * tail kernel's threshold (tail_slots), lanes per SVD (svd_lanes), the
  * kernel variant (pixels per CTA, grid staging, Faddeeva series reciprocals;
  * me_plan_set_kernel_variant), where the SVD keeps its matrix
- * (me_plan_set_svd_registers) and the lanes and check interval after the
- * queue drains (me_plan_set_drain) -- one knob at a time, keeping each
+ * (me_plan_set_svd_registers), the lanes and check interval after the
+ * queue drains (me_plan_set_drain) and the FP32 Faddeeva evaluation
+ * (me_plan_set_faddeeva) -- one knob at a time, keeping each
  * improvement, and leaves the best setting on the plan.  The carried LM chi^2 is restored afterwards.  out (may be NULL)
  * receives the choice, its time and the number of timed runs. */
 typedef struct me_tune_result {
@@ -303,6 +320,7 @@ typedef struct me_tune_result {
   int trials;   /* batches timed */
   int kernel_variant, svd_registers;  /* me_plan_set_kernel_variant / _svd_registers */
   int group_fill, drain_poll;         /* me_plan_set_drain */
+  int faddeeva;                       /* me_plan_set_faddeeva */
 } me_tune_result;
 int me_plan_autotune(me_plan *plan, const double *d_prof, long npix, void *stream,
                      me_tune_result *out);

@@ -229,6 +229,7 @@ int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P
   // shared memory
   P.svd_regs = 0;
   P.kvar = cfg->precision == ME_PREC_FP64 ? 0 : 5;
+  P.faddeeva = cfg->precision == ME_PREC_FP32 ? 1 : 0;
   P.ncut = nl / 5;
   const double c = 299792458.0;
   double t = (lambda[P.ncut] - lam0) * c / 1e3;  // the reference omits /lambda0 here
@@ -543,6 +544,17 @@ extern "C" int me_plan_svd_registers(const me_plan *p) { return p ? p->P.svd_reg
 extern "C" int me_plan_kernel_variant(const me_plan *p) { return p ? p->P.kvar : 0; }
 extern "C" void me_plan_set_kernel_variant(me_plan *p, int v) {
   if (p) p->P.kvar = (v >= 0 && v < me::kKernelVariants) ? v : 0;
+}
+extern "C" int me_plan_faddeeva(const me_plan *p) { return p ? p->P.faddeeva : 0; }
+extern "C" void me_plan_set_faddeeva(me_plan *p, int mode) {
+  if (p) p->P.faddeeva = (mode == 1 && p->precision == ME_PREC_FP32) ? 1 : 0;
+}
+extern "C" void me_weideman16(float *coef, float *L) {
+#define ME_WEID_COPY(n, c) \
+  if (coef) coef[n] = c;
+  ME_WEIDEMAN16(ME_WEID_COPY)
+#undef ME_WEID_COPY
+  if (L) *L = ME_WEIDEMAN16_L;
 }
 extern "C" void me_plan_set_svd_registers(me_plan *p, int mode) {
   if (p) p->P.svd_regs = mode <= 0 ? 0 : (mode >= 2 ? 2 : 1);
@@ -1338,6 +1350,31 @@ extern "C" int me_faddeeva(int nfigures, int precision, const double *nu, const 
   return ME_OK;
 }
 
+extern "C" int me_faddeeva_weideman(const double *nu, const double *a, long n, double *H,
+                                    double *L, int device) {
+  if (!nu || !a || !H || !L || n < 0) return fail(ME_ERR_ARG, "bad argument");
+  int st = check_device(device);
+  if (st) return st;
+  if (n == 0) return ME_OK;
+  me::DevPlan P;
+  memset(&P, 0, sizeof(P));
+  fill_voigt_consts(P, 6);
+  P.faddeeva = 1;
+  DevBuf dn, da, dh, dl;
+  const size_t b = (size_t)n * sizeof(double);
+  CK(dn.ensure(b));
+  CK(da.ensure(b));
+  CK(dh.ensure(b));
+  CK(dl.ensure(b));
+  CK(cudaMemcpy(dn.p, nu, b, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(da.p, a, b, cudaMemcpyHostToDevice));
+  CK(me::launch_voigt(0, P, dn.as<double>(), da.as<double>(), n, dh.as<double>(),
+                      dl.as<double>(), 0));
+  CK(cudaMemcpy(H, dh.p, b, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(L, dl.p, b, cudaMemcpyDeviceToHost));
+  return ME_OK;
+}
+
 extern "C" int me_svd(const double *a, long nmat, int n, double *u, double *w, double *v,
                       int device) {
   if (!a || !u || !w || !v || nmat < 0 || n < 1 || n > 9) return fail(ME_ERR_ARG, "bad argument");
@@ -1473,6 +1510,9 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
       // waves of the Jacobian kernel) and rounds between checks
       {&p->group_fill, {1, 2, 4, 8}},
       {&p->drain_poll, {8, 4, 2}},
+      // the FP32 syntheses' Faddeeva evaluation: the reference's regions and
+      // Alg-916, or Weideman's series (FP64 plans keep the former)
+      {&p->P.faddeeva, {0, p->precision == ME_PREC_FP32 ? 1 : 0}},
   };
   for (Knob &k : knobs) {
     if (rc) break;
@@ -1507,6 +1547,7 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
     out->svd_registers = p->P.svd_regs;
     out->group_fill = p->group_fill;
     out->drain_poll = p->drain_poll;
+    out->faddeeva = p->P.faddeeva;
   }
   return ME_OK;
 }

@@ -45,6 +45,9 @@ struct DevPlan {
   // 1 = in registers (svd9_kernel) in the one-thread-per-slot rounds, 2 = in
   // registers in the lane-split rounds as well
   int svd_regs;
+  // Faddeeva evaluation of the FP32 syntheses: 0 = the reference's regions
+  // and Alg-916, 1 = Weideman's 16-term rational series (FP64 plans: 0)
+  int faddeeva;
   double lambda0, bshift;
   double limits[9][2];
   double step[9];
@@ -99,6 +102,7 @@ struct VoigtK {
   T a, aa, inv_a, log_rmin0, sqrt_log_rmin0;
   T ema2, em2a2;  // exp(-a^2), exp(-2 a^2)
   int nmax, nfig;
+  int weid;  // FP32: Weideman's series (voigt_weideman_f32) in place of the regions
   T thr[5];
   const T *ea2n2;  // exp(-a^2 n^2), n = 0..49 (shared memory, per block)
   const T *e2an;   // exp(-2 a^2 n), n = 0..49 (shared memory, per block)
@@ -118,7 +122,7 @@ __device__ __forceinline__ void voigt_prepare(VoigtK<T> &K, T y, T *rden, int st
   K.inv_y = T(1) / y;
   K.rden = rden;
   K.rstride = stride;
-  if (sizeof(T) == sizeof(float) && rden) {
+  if (sizeof(T) == sizeof(float) && rden && !K.weid) {
 #pragma unroll 4
     for (int n = 0; n < kRden; n++) rden[n * stride] = T(1) / (K.aa * T(n * n) + K.yy);
   }
@@ -436,6 +440,53 @@ __device__ __forceinline__ HL<T> voigt_alg916(T nu, T y, T erfcx_y, const VoigtK
   return {re, nu > T(0) ? im : -im};
 }
 
+// Weideman's rational series for the Faddeeva function (J. A. C. Weideman,
+// "Computation of the complex error function", SIAM J. Numer. Anal. 31 (1994)
+// 1497-1518) with N = 16 terms, for Im z >= 0:
+//   L = (N / sqrt 2)^(1/2),  d = L - i z,  Z = (L + i z) / d,
+//   w(z) = 2 p(Z) / d^2 + 1 / (sqrt(pi) d),  p(Z) = sum_{n < N} c_n Z^n,
+// where c_1..c_N (here c_0..c_15) are the real parts of the discrete Fourier
+// transform (length 4N, divided by 4N) of f(t) = exp(-t^2) (L^2 + t^2) sampled
+// at t = L tan(theta / 2), theta = k pi / (2N), k = -2N+1 .. 2N-1, as the
+// paper constructs them.  In FP32 the result is within 6e-7 of w for every
+// z with Im z >= 0 (the evaluation's rounding; the series' own error at
+// N = 16 is 1.3e-7): no branch, one reciprocal, 4N multiply-adds.  The
+// coefficients, highest power first (me_weideman16 returns them to tests):
+#define ME_WEIDEMAN16_L 3.36358566101485856f
+#define ME_WEIDEMAN16(X)                                                               \
+  X(15, 9.939322536e-07f) X(14, 3.981287575e-06f) X(13, -5.584233411e-06f)            \
+  X(12, -2.734640462e-05f) X(11, 2.170986793e-05f) X(10, 2.107105640e-04f)             \
+  X(9, 8.703158428e-05f) X(8, -1.527659740e-03f) X(7, -3.881015189e-03f)               \
+  X(6, 3.682567317e-03f) X(5, 5.182240243e-02f) X(4, 1.912417267e-01f)                 \
+  X(3, 4.692909009e-01f) X(2, 8.864478302e-01f) X(1, 1.362240822e+00f)                 \
+  X(0, 1.748395886e+00f)
+
+__device__ __forceinline__ HL<float> voigt_weideman_f32(float nu, float y) {
+  constexpr float L = ME_WEIDEMAN16_L;
+  // 1 / d = conj(d) / |d|^2 with d = (L + y) - i nu
+  const float dre = L + y;
+  const float r = __fdividef(1.f, fmaf(dre, dre, nu * nu));
+  const float ire = dre * r, iim = nu * r;
+  // Z = (L + i z) / d, L + i z = (L - y) + i nu
+  const float nre = L - y;
+  const float zre = fmaf(nre, ire, -nu * iim), zim = fmaf(nre, iim, nu * ire);
+  float pre = 0.f, pim = 0.f;
+#define ME_WEID_STEP(n, c)                                   \
+  {                                                          \
+    const float t = fmaf(pre, zre, fmaf(-pim, zim, c));      \
+    pim = fmaf(pre, zim, pim * zre);                         \
+    pre = t;                                                 \
+  }
+  ME_WEIDEMAN16(ME_WEID_STEP)
+#undef ME_WEID_STEP
+  // 2 p / d^2 + (1 / sqrt(pi)) / d
+  const float i2re = fmaf(ire, ire, -iim * iim), i2im = 2.f * ire * iim;
+  const float rsp = float(1.0 / kSqrtPi);
+  const float h = fmaf(2.f, fmaf(pre, i2re, -pim * i2im), ire * rsp);
+  const float l = fmaf(2.f, fmaf(pre, i2im, pim * i2re), iim * rsp);
+  return {h, l};
+}
+
 // Reciprocal: the MUFU approximation on the FP32 path (<= 2 ulp), exact
 // division in FP64.
 __device__ __forceinline__ float rcp_t(float x) { return __fdividef(1.f, x); }
@@ -443,6 +494,9 @@ __device__ __forceinline__ double rcp_t(double x) { return 1.0 / x; }
 
 template <class T>
 __device__ __forceinline__ HL<T> voigt(T nu, T y, T erfcx_y, const VoigtK<T> &K) {
+  if constexpr (sizeof(T) == sizeof(float)) {
+    if (K.weid) return voigt_weideman_f32(nu, y);
+  }
   T H, L;
   if (nu == T(0)) {
     return {erfcx_y, T(0)};
@@ -536,6 +590,7 @@ __device__ __forceinline__ void voigt_block_setup(VoigtK<T> &K, const DevPlan &P
   K.em2a2 = T(exp(-2.0 * P.faa));
   K.nmax = P.fnmax;
   K.nfig = P.nfigures;
+  K.weid = sizeof(T) == sizeof(float) && P.faddeeva == 1;
 #pragma unroll
   for (int i = 0; i < 5; i++) K.thr[i] = T(P.thr[i]);
   K.ea2n2 = s_tab;

@@ -154,6 +154,7 @@ EXPORTED = [
     "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
     "me_mlp_set_gemm", "me_mlp_gemm_launches", "me_gemm_bf16", "me_plan_set_queue_order",
     "me_order_by_key", "me_plan_poll_trace", "me_plan_set_drain", "me_plan_get_drain",
+    "me_plan_faddeeva", "me_plan_set_faddeeva", "me_weideman16", "me_faddeeva_weideman",
 ]
 
 
@@ -167,7 +168,8 @@ class MeTuneResult(ctypes.Structure):
                 ("tail_slots", ctypes.c_int), ("svd_lanes", ctypes.c_int),
                 ("ms", ctypes.c_double), ("trials", ctypes.c_int),
                 ("kernel_variant", ctypes.c_int), ("svd_registers", ctypes.c_int),
-                ("group_fill", ctypes.c_int), ("drain_poll", ctypes.c_int)]
+                ("group_fill", ctypes.c_int), ("drain_poll", ctypes.c_int),
+                ("faddeeva", ctypes.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -269,6 +271,15 @@ def lib() -> ctypes.CDLL:
                                        ctypes.c_void_p, ctypes.POINTER(MeTuneResult)]
         L.me_plan_last_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint),
                                             ctypes.c_long]
+        L.me_plan_faddeeva.argtypes = [ctypes.c_void_p]
+        L.me_plan_faddeeva.restype = ctypes.c_int
+        L.me_plan_set_faddeeva.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_faddeeva.restype = None
+        L.me_weideman16.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.me_weideman16.restype = None
+        L.me_faddeeva_weideman.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.me_faddeeva_weideman.restype = ctypes.c_int
         L.me_plan_set_drain.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.me_plan_set_drain.restype = None
         L.me_plan_get_drain.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
@@ -513,6 +524,16 @@ class Plan:
         return r.as_dict()
 
     @property
+    def faddeeva(self) -> int:
+        """FP32 Faddeeva evaluation: 0 the reference's regions and Alg-916, 1
+        Weideman's 16-term series."""
+        return lib().me_plan_faddeeva(self._h)
+
+    @faddeeva.setter
+    def faddeeva(self, mode: int):
+        lib().me_plan_set_faddeeva(self._h, int(mode))
+
+    @property
     def drain(self) -> tuple:
         """(group_fill, poll_rounds) of the rounds after the queue drains."""
         f, r = ctypes.c_int(), ctypes.c_int()
@@ -658,6 +679,25 @@ def faddeeva(nfigures: int, nu: np.ndarray, a: np.ndarray, precision: int = ME_P
     _check(lib().me_faddeeva(nfigures, precision, _ptr(nu), _ptr(a), nu.size, _ptr(H), _ptr(L),
                              device), "me_faddeeva")
     return H, L
+
+
+def faddeeva_weideman(nu: np.ndarray, a: np.ndarray, device: int = 0):
+    """w(nu + i a) by Weideman's 16-term series in FP32 on the device: (H, L)."""
+    nu = np.ascontiguousarray(nu, dtype=np.float64).ravel()
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    H = np.zeros_like(nu)
+    L = np.zeros_like(nu)
+    _check(lib().me_faddeeva_weideman(_ptr(nu), _ptr(a), nu.size, _ptr(H), _ptr(L), device),
+           "me_faddeeva_weideman")
+    return H, L
+
+
+def weideman16():
+    """(c_0..c_15, L) of the FP32 Weideman series the library evaluates."""
+    c = np.zeros(16, dtype=np.float32)
+    L = ctypes.c_float()
+    lib().me_weideman16(c.ctypes.data_as(ctypes.c_void_p), ctypes.byref(L))
+    return c, L.value
 
 
 def invert_device_noalloc(cfg: MeConfig, wavelengths: np.ndarray, d_prof: int, npix: int,

@@ -78,7 +78,7 @@ def cfg0_map():
 # three run most of the LM steps)
 MODES = {"threads": (1, 0, 1, 1), "lane_split": (32, 0, 4, 1),
          "lane_split_svd_regs": (32, 0, 1, 2), "tail_kernel": (1, -1, 1, 1),
-         "lane_split_half_wave": (32, -1, 1, 1)}
+         "lane_split_half_wave": (32, -1, 1, 1), "faddeeva_regions": (32, -1, 1, 0)}
 # lanes and check interval after the queue drains (me_plan_set_drain), where
 # a mode sets them: half a wave and checks every 8 rounds
 DRAIN = {"lane_split_half_wave": (1, 8)}
@@ -94,6 +94,12 @@ def test_inversion_parity_vs_oracle(cfg0_map, prec, mode):
         if mode in DRAIN:
             plan.drain = DRAIN[mode]
             assert plan.drain == DRAIN[mode]
+        # FP32 plans evaluate the Faddeeva function by Weideman's series unless
+        # set to the reference's regions; FP64 plans always use the regions
+        assert plan.faddeeva == (1 if prec == "FP32" else 0)
+        if mode == "faddeeva_regions":
+            plan.faddeeva = 0
+            assert plan.faddeeva == 0
         res, stats = invert_chunks(plan, m["prof"])
     for st in stats:
         tail_launches = st["launches"] - 4 * st["rounds"]
@@ -288,6 +294,7 @@ def test_autotune_picks_a_setting_and_keeps_results_valid():
         assert (plan.window, plan.max_group, plan.tail_slots, plan.svd_lanes) == \
             (r["window"], r["max_group"], r["tail_slots"], r["svd_lanes"])
         assert r["group_fill"] in (1, 2, 4, 8) and r["drain_poll"] in (2, 4, 8)
+        assert r["faddeeva"] in (0, 1) and plan.faddeeva == r["faddeeva"]
         assert plan.drain == (r["group_fill"], r["drain_poll"])
         res, st = plan.invert(prof)
         assert st["valid"] == prof.shape[0] and (res[:, 9] > 0).all()
