@@ -274,8 +274,8 @@ int me_plan_poll_trace(const me_plan *plan, me_poll_record *out, int cap);
  * for skipped pixels.  npix at most the last batch's. */
 int me_plan_last_counters(const me_plan *plan, unsigned int *counters, long npix);
 
-/* Variant of the one-thread-per-pixel Jacobian and trial kernels (default:
- * 5 on FP32 plans, 0 on FP64 plans): 0 = 128 pixels per CTA, the wavelength
+/* Variant of the one-thread-per-pixel Jacobian and trial kernels (default
+ * 0): 0 = 128 pixels per CTA, the wavelength
  * grid read through the L1 cache, the FP32 Faddeeva (Alg-916) series terms
  * 1 / (a^2 n^2 + y^2) from a per-synthesis table in shared memory; 1 = 64 and 2 = 256 pixels per CTA; 3 = the grid
  * staged in shared memory per CTA; 4 = no table, each term's correctly
@@ -296,6 +296,15 @@ void me_plan_set_kernel_variant(me_plan *plan, int variant);
  * always use 0, the reference's method. */
 int me_plan_faddeeva(const me_plan *plan);
 void me_plan_set_faddeeva(me_plan *plan, int mode);
+/* How an FP32 plan's 9x9 SVD solves form the Givens rotations of their QR
+ * sweeps: 1 (default) = the radius z = sqrt(a^2 + b^2) and its reciprocal from
+ * one reciprocal square root (each within two ulps of the correctly rounded
+ * values; a third of the dependent latency of a square root and a division);
+ * 0 = the reference's pythag and division (SVD_TEMPLATE.h).  The SVD and the
+ * chi^2 stay FP64; results agree with mode 0 to rounding.  FP64 plans always
+ * use 0, so they stay bit-exact with the reference's arithmetic. */
+int me_plan_givens(const me_plan *plan);
+void me_plan_set_givens(me_plan *plan, int mode);
 /* The coefficients c_0..c_15 and the scale L of that series, for checking. */
 void me_weideman16(float *coef, float *L);
 /* w(nu + i a) by that series in FP32 on the device: H = Re w, L = Im w. */

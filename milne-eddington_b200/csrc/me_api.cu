@@ -228,8 +228,9 @@ int build_devplan(const me_config *cfg, const double *lambda, int nl, DevPlan &P
   // shared-memory SVD; on the FP32 path the Jacobian kernel with its sums in
   // shared memory
   P.svd_regs = 0;
-  P.kvar = cfg->precision == ME_PREC_FP64 ? 0 : 5;
+  P.kvar = 0;
   P.faddeeva = cfg->precision == ME_PREC_FP32 ? 1 : 0;
+  P.fastg = cfg->precision == ME_PREC_FP32 ? 1 : 0;
   P.ncut = nl / 5;
   const double c = 299792458.0;
   double t = (lambda[P.ncut] - lam0) * c / 1e3;  // the reference omits /lambda0 here
@@ -548,6 +549,10 @@ extern "C" void me_plan_set_kernel_variant(me_plan *p, int v) {
 extern "C" int me_plan_faddeeva(const me_plan *p) { return p ? p->P.faddeeva : 0; }
 extern "C" void me_plan_set_faddeeva(me_plan *p, int mode) {
   if (p) p->P.faddeeva = (mode == 1 && p->precision == ME_PREC_FP32) ? 1 : 0;
+}
+extern "C" int me_plan_givens(const me_plan *p) { return p ? p->P.fastg : 0; }
+extern "C" void me_plan_set_givens(me_plan *p, int mode) {
+  if (p) p->P.fastg = (mode == 1 && p->precision == ME_PREC_FP32) ? 1 : 0;
 }
 extern "C" void me_weideman16(float *coef, float *L) {
 #define ME_WEID_COPY(n, c) \

@@ -48,6 +48,9 @@ struct DevPlan {
   // Faddeeva evaluation of the FP32 syntheses: 0 = the reference's regions
   // and Alg-916, 1 = Weideman's 16-term rational series (FP64 plans: 0)
   int faddeeva;
+  // Givens rotations of the SVD's QR sweeps from one reciprocal square root
+  // (givens_radius<true>; FP32 plans) or as the reference forms them (FP64)
+  int fastg;
   double lambda0, bshift;
   double limits[9][2];
   double step[9];
@@ -1104,6 +1107,28 @@ __device__ __forceinline__ double pythag_d(double a, double b) {
   return mx * sqrt(1.0 + r * r);
 }
 
+// The radius z = pythag(a, b) of a Givens rotation of the QR sweeps and its
+// reciprocal 1 / z, from which the rotation's cosine and sine follow.  FAST:
+// both from one reciprocal square root, z = q rsqrt(q) and 1 / z = rsqrt(q)
+// with q = a^2 + b^2 -- each within two ulps of the correctly rounded square
+// root and quotient, and a third of their dependent latency -- while q lies
+// well inside the normal range; otherwise, and always when !FAST, pythag_d
+// and a division, as the reference computes them.
+template <bool FAST>
+__device__ __forceinline__ double givens_radius(double a, double b, double &inv) {
+  if constexpr (FAST) {
+    const double q = a * a + b * b;
+    if (q > 1e-290 && q < 1e290) {
+      const double r = rsqrt(q);
+      inv = r;
+      return q * r;
+    }
+  }
+  const double z = pythag_d(a, b);
+  inv = 1.0 / z;
+  return z;
+}
+
 static __device__ __noinline__ int gr_svd(double *a, int n, double *w, double *v) {
 #define A_(i, j) a[(i) * n + (j)]
 #define V_(i, j) v[(i) * n + (j)]
@@ -1300,7 +1325,7 @@ static __device__ __noinline__ int gr_svd(double *a, int n, double *w, double *v
 // scalars that are reassigned before their next use), so U and w come out
 // identical.  Matrix element (i, j) lives at a[(i * n + j) * STR], w[i] at
 // w[i * STR], so one thread's matrix can sit in a column of shared memory.
-template <int STR>
+template <int STR, bool FAST = false>
 __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
 #define A_(i, j) a[((i) * n + (j)) * STR]
 #define W_(i) w[(i) * STR]
@@ -1400,11 +1425,11 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
           R_(i) = c * R_(i);
           if ((fabs(f) + anorm) == anorm) break;
           g = W_(i);
-          h = pythag_d(f, g);
+          double ih;
+          h = givens_radius<FAST>(f, g, ih);
           W_(i) = h;
-          h = 1.0 / h;
-          c = g * h;
-          s = -f * h;
+          c = g * ih;
+          s = -f * ih;
           for (int j = 0; j < m; j++) {
             y = A_(j, nm);
             z = A_(j, i);
@@ -1434,21 +1459,20 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
         y = W_(i);
         h = s * g;
         g *= c;
-        z = pythag_d(f, h);
+        double iz;
+        z = givens_radius<FAST>(f, h, iz);
         R_(j) = z;
-        const double iz = 1.0 / z;
         c = f * iz;
         s = h * iz;
         f = x * c + g * s;
         g = g * c - x * s;
         h = y * s;
         y *= c;
-        z = pythag_d(f, h);
+        z = givens_radius<FAST>(f, h, iz);
         W_(j) = z;
         if (z) {
-          z = 1.0 / z;
-          c = f * z;
-          s = h * z;
+          c = f * iz;
+          s = h * iz;
         }
         f = c * g + s * y;
         x = c * y - s * g;
@@ -1478,7 +1502,7 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
 // the QR chase) run redundantly in every lane on private copies.  The
 // arithmetic is gr_svd_u's operation for operation; only the latency
 // changes.  w [n] is private to the lane.  All lanes of the group call it.
-template <int G>
+template <int G, bool FAST = false>
 __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, unsigned mask) {
 #define A_(i, j) a[(i) * n + (j)]
 #define GSYNC()                  \
@@ -1594,11 +1618,11 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
           rv1[i] = c * rv1[i];
           if ((fabs(f) + anorm) == anorm) break;
           g = w[i];
-          h = pythag_d(f, g);
+          double ih;
+          h = givens_radius<FAST>(f, g, ih);
           w[i] = h;
-          h = 1.0 / h;
-          c = g * h;
-          s = -f * h;
+          c = g * ih;
+          s = -f * ih;
           for (int jj = lane; jj < m; jj += G) {
             const double yy = A_(jj, nm), zz = A_(jj, i);
             A_(jj, nm) = yy * c + zz * s;
@@ -1627,21 +1651,20 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
         y = w[i];
         h = s * g;
         g *= c;
-        z = pythag_d(f, h);
+        double iz;
+        z = givens_radius<FAST>(f, h, iz);
         rv1[j] = z;
-        const double iz = 1.0 / z;
         c = f * iz;
         s = h * iz;
         f = x * c + g * s;
         g = g * c - x * s;
         h = y * s;
         y *= c;
-        z = pythag_d(f, h);
+        z = givens_radius<FAST>(f, h, iz);
         w[j] = z;
         if (z) {
-          z = 1.0 / z;
-          c = f * z;
-          s = h * z;
+          c = f * iz;
+          s = h * iz;
         }
         f = c * g + s * y;
         x = c * y - s * g;
@@ -1673,6 +1696,7 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
 // gr_svd_u's (SVD_TEMPLATE.h:84-344 without V).  A NaN matrix, for which no
 // negligible entry is found, is left unrotated (the reference's loop would
 // index below the matrix there).
+template <bool FAST = false>
 __device__ __forceinline__ int gr_svd_u9(double (&A)[9][9], double (&w)[9]) {
   constexpr int n = 9, m = 9;
   double rv1[9];
@@ -1809,11 +1833,11 @@ __device__ __forceinline__ int gr_svd_u9(double (&A)[9][9], double (&w)[9]) {
                   stop = true;
                 } else {
                   const double gg = w[i];
-                  double h = pythag_d(f, gg);
+                  double ih;
+                  const double h = givens_radius<FAST>(f, gg, ih);
                   w[i] = h;
-                  h = 1.0 / h;
-                  c = gg * h;
-                  s = -f * h;
+                  c = gg * ih;
+                  s = -f * ih;
 #pragma unroll
                   for (int j = 0; j < m; j++) {
                     const double y = A[j][lc - 1], z = A[j][i];
@@ -1852,21 +1876,20 @@ __device__ __forceinline__ int gr_svd_u9(double (&A)[9][9], double (&w)[9]) {
           y = w[i];
           h = s * gq;
           gq *= c;
-          z = pythag_d(f, h);
+          double iz;
+          z = givens_radius<FAST>(f, h, iz);
           rv1[j] = z;
-          const double iz = 1.0 / z;
           c = f * iz;
           s = h * iz;
           f = x * c + gq * s;
           gq = gq * c - x * s;
           h = y * s;
           y *= c;
-          z = pythag_d(f, h);
+          z = givens_radius<FAST>(f, h, iz);
           w[j] = z;
           if (z) {
-            z = 1.0 / z;
-            c = f * z;
-            s = h * z;
+            c = f * iz;
+            s = h * iz;
           }
           f = c * gq + s * y;
           x = c * y - s * gq;

@@ -423,9 +423,10 @@ __device__ __forceinline__ int solve_slot(const DevPlan &P, const Slots &S, int 
   if (WARP) __syncwarp(mask);
   auto decompose = [&]() {
     if constexpr (WARP)
-      return gr_svd_u_grp<G>(a, n, w, lane, mask);
+      return P.fastg ? gr_svd_u_grp<G, true>(a, n, w, lane, mask)
+                     : gr_svd_u_grp<G, false>(a, n, w, lane, mask);
     else
-      return gr_svd_u<STR>(a, n, w, rv1);
+      return P.fastg ? gr_svd_u<STR, true>(a, n, w, rv1) : gr_svd_u<STR, false>(a, n, w, rv1);
   };
   if (tk == 1) {
     hits += decompose();
@@ -504,6 +505,7 @@ __device__ __forceinline__ void trial_params9(const DevPlan &P, const Slots &S, 
   store9(S.ptmp, W, s, ptmp);
 }
 
+template <bool FAST>
 __device__ __forceinline__ int solve_slot9(const DevPlan &P, const Slots &S, int s) {
   const int W = S.W;
   const int tk = S.tk[s];
@@ -527,7 +529,7 @@ __device__ __forceinline__ int solve_slot9(const DevPlan &P, const Slots &S, int
   for (int r = 0; r < 9; r++)
 #pragma unroll
     for (int c = 0; c < 9; c++) A[r][c] = S.hess[(size_t)(r * 9 + c) * W + s];
-  const int hits = gr_svd_u9(A, w);
+  const int hits = gr_svd_u9<FAST>(A, w);
 #pragma unroll
   for (int r = 0; r < 9; r++)
 #pragma unroll
@@ -827,6 +829,7 @@ static __global__ void __launch_bounds__(kSvdBlock) svd_kernel(const __grid_cons
 
 // svd_kernel for plans with all nine parameters free: each thread's matrix in
 // its registers (solve_slot9), no shared memory.
+template <bool FAST>
 static __global__ void __launch_bounds__(kSvdBlock) svd9_kernel(const __grid_constant__ DevPlan P,
                                                                 const __grid_constant__ InvertArgs A,
                                                                 const __grid_constant__ Slots S,
@@ -838,7 +841,7 @@ static __global__ void __launch_bounds__(kSvdBlock) svd9_kernel(const __grid_con
   for (int i = blockIdx.x * kSvdBlock + threadIdx.x; i < count; i += gridDim.x * kSvdBlock) {
     const int s = list[i];
     if (S.state[s] != SL_TRIAL) continue;
-    tl.svdlim += solve_slot9(P, S, s);
+    tl.svdlim += solve_slot9<FAST>(P, S, s);
   }
   tl.flush(A, S);
 }
@@ -1320,7 +1323,10 @@ int round_grid_impl(int which, int device) {
     cudaFuncSetAttribute(svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSvdSmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, svd_kernel, kSvdBlock, kSvdSmem);
     int per_sm9 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm9, svd9_kernel, kSvdBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm9, svd9_kernel<false>, kSvdBlock, 0);
+    int per_sm9f = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm9f, svd9_kernel<true>, kSvdBlock, 0);
+    if (per_sm9f > per_sm9) per_sm9 = per_sm9f;
     if (per_sm9 > per_sm) per_sm = per_sm9;
   }
   if (per_sm < 1) per_sm = 1;
@@ -1339,8 +1345,10 @@ static inline void launch_svd_lanes(int lanes, const DevPlan &P, const InvertArg
     case 4: svd_grp_kernel<4><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
     case 8: svd_grp_kernel<8><<<grid, kBlock, 0, st>>>(P, A, S, parity, which); break;
     default:
-      if (P.npar == 9 && P.svd_regs)
-        svd9_kernel<<<grid, kSvdBlock, 0, st>>>(P, A, S, parity, which);
+      if (P.npar == 9 && P.svd_regs && P.fastg)
+        svd9_kernel<true><<<grid, kSvdBlock, 0, st>>>(P, A, S, parity, which);
+      else if (P.npar == 9 && P.svd_regs)
+        svd9_kernel<false><<<grid, kSvdBlock, 0, st>>>(P, A, S, parity, which);
       else
         svd_kernel<<<grid, kSvdBlock, kSvdSmem, st>>>(P, A, S, parity, which);
       break;
@@ -1418,8 +1426,10 @@ cudaError_t launch_round_impl(const DevPlan &P, const InvertArgs &A, const Slots
 template <int G>
 static inline void launch_svd_grp(const DevPlan &P, const InvertArgs &A, const Slots &S,
                                   int parity, int which, int grid, cudaStream_t st) {
-  if (P.npar == 9 && P.svd_regs == 2)
-    svd9_kernel<<<grid * (kBlock / kSvdBlock), kSvdBlock, 0, st>>>(P, A, S, parity, which);
+  if (P.npar == 9 && P.svd_regs == 2 && P.fastg)
+    svd9_kernel<true><<<grid * (kBlock / kSvdBlock), kSvdBlock, 0, st>>>(P, A, S, parity, which);
+  else if (P.npar == 9 && P.svd_regs == 2)
+    svd9_kernel<false><<<grid * (kBlock / kSvdBlock), kSvdBlock, 0, st>>>(P, A, S, parity, which);
   else
     svd_grp_kernel<G><<<grid, kBlock, 0, st>>>(P, A, S, parity, which);
 }

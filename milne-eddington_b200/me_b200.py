@@ -154,7 +154,7 @@ EXPORTED = [
     "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
     "me_mlp_set_gemm", "me_mlp_gemm_launches", "me_gemm_bf16", "me_plan_set_queue_order",
     "me_order_by_key", "me_plan_poll_trace", "me_plan_set_drain", "me_plan_get_drain",
-    "me_plan_faddeeva", "me_plan_set_faddeeva", "me_weideman16", "me_faddeeva_weideman",
+    "me_plan_faddeeva", "me_plan_set_faddeeva", "me_plan_givens", "me_plan_set_givens", "me_weideman16", "me_faddeeva_weideman",
 ]
 
 
@@ -271,6 +271,10 @@ def lib() -> ctypes.CDLL:
                                        ctypes.c_void_p, ctypes.POINTER(MeTuneResult)]
         L.me_plan_last_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint),
                                             ctypes.c_long]
+        L.me_plan_givens.argtypes = [ctypes.c_void_p]
+        L.me_plan_givens.restype = ctypes.c_int
+        L.me_plan_set_givens.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_givens.restype = None
         L.me_plan_faddeeva.argtypes = [ctypes.c_void_p]
         L.me_plan_faddeeva.restype = ctypes.c_int
         L.me_plan_set_faddeeva.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -522,6 +526,16 @@ class Plan:
                                       ctypes.c_void_p(stream) if stream else None,
                                       ctypes.byref(r)), "me_plan_autotune")
         return r.as_dict()
+
+    @property
+    def givens(self) -> int:
+        """FP32 plans' SVD Givens rotations: 1 from one reciprocal square root,
+        0 the reference's pythag and division."""
+        return lib().me_plan_givens(self._h)
+
+    @givens.setter
+    def givens(self, mode: int):
+        lib().me_plan_set_givens(self._h, int(mode))
 
     @property
     def faddeeva(self) -> int:

@@ -78,7 +78,8 @@ def cfg0_map():
 # three run most of the LM steps)
 MODES = {"threads": (1, 0, 1, 1), "lane_split": (32, 0, 4, 1),
          "lane_split_svd_regs": (32, 0, 1, 2), "tail_kernel": (1, -1, 1, 1),
-         "lane_split_half_wave": (32, -1, 1, 1), "faddeeva_regions": (32, -1, 1, 0)}
+         "lane_split_half_wave": (32, -1, 1, 1), "faddeeva_regions": (32, -1, 1, 0),
+         "givens_reference": (32, -1, 1, 1)}
 # lanes and check interval after the queue drains (me_plan_set_drain), where
 # a mode sets them: half a wave and checks every 8 rounds
 DRAIN = {"lane_split_half_wave": (1, 8)}
@@ -100,6 +101,12 @@ def test_inversion_parity_vs_oracle(cfg0_map, prec, mode):
         if mode == "faddeeva_regions":
             plan.faddeeva = 0
             assert plan.faddeeva == 0
+        # FP32 plans form the SVD's Givens rotations from a reciprocal square
+        # root unless set to the reference's pythag and division
+        assert plan.givens == (1 if prec == "FP32" else 0)
+        if mode == "givens_reference":
+            plan.givens = 0
+            assert plan.givens == 0
         res, stats = invert_chunks(plan, m["prof"])
     for st in stats:
         tail_launches = st["launches"] - 4 * st["rounds"]
