@@ -305,6 +305,13 @@ void me_plan_set_faddeeva(me_plan *plan, int mode);
  * use 0, so they stay bit-exact with the reference's arithmetic. */
 int me_plan_givens(const me_plan *plan);
 void me_plan_set_givens(me_plan *plan, int mode);
+/* 1: the one-thread-per-pixel Jacobian and trial kernels read each pixel's
+ * observed profile from a slot-major copy made when the pixel enters a slot
+ * (4 nl doubles per slot in flight), so that a warp's reads are coalesced;
+ * 0 (default): from the pixel's rows of the map.  Same values, same results.
+ * The copy pays when pixels take many trials (the plain LM: 7 % faster per
+ * batch) and costs a little when most end after a learned start. */
+void me_plan_set_slot_profiles(me_plan *plan, int on);
 /* The coefficients c_0..c_15 and the scale L of that series, for checking. */
 void me_weideman16(float *coef, float *L);
 /* w(nu + i a) by that series in FP32 on the device: H = Re w, L = Im w. */
@@ -319,8 +326,9 @@ int me_faddeeva_weideman(const double *nu, const double *a, long n, double *H, d
  * kernel variant (pixels per CTA, grid staging, Faddeeva series reciprocals;
  * me_plan_set_kernel_variant), where the SVD keeps its matrix
  * (me_plan_set_svd_registers), the lanes and check interval after the
- * queue drains (me_plan_set_drain) and the FP32 Faddeeva evaluation
- * (me_plan_set_faddeeva) -- one knob at a time, keeping each
+ * queue drains (me_plan_set_drain), the FP32 Faddeeva evaluation
+ * (me_plan_set_faddeeva) and the slot-major profile copy
+ * (me_plan_set_slot_profiles) -- one knob at a time, keeping each
  * improvement, and leaves the best setting on the plan.  The carried LM chi^2 is restored afterwards.  out (may be NULL)
  * receives the choice, its time and the number of timed runs. */
 typedef struct me_tune_result {
@@ -330,6 +338,7 @@ typedef struct me_tune_result {
   int kernel_variant, svd_registers;  /* me_plan_set_kernel_variant / _svd_registers */
   int group_fill, drain_poll;         /* me_plan_set_drain */
   int faddeeva;                       /* me_plan_set_faddeeva */
+  int slot_profiles;                  /* me_plan_set_slot_profiles */
 } me_tune_result;
 int me_plan_autotune(me_plan *plan, const double *d_prof, long npix, void *stream,
                      me_tune_result *out);

@@ -108,6 +108,11 @@ struct me_plan {
   int slots_w = 0;         // allocated slot count
   DevBuf d_slot_pix, d_slot_i32, d_slot_cnt, d_slot_u8, d_slot_sc, d_slot_vec, d_slot_hess,
       d_slot_list, d_slot_small;
+  // the slot-major copy of the slots' observed profiles (me::Slots::obs;
+  // me_plan_set_slot_profiles), sized for obs_w slots
+  int slot_obs = 0;
+  int obs_w = 0;
+  DevBuf d_slot_obs;
   int grid_jac = 0, grid_trial = 0, grid_svd = 0, grid_fin = 0;
   // pixels in flight at or below which, with the queue empty, the tail kernel
   // finishes the batch (-1: half a wave of its warps; 0: rounds only)
@@ -550,6 +555,9 @@ extern "C" int me_plan_faddeeva(const me_plan *p) { return p ? p->P.faddeeva : 0
 extern "C" void me_plan_set_faddeeva(me_plan *p, int mode) {
   if (p) p->P.faddeeva = (mode == 1 && p->precision == ME_PREC_FP32) ? 1 : 0;
 }
+extern "C" void me_plan_set_slot_profiles(me_plan *p, int on) {
+  if (p) p->slot_obs = on != 0 ? 1 : 0;
+}
 extern "C" int me_plan_givens(const me_plan *p) { return p ? p->P.fastg : 0; }
 extern "C" void me_plan_set_givens(me_plan *p, int mode) {
   if (p) p->P.fastg = (mode == 1 && p->precision == ME_PREC_FP32) ? 1 : 0;
@@ -655,6 +663,14 @@ int ensure_slots(me_plan *p, int W, me::Slots &S) {
   S.jcount = small;
   S.rcount = small + 2;
   S.busy = small + 4;
+  S.obs = nullptr;
+  if (p->slot_obs) {
+    if (W > p->obs_w) {
+      CK(p->d_slot_obs.ensure(w * 4 * (size_t)p->P.nl * sizeof(double)));
+      p->obs_w = W;
+    }
+    S.obs = p->d_slot_obs.as<double>();
+  }
   return ME_OK;
 }
 
@@ -1518,6 +1534,8 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
       // the FP32 syntheses' Faddeeva evaluation: the reference's regions and
       // Alg-916, or Weideman's series (FP64 plans keep the former)
       {&p->P.faddeeva, {0, p->precision == ME_PREC_FP32 ? 1 : 0}},
+      // the observed profiles read from a slot-major copy made at refill
+      {&p->slot_obs, {0, 1}},
   };
   for (Knob &k : knobs) {
     if (rc) break;
@@ -1553,6 +1571,7 @@ extern "C" int me_plan_autotune(me_plan *p, const double *d_prof, long npix, voi
     out->group_fill = p->group_fill;
     out->drain_poll = p->drain_poll;
     out->faddeeva = p->P.faddeeva;
+    out->slot_profiles = p->slot_obs;
   }
   return ME_OK;
 }

@@ -34,12 +34,14 @@ namespace detail {
 // sw[s] = weight_s / sqrt(norm0): sum (J sw)(J sw) = J^T W J with
 // W = weight^2 / norm0 (Noise_Init, Src/ME_SOLVER.c:410-441).  H45 = upper
 // triangle of the full 9x9 (row-major, i <= j), g9 = -J^T W r; returns
-// sum (r sw)^2 / (4 nl) accumulated in FP64.
+// sum (r sw)^2 / (4 nl) accumulated in FP64.  The observed value of Stokes s
+// at wavelength iw is prof[(s nl + iw) pstr]: pstr 1 for a pixel's rows of the
+// input map, W for a slot's column of the slot-major copy (Slots::obs).
 template <class T, bool FILT>
 __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                              const double *par, const double *step,
                                              const double *prof, const double sw[4], double *H45,
-                                             double *g9, const T *sgrid = nullptr) {
+                                             double *g9, const T *sgrid = nullptr, int pstr = 1) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
   c.grid = sgrid;
@@ -59,7 +61,7 @@ __device__ __forceinline__ double deriv_pass(const DevPlan &P, VoigtK<T> &K, T *
     T r[4];
 #pragma unroll
     for (int s = 0; s < 4; s++) {
-      const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+      const double rd = ((double)syn[s] - __ldg(prof + (size_t)(s * nl + iw) * pstr)) * sw[s];
       chi += rd * rd;
       r[s] = T(rd);
     }
@@ -90,7 +92,7 @@ __device__ __forceinline__ double deriv_pass_sacc(const DevPlan &P, VoigtK<T> &K
                                                   const double *par, const double *step,
                                                   const double *prof, const double sw[4],
                                                   double *H45, double *g9, const T *sgrid,
-                                                  T *acc) {
+                                                  T *acc, int pstr = 1) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
   c.grid = sgrid;
@@ -107,7 +109,7 @@ __device__ __forceinline__ double deriv_pass_sacc(const DevPlan &P, VoigtK<T> &K
     T r[4];
 #pragma unroll
     for (int s = 0; s < 4; s++) {
-      const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+      const double rd = ((double)syn[s] - __ldg(prof + (size_t)(s * nl + iw) * pstr)) * sw[s];
       chi += rd * rd;
       r[s] = T(rd);
     }
@@ -136,7 +138,7 @@ template <class T, bool FILT>
 __device__ __forceinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T *rden,
                                             const double *par, const double *step,
                                             const double *prof, const double sw[4],
-                                            double *fit, const T *sgrid = nullptr) {
+                                            double *fit, const T *sgrid = nullptr, int pstr = 1) {
   SynthCall<T> c;
   synth_setup<T>(c, par, P, step);
   c.grid = sgrid;
@@ -151,7 +153,7 @@ __device__ __forceinline__ double forward_pass(const DevPlan &P, VoigtK<T> &K, T
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       if (prof) {
-        const double rd = ((double)syn[s] - __ldg(prof + s * nl + iw)) * sw[s];
+        const double rd = ((double)syn[s] - __ldg(prof + (size_t)(s * nl + iw) * pstr)) * sw[s];
         chi += rd * rd;
       }
       if (fit) fit[s * nl + iw] = (double)syn[s];
@@ -237,6 +239,8 @@ static __device__ int refill(const DevPlan &P, const InvertArgs &A, const Slots 
     t_valid++;
     S.pix[s] = pix;
     S.it[s] = 0;
+    if (S.obs)
+      for (int i = 0; i < 4 * nl; i++) S.obs[(size_t)i * W + s] = pp[i];
     store9(S.guess, W, s, pin.guess);
     if (A.init_par) {
       // learned start: the free parameters from the initialiser, folded into
@@ -783,15 +787,16 @@ __global__ void __launch_bounds__(BLOCK, SACC ? 3 : ME_JAC_MINB * kBlock / BLOCK
   Tally t;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const int s = S.jlist[parity * W + i];
-    const double *pp = A.prof + (size_t)S.pix[s] * 4 * nl;
+    const double *pp = S.obs ? S.obs + s : A.prof + (size_t)S.pix[s] * 4 * nl;
+    const int pstr = S.obs ? W : 1;
     double par[9], step[9], sw[4];
     load9(S.par, W, s, par);
     slot_weights(P, S, s, step, sw);
     double H45[45], g9[9];
     const double chi0 =
         SACC ? deriv_pass_sacc<T, FILT, BLOCK>(P, K, rden, par, step, pp, sw, H45, g9, sgrid,
-                                               s_acc + threadIdx.x)
-             : deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9, sgrid);
+                                               s_acc + threadIdx.x, pstr)
+             : deriv_pass<T, FILT>(P, K, rden, par, step, pp, sw, H45, g9, sgrid, pstr);
     t.jac++;
     jac_store<sizeof(T) == sizeof(float)>(P, S, s, par, chi0, H45, g9);
   }
@@ -884,8 +889,11 @@ __global__ void __launch_bounds__(BLOCK) trial_kernel(const __grid_constant__ De
       double ptmp[9], step[9], sw[4];
       load9(S.ptmp, W, s, ptmp);
       slot_weights(P, S, s, step, sw);
-      chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl, sw,
-                                      nullptr, sgrid);
+      if (S.obs)
+        chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, S.obs + s, sw, nullptr, sgrid, W);
+      else
+        chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl,
+                                        sw, nullptr, sgrid);
     }
     trial_transition<true>(P, A, S, s, st, chi_new, next_parity, t);
   }

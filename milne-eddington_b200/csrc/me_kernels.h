@@ -80,6 +80,10 @@ struct Slots {
   int *rlist;                // [2][W] slots going on to another trial after a rejected one
   int *rcount;               // [2]
   int *busy;                 // slots holding a pixel
+  // [4 nl][W]: the observed profile of each slot's pixel, slot-major, copied
+  // at refill so that the one-thread-per-slot kernels read it coalesced
+  // (null: they read the pixel's rows of the input map)
+  double *obs;
 };
 
 // An upper bound on the LM steps (syntheses with Jacobian + trial steps) of

@@ -236,6 +236,7 @@ extern "C" int me_invert_batch_device_noalloc(const me_config *cfg, const double
   S.jcount = d_small->jcount;
   S.rcount = d_small->rcount;
   S.busy = &d_small->busy;
+  S.obs = nullptr;  // the kernels read the pixels' rows of the map
   // (the kernels index the [k][W] arrays with the active slot count W as
   // their stride; with W < kSlots each region is used densely from its start)
 

@@ -154,7 +154,8 @@ EXPORTED = [
     "me_run_options_default", "me_run", "me_run_config", "me_plan_set_filter",
     "me_mlp_set_gemm", "me_mlp_gemm_launches", "me_gemm_bf16", "me_plan_set_queue_order",
     "me_order_by_key", "me_plan_poll_trace", "me_plan_set_drain", "me_plan_get_drain",
-    "me_plan_faddeeva", "me_plan_set_faddeeva", "me_plan_givens", "me_plan_set_givens", "me_weideman16", "me_faddeeva_weideman",
+    "me_plan_faddeeva", "me_plan_set_faddeeva", "me_plan_givens", "me_plan_set_givens",
+    "me_plan_set_slot_profiles", "me_weideman16", "me_faddeeva_weideman",
 ]
 
 
@@ -169,7 +170,7 @@ class MeTuneResult(ctypes.Structure):
                 ("ms", ctypes.c_double), ("trials", ctypes.c_int),
                 ("kernel_variant", ctypes.c_int), ("svd_registers", ctypes.c_int),
                 ("group_fill", ctypes.c_int), ("drain_poll", ctypes.c_int),
-                ("faddeeva", ctypes.c_int)]
+                ("faddeeva", ctypes.c_int), ("slot_profiles", ctypes.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -271,6 +272,8 @@ def lib() -> ctypes.CDLL:
                                        ctypes.c_void_p, ctypes.POINTER(MeTuneResult)]
         L.me_plan_last_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint),
                                             ctypes.c_long]
+        L.me_plan_set_slot_profiles.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.me_plan_set_slot_profiles.restype = None
         L.me_plan_givens.argtypes = [ctypes.c_void_p]
         L.me_plan_givens.restype = ctypes.c_int
         L.me_plan_set_givens.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -526,6 +529,10 @@ class Plan:
                                       ctypes.c_void_p(stream) if stream else None,
                                       ctypes.byref(r)), "me_plan_autotune")
         return r.as_dict()
+
+    def set_slot_profiles(self, on: bool):
+        """Kernels read the observed profiles from a slot-major copy (default off)."""
+        lib().me_plan_set_slot_profiles(self._h, int(bool(on)))
 
     @property
     def givens(self) -> int:

@@ -302,6 +302,7 @@ def test_autotune_picks_a_setting_and_keeps_results_valid():
             (r["window"], r["max_group"], r["tail_slots"], r["svd_lanes"])
         assert r["group_fill"] in (1, 2, 4, 8) and r["drain_poll"] in (2, 4, 8)
         assert r["faddeeva"] in (0, 1) and plan.faddeeva == r["faddeeva"]
+        assert r["slot_profiles"] in (0, 1)
         assert plan.drain == (r["group_fill"], r["drain_poll"])
         res, st = plan.invert(prof)
         assert st["valid"] == prof.shape[0] and (res[:, 9] > 0).all()
@@ -334,3 +335,23 @@ def test_poll_trace_records_the_batch():
     # checks in the lane-split phase come every 2 rounds
     steps = {b["rounds"] - a["rounds"] for a, b in zip(tr, tr[1:-1]) if a["group"] > 1 and b["group"] > 1}
     assert steps <= {2}
+
+
+@pytest.mark.parametrize("prec", ["FP32", "FP64"])
+def test_slot_profiles_change_nothing(prec):
+    """me_plan_set_slot_profiles: the slot-major copy of the observed profiles
+    holds the same values, so the results are bit for bit those of the reads
+    from the map's rows."""
+    name = "fe15648_64x64"
+    lam = me_maps.wavelengths(name)
+    cfg = me_b200.parse_config_text(me_maps.control_text(name, precision=prec))
+    with me_b200.Plan(cfg, lam) as plan:
+        par = me_maps.draw_parameters(name, 4096, 63)
+        prof = me_maps.add_noise(plan.synthesize(par), 1e-3, 63)
+        plan.window, plan.max_group = 1024, 1  # one thread per pixel, refills throughout
+        out = {}
+        for on in (False, True):
+            plan.set_slot_profiles(on)
+            plan.carry_chisq = 0.0
+            out[on], _ = plan.invert(prof)
+    assert np.array_equal(out[False], out[True])
