@@ -889,11 +889,11 @@ __global__ void __launch_bounds__(BLOCK) trial_kernel(const __grid_constant__ De
       double ptmp[9], step[9], sw[4];
       load9(S.ptmp, W, s, ptmp);
       slot_weights(P, S, s, step, sw);
-      if (S.obs)
-        chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, S.obs + s, sw, nullptr, sgrid, W);
-      else
-        chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, A.prof + (size_t)S.pix[s] * 4 * nl,
-                                        sw, nullptr, sgrid);
+      // one call site, so that both sources of the observed values run the
+      // same compiled synthesis
+      const double *pp = S.obs ? S.obs + s : A.prof + (size_t)S.pix[s] * 4 * nl;
+      chi_new = forward_pass<T, FILT>(P, K, rden, ptmp, step, pp, sw, nullptr, sgrid,
+                                      S.obs ? W : 1);
     }
     trial_transition<true>(P, A, S, s, st, chi_new, next_parity, t);
   }
