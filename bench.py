@@ -366,8 +366,8 @@ def event_flops(fc, nl, jacobians, trials):
 def kernel_rooflines(st, fc, nl, peak, peak64):
     """Per-kernel algorithmic FLOP/s from a profiled batch (me_plan_set_profiling):
     the round kernels over the events the rounds did, the tail kernel over
-    the rest.  frac: of the FP32 peak; the SVD solve (FP64 arithmetic) also
-    against the FP64 peak."""
+    the rest.  frac: of the FP32 peak; frac_of_fp64_peak: of the FP64 peak,
+    the one that bounds the SVD solve (FP64 arithmetic)."""
     tj, tt = st["tail_jacobians"], st["tail_trials"]
     rounds = event_flops(fc, nl, st["jacobians"] - tj, st["trials"] - tt)
     tail = event_flops(fc, nl, tj, tt)
@@ -379,7 +379,7 @@ def kernel_rooflines(st, fc, nl, peak, peak64):
         if ms > 0:
             tf = fl / (ms / 1e3) / 1e12
             out[name] = {"ms": ms, "algorithmic_flop": fl, "tflops": tf, "frac": tf / peak}
-            if name == "svd_kernel" and peak64:
+            if peak64:
                 out[name]["frac_of_fp64_peak"] = tf / peak64
     return out
 
@@ -978,6 +978,10 @@ def main():
             "param_err_vs_fp64_ref_median_p99": out["err_vs_ref"],
             "param_err_vs_truth_median_p99": out["err_vs_truth"],
             "ref_param_err_vs_truth_median_p99": out["err_vs_truth_ref"]})
+        # the SVD solve computes in FP64: its roofline is the FP64 rate
+        top_is64 = out["top"] == "svd_kernel" and bool(out["peak64"])
+        top_bound = "fp64" if top_is64 else "fp32"
+        top_peak = out["peak64"] if top_is64 else out["peak"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
@@ -992,18 +996,19 @@ def main():
             "parity_all_pass": parity["all_pass"] if parity else None,
             "gpu_launches": int(sum(s["launches"] for s in stats)),
             "e2e": None, "clocks": out["clk"],
-            "roofline": {"bound": "fp32", "kernel": out["top"],
+            "roofline": {"bound": top_bound, "kernel": out["top"],
                          "achieved": out["kernels"][out["top"]]["tflops"],
-                         "peak": out["peak"], "unit": "TFLOP/s",
-                         "frac": out["kernels"][out["top"]]["frac"],
+                         "peak": top_peak, "unit": "TFLOP/s",
+                         "frac": out["kernels"][out["top"]]["tflops"] / top_peak,
                          "traffic": None,
                          "note": "dominant kernel by device time in a profiled step (CUDA "
                                  "events around every launch): algorithmic FLOPs of the "
                                  "reference algorithm for the events it ran (counted with a "
-                                 "counting scalar type) / its time; peak = FP32 FFMA rate "
-                                 "measured in this run with cuBLAS SGEMM, TF32 off "
-                                 "(MEASURED_PEAKS.json has no FP32 figure); the SVD solve is "
-                                 "also given against the FP64 DGEMM rate measured in this run",
+                                 "counting scalar type) / its time; peak = the rate of the "
+                                 "kernel's arithmetic measured in this run: FP32 FFMA (cuBLAS "
+                                 "SGEMM, TF32 off) for the synthesis kernels, FP64 (cuBLAS "
+                                 "DGEMM) for the SVD solve (MEASURED_PEAKS.json has neither); "
+                                 "every kernel against both in 'kernels'",
                          "fp64_peak": out["peak64"],
                          "kernels": out["kernels"],
                          "step_algorithmic_tflops": out["step_tflops"],

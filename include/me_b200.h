@@ -392,10 +392,24 @@ int me_faddeeva(int nfigures, int precision, const double *nu, const double *a, 
  * a = u * diag(w) * v^T.  Replaces svdcmp_double (Src/SVD_TEMPLATE.h:84-344). */
 int me_svd(const double *a, long nmat, int n, double *u, double *w, double *v, int device);
 
+/* The same decomposition as the inversion's trial-step solve runs it: U and w
+ * only (the operations on V left out; SVD_solve_mem, Src/LM_FIT.c:400-469,
+ * through svdcmp_double, Src/SVD_TEMPLATE.h:84-344), with `lanes` lanes per
+ * matrix (1, 2, 4, 8, 16 or 32: one thread, the lane-split rounds, the tail
+ * kernel) and the Givens rotations' radius from the reference's pythag and a
+ * division (fast = 0, FP64 plans) or from one reciprocal square root
+ * (fast = 1, FP32 plans).  u and w as me_svd's.  Returns the number of
+ * matrices whose QR sweeps hit the 50-sweep limit in *limit_hits (may be
+ * NULL). */
+int me_svd_u(const double *a, long nmat, int n, int lanes, int fast, double *u, double *w,
+             int *limit_hits, int device);
+
 /* Device-buffer variants (work ordered on `stream`, a cudaStream_t; NULL =
  * the default stream, waited for before returning). */
 int me_svd_device(const double *d_a, long nmat, int n, double *d_u, double *d_w, double *d_v,
                   void *stream);
+int me_svd_u_device(const double *d_a, long nmat, int n, int lanes, int fast, double *d_u,
+                    double *d_w, void *stream);
 int me_synthesize_jacobian_device(me_plan *plan, const double *d_par, long npix, double step7,
                                   double *d_prof, double *d_jac, void *stream);
 

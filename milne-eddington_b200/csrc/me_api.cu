@@ -1424,6 +1424,35 @@ extern "C" int me_svd(const double *a, long nmat, int n, double *u, double *w, d
   return ME_OK;
 }
 
+extern "C" int me_svd_u(const double *a, long nmat, int n, int lanes, int fast, double *u,
+                        double *w, int *limit_hits, int device) {
+  if (!a || !u || !w || nmat < 0 || n < 1 || n > 9) return fail(ME_ERR_ARG, "bad argument");
+  if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(ME_ERR_ARG, "lanes must be 1, 2, 4, 8, 16 or 32");
+  int st = check_device(device);
+  if (st) return st;
+  if (limit_hits) *limit_hits = 0;
+  if (nmat == 0) return ME_OK;
+  const size_t mb = (size_t)nmat * n * n * sizeof(double), wb = (size_t)nmat * n * sizeof(double);
+  DevBuf da, du, dw, dh;
+  CK(da.ensure(mb));
+  CK(du.ensure(mb));
+  CK(dw.ensure(wb));
+  CK(dh.ensure(sizeof(int)));
+  CK(cudaMemset(dh.p, 0, sizeof(int)));
+  CK(cudaMemcpy(da.p, a, mb, cudaMemcpyHostToDevice));
+  CK(me::launch_svd_u(da.as<double>(), nmat, n, lanes, fast ? 1 : 0, du.as<double>(),
+                      dw.as<double>(), dh.as<int>(), 0));
+  CK(cudaMemcpy(u, du.p, mb, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(w, dw.p, wb, cudaMemcpyDeviceToHost));
+  if (limit_hits) CK(cudaMemcpy(limit_hits, dh.p, sizeof(int), cudaMemcpyDeviceToHost));
+  da.release();
+  du.release();
+  dw.release();
+  dh.release();
+  return ME_OK;
+}
+
 extern "C" int me_init_guess(me_plan *p, const double *prof, long npix, double *guess,
                              double *extra, int *status) {
   if (!p || !prof || !guess || !extra || !status || npix < 0)
@@ -1456,6 +1485,17 @@ extern "C" int me_svd_device(const double *d_a, long nmat, int n, double *d_u, d
     return fail(ME_ERR_ARG, "bad argument");
   cudaStream_t st = (cudaStream_t)stream;
   CK(me::launch_svd(d_a, nmat, n, d_u, d_w, d_v, nullptr, st));
+  if (!stream) CK(cudaStreamSynchronize(st));
+  return ME_OK;
+}
+
+extern "C" int me_svd_u_device(const double *d_a, long nmat, int n, int lanes, int fast,
+                               double *d_u, double *d_w, void *stream) {
+  if (!d_a || !d_u || !d_w || nmat < 0 || n < 1 || n > 9) return fail(ME_ERR_ARG, "bad argument");
+  if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    return fail(ME_ERR_ARG, "lanes must be 1, 2, 4, 8, 16 or 32");
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(me::launch_svd_u(d_a, nmat, n, lanes, fast ? 1 : 0, d_u, d_w, nullptr, st));
   if (!stream) CK(cudaStreamSynchronize(st));
   return ME_OK;
 }

@@ -1129,6 +1129,21 @@ __device__ __forceinline__ double givens_radius(double a, double b, double &inv)
   return z;
 }
 
+// The chase's first rotation of each step: the reference divides by the
+// radius (c = f / z, s = h / z, SVD_TEMPLATE.h:305-306); FAST multiplies by
+// the reciprocal square root givens_radius gave.
+template <bool FAST>
+__device__ __forceinline__ void chase_cs(double f, double h, double z, double iz, double &c,
+                                         double &s) {
+  if constexpr (FAST) {
+    c = f * iz;
+    s = h * iz;
+  } else {
+    c = f / z;
+    s = h / z;
+  }
+}
+
 static __device__ __noinline__ int gr_svd(double *a, int n, double *w, double *v) {
 #define A_(i, j) a[(i) * n + (j)]
 #define V_(i, j) v[(i) * n + (j)]
@@ -1351,7 +1366,24 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
       h = f * g - s;
       A_(i, i) = f - g;
       const double ih = 1.0 / h;
-      for (int j = l; j < n; j++) {
+      // columns j and j + 1 side by side: two independent chains, each
+      // summed and updated in the order of the one-column loop
+      int j = l;
+      for (; j + 1 < n; j += 2) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int k = i; k < m; k++) {
+          const double aki = A_(k, i);
+          s0 += aki * A_(k, j);
+          s1 += aki * A_(k, j + 1);
+        }
+        const double f0 = s0 * ih, f1 = s1 * ih;
+        for (int k = i; k < m; k++) {
+          const double aki = A_(k, i);
+          A_(k, j) += f0 * aki;
+          A_(k, j + 1) += f1 * aki;
+        }
+      }
+      if (j < n) {
         s = 0.0;
         for (int k = i; k < m; k++) s += A_(k, i) * A_(k, j);
         f = s * ih;
@@ -1376,7 +1408,21 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
         A_(i, l) = f - g;
         const double ih = 1.0 / h;
         for (int k = l; k < n; k++) R_(k) = A_(i, k) * ih;
-        for (int j = l; j < m; j++) {
+        int j = l;
+        for (; j + 1 < m; j += 2) {  // rows j and j + 1 side by side
+          double s0 = 0.0, s1 = 0.0;
+          for (int k = l; k < n; k++) {
+            const double aik = A_(i, k);
+            s0 += A_(j, k) * aik;
+            s1 += A_(j + 1, k) * aik;
+          }
+          for (int k = l; k < n; k++) {
+            const double rk = R_(k);
+            A_(j, k) += s0 * rk;
+            A_(j + 1, k) += s1 * rk;
+          }
+        }
+        if (j < m) {
           s = 0.0;
           for (int k = l; k < n; k++) s += A_(j, k) * A_(i, k);
           for (int k = l; k < n; k++) A_(j, k) += s * R_(k);
@@ -1394,7 +1440,22 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
     if (g != 0.0) {
       g = 1.0 / g;
       const double iaii = 1.0 / A_(i, i);
-      for (int j = l; j < n; j++) {
+      int j = l;
+      for (; j + 1 < n; j += 2) {  // columns j and j + 1 side by side
+        double s0 = 0.0, s1 = 0.0;
+        for (int k = l; k < m; k++) {
+          const double aki = A_(k, i);
+          s0 += aki * A_(k, j);
+          s1 += aki * A_(k, j + 1);
+        }
+        const double f0 = (s0 * iaii) * g, f1 = (s1 * iaii) * g;
+        for (int k = i; k < m; k++) {
+          const double aki = A_(k, i);
+          A_(k, j) += f0 * aki;
+          A_(k, j + 1) += f1 * aki;
+        }
+      }
+      if (j < n) {
         s = 0.0;
         for (int k = l; k < m; k++) s += A_(k, i) * A_(k, j);
         f = (s * iaii) * g;
@@ -1462,8 +1523,7 @@ __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
         double iz;
         z = givens_radius<FAST>(f, h, iz);
         R_(j) = z;
-        c = f * iz;
-        s = h * iz;
+        chase_cs<FAST>(f, h, z, iz, c, s);
         f = x * c + g * s;
         g = g * c - x * s;
         h = y * s;
@@ -1509,92 +1569,110 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
   do {                           \
     if (G > 1) __syncwarp(mask); \
   } while (0)
+// k runs over 0 ... 8 unrolled, so that the column or row a lane holds stays in
+// registers; the predicate keeps the reference's range and order
+#define FOR9(k) _Pragma("unroll") for (int k = 0; k < 9; k++)
   const int m = n;
   int l = 0, nm = 0;
   double anorm = 0., c, f, g = 0., h, s, scale = 0., x, y, z;
   double rv1[9];
   int hit = 0;
+  // Householder reduction.  Every lane reads the column (then the row) being
+  // reduced into registers and scales it there, so the transforms of the
+  // other columns (rows) read it from registers; the scaled vector goes back
+  // to shared memory once, after the transforms: one synchronisation per
+  // column and per row.
   for (int i = 0; i < n; i++) {
     l = i + 1;
     rv1[i] = scale * g;
     g = s = scale = 0.0;
-    for (int k = i; k < m; k++) scale += fabs(A_(k, i));
+    double col[9];
+    FOR9(k) col[k] = (k >= i && k < m) ? A_(k, i) : 0.0;
+    FOR9(k) if (k >= i && k < m) scale += fabs(col[k]);
     if (scale) {
       const double is = 1.0 / scale;
-      for (int k = i; k < m; k++) {
-        const double t = A_(k, i) * is;
-        s += t * t;
+      FOR9(k) if (k >= i && k < m) {
+        col[k] *= is;
+        s += col[k] * col[k];
       }
       f = A_(i, i) * is;
       g = f >= 0 ? -sqrt(s) : sqrt(s);
       h = f * g - s;
-      GSYNC();
-      for (int k = i + lane; k < m; k += G) A_(k, i) = k == i ? f - g : A_(k, i) * is;
-      GSYNC();
+      FOR9(k) if (k == i) col[k] = f - g;
       const double ih = 1.0 / h;
       for (int j = l + lane; j < n; j += G) {
         double sj = 0.0;
-        for (int k = i; k < m; k++) sj += A_(k, i) * A_(k, j);
+        FOR9(k) if (k >= i && k < m) sj += col[k] * A_(k, j);
         const double fj = sj * ih;
-        for (int k = i; k < m; k++) A_(k, j) += fj * A_(k, i);
+        FOR9(k) if (k >= i && k < m) A_(k, j) += fj * col[k];
       }
       GSYNC();
-      for (int k = i + lane; k < m; k += G) A_(k, i) *= scale;
-      GSYNC();
+      FOR9(k) if (k >= i && k < m && ((k - i) & (G - 1)) == lane) A_(k, i) = col[k] * scale;
     }
     w[i] = scale * g;
     g = s = scale = 0.0;
     if (i != n - 1) {
-      for (int k = l; k < n; k++) scale += fabs(A_(i, k));
+      double row[9];
+      FOR9(k) row[k] = (k >= l && k < n) ? A_(i, k) : 0.0;
+      FOR9(k) if (k >= l && k < n) scale += fabs(row[k]);
       if (scale) {
         const double is = 1.0 / scale;
-        for (int k = l; k < n; k++) {
-          const double t = A_(i, k) * is;
-          s += t * t;
+        FOR9(k) if (k >= l && k < n) {
+          row[k] *= is;
+          s += row[k] * row[k];
         }
         f = A_(i, l) * is;
         g = f >= 0 ? -sqrt(s) : sqrt(s);
         h = f * g - s;
         const double ih = 1.0 / h;
-        // the scaled row i (with f - g at l) and rv1 = row / h, in every lane
-        for (int k = l; k < n; k++) rv1[k] = (k == l ? f - g : A_(i, k) * is) * ih;
-        GSYNC();
-        for (int k = l + lane; k < n; k += G) A_(i, k) = k == l ? f - g : A_(i, k) * is;
-        GSYNC();
+        FOR9(k) if (k == l) row[k] = f - g;
+        double rk[9];  // rv1 = the scaled row / h, in every lane
+        FOR9(k) {
+          rk[k] = row[k] * ih;
+          if (k >= l && k < n) rv1[k] = rk[k];
+        }
         for (int j = l + lane; j < m; j += G) {
           double sj = 0.0;
-          for (int k = l; k < n; k++) sj += A_(j, k) * A_(i, k);
-          for (int k = l; k < n; k++) A_(j, k) += sj * rv1[k];
+          FOR9(k) if (k >= l && k < n) sj += A_(j, k) * row[k];
+          FOR9(k) if (k >= l && k < n) A_(j, k) += sj * rk[k];
         }
         GSYNC();
-        for (int k = l + lane; k < n; k += G) A_(i, k) *= scale;
-        GSYNC();
+        FOR9(k) if (k >= l && k < n && ((k - l) & (G - 1)) == lane) A_(i, k) = row[k] * scale;
       }
     }
     const double t = fabs(w[i]) + fabs(rv1[i]);
     if (anorm < t) anorm = t;
   }
+  GSYNC();
+  // Accumulation of the left-hand transformations.  Column i is read into
+  // registers before anything changes it; the lane that owns column j zeroes
+  // A(i, j) and updates the column, so only the new column i needs a
+  // synchronisation before the next step reads it.
   for (int i = n - 1; i >= 0; i--) {
     l = i + 1;
     g = w[i];
+    double col[9];
+    FOR9(k) col[k] = (k >= i && k < m) ? A_(k, i) : 0.0;
+    const double aii = A_(i, i);
     for (int j = l + lane; j < n; j += G) A_(i, j) = 0.0;
-    GSYNC();
     if (g != 0.0) {
       g = 1.0 / g;
-      const double iaii = 1.0 / A_(i, i);
+      const double iaii = 1.0 / aii;
       for (int j = l + lane; j < n; j += G) {
         double sj = 0.0;
-        for (int k = l; k < m; k++) sj += A_(k, i) * A_(k, j);
+        FOR9(k) if (k >= l && k < m) sj += col[k] * A_(k, j);
         const double fj = (sj * iaii) * g;
-        for (int k = i; k < m; k++) A_(k, j) += fj * A_(k, i);
+        FOR9(k) if (k >= i && k < m) A_(k, j) += fj * col[k];
       }
-      GSYNC();
-      for (int j = i + lane; j < m; j += G) A_(j, i) *= g;
+      GSYNC();  // every lane has read column i
+      // A(k, i) * g, then + 1 on the diagonal: two roundings, as the
+      // reference's separate statements make them
+      FOR9(k) if (k >= i && k < m && ((k - i) & (G - 1)) == lane)
+        A_(k, i) = k == i ? __dadd_rn(__dmul_rn(col[k], g), 1.0) : __dmul_rn(col[k], g);
     } else {
-      for (int j = i + lane; j < m; j += G) A_(j, i) = 0.0;
+      GSYNC();
+      FOR9(k) if (k >= i && k < m && ((k - i) & (G - 1)) == lane) A_(k, i) = k == i ? 1.0 : 0.0;
     }
-    GSYNC();
-    if (lane == 0) A_(i, i) += 1.0;
     GSYNC();
   }
   // QR sweeps: each rotation touches the lane's own rows only, so the lanes
@@ -1645,17 +1723,40 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
       g = pythag_d(f, 1.0);
       f = ((x - z) * (x + z) + h * (y / (f + (f >= 0.0 ? g : -g)) - h)) / x;
       c = s = 1.0;
+      // each rotation is applied to the lane's rows one step late, beside
+      // the next rotation's scalar chain, with the rows' column j + 1 carried
+      // in registers (as in gr_svd_u)
+      constexpr int R = (9 + G - 1) / G;  // rows per lane
+      double cy[R];
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (lane + r * G < m) cy[r] = A_(lane + r * G, l);
+      double pc = 0.0, ps = 0.0;
+      double gi = rv1[l + 1], yi = w[l + 1];
       for (int j = l; j <= nm; j++) {
         const int i = j + 1;
-        g = rv1[i];
-        y = w[i];
+        g = gi;
+        y = yi;
+        if (i < k) {
+          gi = rv1[i + 1];
+          yi = w[i + 1];
+        }
+        if (j > l) {
+#pragma unroll
+          for (int r = 0; r < R; r++)
+            if (lane + r * G < m) {
+              const int jj = lane + r * G;
+              const double yy = cy[r], zz = A_(jj, j);
+              A_(jj, j - 1) = yy * pc + zz * ps;
+              cy[r] = zz * pc - yy * ps;
+            }
+        }
         h = s * g;
         g *= c;
         double iz;
         z = givens_radius<FAST>(f, h, iz);
         rv1[j] = z;
-        c = f * iz;
-        s = h * iz;
+        chase_cs<FAST>(f, h, z, iz, c, s);
         f = x * c + g * s;
         g = g * c - x * s;
         h = y * s;
@@ -1668,12 +1769,17 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
         }
         f = c * g + s * y;
         x = c * y - s * g;
-        for (int jj = lane; jj < m; jj += G) {
-          const double yy = A_(jj, j), zz = A_(jj, i);
-          A_(jj, j) = yy * c + zz * s;
-          A_(jj, i) = zz * c - yy * s;
-        }
+        pc = c;
+        ps = s;
       }
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (lane + r * G < m) {
+          const int jj = lane + r * G;
+          const double yy = cy[r], zz = A_(jj, k);
+          A_(jj, nm) = yy * pc + zz * ps;
+          A_(jj, k) = zz * pc - yy * ps;
+        }
       rv1[l] = 0.0;
       rv1[k] = f;
       w[k] = x;
@@ -1681,6 +1787,7 @@ __device__ __noinline__ int gr_svd_u_grp(double *a, int n, double *w, int lane, 
   }
   GSYNC();
   return hit;
+#undef FOR9
 #undef GSYNC
 #undef A_
 }
@@ -1879,8 +1986,7 @@ __device__ __forceinline__ int gr_svd_u9(double (&A)[9][9], double (&w)[9]) {
           double iz;
           z = givens_radius<FAST>(f, h, iz);
           rv1[j] = z;
-          c = f * iz;
-          s = h * iz;
+          chase_cs<FAST>(f, h, z, iz, c, s);
           f = x * c + gq * s;
           gq = gq * c - x * s;
           h = y * s;

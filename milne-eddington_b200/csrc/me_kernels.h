@@ -172,6 +172,11 @@ cudaError_t launch_voigt(int precision, const DevPlan &P, const double *d_nu, co
                          long long n, double *d_H, double *d_L, cudaStream_t st);
 cudaError_t launch_svd(const double *d_a, long long nmat, int n, double *d_u, double *d_w,
                        double *d_v, int *d_hits, cudaStream_t st);
+// The trial-step solve's U-only decomposition (no V) with `lanes` lanes per
+// matrix (1, 2, 4, 8, 16, 32) and the Givens rotations' form (fast: from one
+// reciprocal square root, as FP32 plans run it).
+cudaError_t launch_svd_u(const double *d_a, long long nmat, int n, int lanes, int fast,
+                         double *d_u, double *d_w, int *d_hits, cudaStream_t st);
 cudaError_t launch_init_guess(const DevPlan &P, const double *d_prof, long long npix,
                               double *d_guess, double *d_extra, int *d_status, cudaStream_t st);
 // Queue order of a learned start: pixels by descending misfit of their run -1

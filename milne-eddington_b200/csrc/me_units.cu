@@ -377,6 +377,68 @@ cudaError_t launch_svd(const double *d_a, long long nmat, int n, double *d_u, do
   return cudaGetLastError();
 }
 
+// The trial-step solve's U-only decomposition (gr_svd_u, gr_svd_u_grp) of
+// nmat n x n matrices: G = 1, one thread per matrix in a column of shared
+// memory (stride 32), as svd_kernel of the rounds holds it; G > 1, a group of
+// G lanes per matrix, row-major in shared memory, as svd_grp_kernel and the
+// tail kernel hold it.  Blocks of 32 threads.
+template <int G, bool FAST>
+__global__ void __launch_bounds__(32) svd_u_kernel(const double *a, long long nmat, int n,
+                                                   double *u, double *w, int *limit_hits) {
+  constexpr int kPer = 32 / G;  // matrices per block
+  constexpr int kWords = G == 1 ? 99 * 32 : kPer * 81;
+  __shared__ double sm[kWords];
+  const int t = threadIdx.x;
+  const long long i = blockIdx.x * (long long)kPer + t / G;
+  if (i >= nmat) return;  // uniform across each group
+  const int nn = n * n;
+  int hit;
+  if constexpr (G == 1) {
+    double *am = sm + t, *wm = sm + 81 * 32 + t, *rv = sm + 90 * 32 + t;
+    for (int k = 0; k < nn; k++) am[k * 32] = a[i * nn + k];
+    hit = gr_svd_u<32, FAST>(am, n, wm, rv);
+    for (int k = 0; k < nn; k++) u[i * nn + k] = am[k * 32];
+    for (int k = 0; k < n; k++) w[i * n + k] = wm[k * 32];
+  } else {
+    const int lane = t % G;
+    const unsigned mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (t & ~(G - 1)));
+    double *am = sm + (t / G) * 81;
+    for (int k = lane; k < nn; k += G) am[k] = a[i * nn + k];
+    __syncwarp(mask);
+    double wl[9];
+    hit = gr_svd_u_grp<G, FAST>(am, n, wl, lane, mask);
+    for (int k = lane; k < nn; k += G) u[i * nn + k] = am[k];
+    if (lane == 0)
+      for (int k = 0; k < n; k++) w[i * n + k] = wl[k];
+  }
+  if (hit && limit_hits && (G == 1 || t % G == 0)) atomicAdd(limit_hits, 1);
+}
+
+template <int G>
+static void launch_svd_u_g(const double *d_a, long long nmat, int n, int fast, double *d_u,
+                           double *d_w, int *d_hits, cudaStream_t st) {
+  const unsigned g = (unsigned)((nmat + 32 / G - 1) / (32 / G));
+  if (fast)
+    svd_u_kernel<G, true><<<g, 32, 0, st>>>(d_a, nmat, n, d_u, d_w, d_hits);
+  else
+    svd_u_kernel<G, false><<<g, 32, 0, st>>>(d_a, nmat, n, d_u, d_w, d_hits);
+}
+
+cudaError_t launch_svd_u(const double *d_a, long long nmat, int n, int lanes, int fast,
+                         double *d_u, double *d_w, int *d_hits, cudaStream_t st) {
+  if (nmat <= 0) return cudaSuccess;
+  switch (lanes) {
+    case 1: launch_svd_u_g<1>(d_a, nmat, n, fast, d_u, d_w, d_hits, st); break;
+    case 2: launch_svd_u_g<2>(d_a, nmat, n, fast, d_u, d_w, d_hits, st); break;
+    case 4: launch_svd_u_g<4>(d_a, nmat, n, fast, d_u, d_w, d_hits, st); break;
+    case 8: launch_svd_u_g<8>(d_a, nmat, n, fast, d_u, d_w, d_hits, st); break;
+    case 16: launch_svd_u_g<16>(d_a, nmat, n, fast, d_u, d_w, d_hits, st); break;
+    case 32: launch_svd_u_g<32>(d_a, nmat, n, fast, d_u, d_w, d_hits, st); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_order_by_key(const unsigned char *d_key, long long n, int *d_hist,
                                 long long *d_order, cudaStream_t st, long long base) {
   if (n <= 0) return cudaSuccess;

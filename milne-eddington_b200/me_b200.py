@@ -139,7 +139,7 @@ EXPORTED = [
     "me_config_parse_text", "me_plan_create", "me_plan_destroy", "me_plan_get_facts",
     "me_plan_get_carry_chisq", "me_plan_set_carry_chisq", "me_plan_grid", "me_plan_set_grid",
     "me_invert_batch", "me_invert_batch_device", "me_synthesize", "me_synthesize_device",
-    "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_init_guess", "me_svd_device",
+    "me_synthesize_jacobian", "me_faddeeva", "me_svd", "me_svd_u", "me_init_guess", "me_svd_device", "me_svd_u_device",
     "me_synthesize_jacobian_device", "me_plan_window", "me_plan_set_window",
     "me_invert_batch_device_noalloc", "me_plan_tail_slots", "me_plan_set_tail_slots",
     "me_plan_set_profiling", "me_plan_max_group", "me_plan_set_max_group",
@@ -326,6 +326,11 @@ def lib() -> ctypes.CDLL:
         L.me_faddeeva.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, ctypes.c_long, _D, _D,
                                   ctypes.c_int]
         L.me_svd.argtypes = [_D, ctypes.c_long, ctypes.c_int, _D, _D, _D, ctypes.c_int]
+        L.me_svd_u.argtypes = [_D, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D,
+                               _D, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.me_svd_u_device.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]
         L.me_svd_device.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.me_synthesize_jacobian_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p,
@@ -750,6 +755,28 @@ def svd(a: np.ndarray, device: int = 0):
     w = np.zeros((nmat, n))
     _check(lib().me_svd(_ptr(a), nmat, n, _ptr(u), _ptr(w), _ptr(v), device), "me_svd")
     return u, w, v
+
+
+def svd_u_device(d_a: int, nmat: int, n: int, d_u: int, d_w: int, lanes: int = 1,
+                 fast: bool = False, stream: int = 0):
+    _check(lib().me_svd_u_device(ctypes.c_void_p(d_a), nmat, n, lanes, 1 if fast else 0,
+                                 ctypes.c_void_p(d_u), ctypes.c_void_p(d_w),
+                                 ctypes.c_void_p(stream) if stream else None), "me_svd_u_device")
+
+
+def svd_u(a: np.ndarray, lanes: int = 1, fast: bool = False, device: int = 0):
+    """U and w of the inversion's trial-step decomposition (no V) of each
+    n x n matrix of a [nmat, n, n], with `lanes` lanes per matrix and the
+    Givens rotations' fast form (FP32 plans) or the reference's; returns
+    (u, w, number of matrices that hit the 50-sweep limit)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    nmat, n, _ = a.shape
+    u = np.zeros_like(a)
+    w = np.zeros((nmat, n))
+    hits = ctypes.c_int(0)
+    _check(lib().me_svd_u(_ptr(a), nmat, n, lanes, 1 if fast else 0, _ptr(u), _ptr(w),
+                          ctypes.byref(hits), device), "me_svd_u")
+    return u, w, hits.value
 
 
 def _fptr(a: np.ndarray):

@@ -118,6 +118,51 @@ def test_svd_smaller_orders():
             np.testing.assert_allclose((u[i] * w[i]) @ v[i].T, a[i], atol=1e-12)
 
 
+def _svd_u_inputs():
+    """The reference's golden SVD inputs, plus the matrices the trial steps
+    decompose: normal matrices J^T J of random Jacobians (first trials) and
+    the orthogonal U factors of earlier decompositions (later trials), at the
+    full order 9 and at 5 (four parameters fixed)."""
+    rng = np.random.default_rng(11)
+    out = [np.asarray(load("svd")["a"], dtype=np.float64)]
+    for n in (9, 5):
+        j = rng.normal(size=(64, 240, n)) * np.logspace(0, 2, n)
+        h = np.einsum("mki,mkj->mij", j, j)
+        q, _ = np.linalg.qr(rng.normal(size=(64, n, n)))
+        out += [h, q]
+    return out
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_svd_u_lanes_and_forms(fast):
+    """The U-only decomposition of the trial-step solve (one thread, the
+    lane-split groups, the tail kernel's warp) against the full decomposition
+    me_svd runs.  An orthogonal input (the later trials' U factors) has all
+    singular values 1 and no unique U: the last bit of any operation picks
+    another one, so there U is checked for orthogonality only.  Elsewhere U
+    and w agree with me_svd's to rounding, whatever the lanes, up to the sign
+    of a column (a QR sweep more or less, which rounding decides, can turn a
+    rotation by pi); fast: the FP32 plans' Givens radius from one reciprocal
+    square root (two ulps per rotation)."""
+    for a in _svd_u_inputs():
+        n = a.shape[1]
+        u_ref, w_ref, _ = me_b200.svd(a)
+        scale = np.abs(a).max(axis=(1, 2))
+        ortho = np.ptp(w_ref, axis=1) < 1e-8
+        # rounding moves a column by about eps * |a| / (gap to its neighbours)
+        tol_u = 1e-9 if fast else 1e-10
+        for lanes in (1, 2, 4, 8, 16, 32):
+            u, w, hits = me_b200.svd_u(a, lanes=lanes, fast=fast)
+            assert hits == 0
+            assert np.max(np.abs(w - w_ref) / scale[:, None]) < 1e-13, lanes
+            eye = np.einsum("mki,mkj->mij", u, u)
+            assert np.max(np.abs(eye - np.eye(n))) < 1e-13, lanes
+            if np.any(~ortho):
+                ug, ur = u[~ortho], u_ref[~ortho]
+                sign = np.sign(np.sum(ug * ur, axis=1))[:, None, :]
+                assert np.max(np.abs(ug * sign - ur)) < tol_u, lanes
+
+
 @pytest.mark.parametrize("case", CASES + ["fe15648_widened", "fe15648_run2_nr"])
 def test_init_guess_vs_reference(case):
     f = load(case)
