@@ -55,3 +55,21 @@ def test_no_cpu_fallback_without_gpu():
     with pytest.raises(me_b200.MeError) as e:
         me_b200.faddeeva(6, np.zeros(3), np.ones(3))
     assert e.value.status == -5
+
+
+def test_svd_u_rejects_bad_arguments_before_the_device():
+    """The U-only decomposition's unit entry point checks its order and lane
+    count before it looks for a device (ME_ERR_ARG), and without a GPU has no
+    CPU path (ME_ERR_NODEVICE)."""
+    a = np.eye(9)[None].copy()
+    for kw in ({"lanes": 3}, {"lanes": 64}):
+        with pytest.raises(me_b200.MeError) as e:
+            me_b200.svd_u(a, **kw)
+        assert e.value.status == -1 and "lanes" in str(e.value)
+    with pytest.raises(me_b200.MeError) as e:
+        me_b200.svd_u(np.eye(10)[None].copy())
+    assert e.value.status == -1
+    if not _has_gpu():
+        with pytest.raises(me_b200.MeError) as e:
+            me_b200.svd_u(a, lanes=4)
+        assert e.value.status == -5
