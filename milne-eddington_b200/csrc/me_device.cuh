@@ -1336,9 +1336,11 @@ static __device__ __noinline__ int gr_svd(double *a, int n, double *w, double *v
 // The same Golub-Reinsch decomposition producing U and w only (no V): the
 // Householder reduction, the accumulation of the left transformations and the
 // implicit-shift QR sweeps of gr_svd with every operation on V left out.  The
-// operations on U and w are gr_svd's own (V's loops only overwrite scratch
-// scalars that are reassigned before their next use), so U and w come out
-// identical.  Matrix element (i, j) lives at a[(i * n + j) * STR], w[i] at
+// operations on U and w are gr_svd's own, in its order (V's loops only
+// overwrite scratch scalars that are reassigned before their next use); the
+// compiler may contract multiply-adds differently in the two functions, so U
+// and w agree with gr_svd's to rounding (me_svd_u against me_svd in the unit
+// tests).  Matrix element (i, j) lives at a[(i * n + j) * STR], w[i] at
 // w[i * STR], so one thread's matrix can sit in a column of shared memory.
 template <int STR, bool FAST = false>
 __device__ __noinline__ int gr_svd_u(double *a, int n, double *w, double *rv1) {
