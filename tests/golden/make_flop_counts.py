@@ -44,66 +44,69 @@ def counts(vec):
 
 
 def main(npix=96):
-    L = ob.oracle_lib()
-    L.meo_count_synth.argtypes = [ctypes.c_void_p, D, ctypes.c_int, D]
-    L.meo_count_svd_solve.argtypes = [D, D, ctypes.c_int, ctypes.c_double, D]
-    out = {}
-    for name in me_maps.WORKLOADS:
-        lam = me_maps.wavelengths(name)
-        nl = lam.size
-        cfg = me_b200.parse_config_text(me_maps.control_text(name, precision="FP64"))
-        o = ob.Oracle(cfg, lam)
-        par = me_maps.draw_parameters(name, npix, 77)
-        prof = me_maps.add_noise(o.synth_many(par), 1e-3, 77)
-        res = o.invert(prof)
-        visited = []
-        for i in range(npix):
-            st, g, e = o.init_guess(prof[i])
-            if st == 0:
-                visited.append((g, e))
-            if res[i, 9] > 0:
-                visited.append((res[i, :9], e))
-        fwd = np.zeros(8)
-        der = np.zeros(8)
-        svd1 = np.zeros(8)
-        svd2 = np.zeros(8)
-        for p, e in visited:
-            c = np.zeros(8)
-            L.meo_count_synth(o.h, np.ascontiguousarray(p).ctypes.data_as(D), 0, c.ctypes.data_as(D))
-            fwd += c
-            L.meo_count_synth(o.h, np.ascontiguousarray(p).ctypes.data_as(D), 1, c.ctypes.data_as(D))
-            der += c
-            H, g, _ = o.normal_equations(prof[0], p, e[4], e[0])
-            H = np.ascontiguousarray(H)
-            g = np.ascontiguousarray(g)
-            L.meo_count_svd_solve(H.ctypes.data_as(D), g.ctypes.data_as(D), 9, 1e-6,
-                                  c.ctypes.data_as(D))
-            svd1 += c
-            u, w, v, _ = ob.oracle_svd(H)
-            u = np.ascontiguousarray(u)
-            L.meo_count_svd_solve(u.ctypes.data_as(D), g.ctypes.data_as(D), 9, 1e-6,
-                                  c.ctypes.data_as(D))
-            svd2 += c
-        n = len(visited)
-        fwd /= n * nl
-        der /= n * nl
-        svd1 /= n
-        svd2 /= n
-        npar = 9
-        normal = {"add": 4 * (npar * (npar + 1) // 2) + 8 * npar, "mul": 8 * (npar * (npar + 1) // 2)
-                  + 8 * npar}  # s += iv*Ji*Jj per Stokes; s -= iv*Ji*(syn-obs)
-        loss = {"add": 8.0, "mul": 8.0}  # diff, diff*diff*iv, += per Stokes
-        out[name] = {"nl": nl, "samples": n,
-                     "forward_per_lambda": counts(fwd),
-                     "jacobian_per_lambda": counts(der),
-                     "normal_equations_per_lambda": normal,
-                     "loss_per_lambda": loss,
-                     "svd_solve_normal_matrix": counts(svd1),
-                     "svd_solve_orthogonal": counts(svd2)}
+    out = {name: workload_counts(name, npix) for name in me_maps.WORKLOADS}
     path = os.path.join(HERE, "flop_counts.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", path)
+
+
+def workload_counts(name, npix=96):
+    """The per-event counts of one workload (the entry flop_counts.json holds)."""
+    L = ob.oracle_lib()
+    L.meo_count_synth.argtypes = [ctypes.c_void_p, D, ctypes.c_int, D]
+    L.meo_count_svd_solve.argtypes = [D, D, ctypes.c_int, ctypes.c_double, D]
+    lam = me_maps.wavelengths(name)
+    nl = lam.size
+    cfg = me_b200.parse_config_text(me_maps.control_text(name, precision="FP64"))
+    o = ob.Oracle(cfg, lam)
+    par = me_maps.draw_parameters(name, npix, 77)
+    prof = me_maps.add_noise(o.synth_many(par), 1e-3, 77)
+    res = o.invert(prof)
+    visited = []
+    for i in range(npix):
+        st, g, e = o.init_guess(prof[i])
+        if st == 0:
+            visited.append((g, e))
+        if res[i, 9] > 0:
+            visited.append((res[i, :9], e))
+    fwd = np.zeros(8)
+    der = np.zeros(8)
+    svd1 = np.zeros(8)
+    svd2 = np.zeros(8)
+    for p, e in visited:
+        c = np.zeros(8)
+        L.meo_count_synth(o.h, np.ascontiguousarray(p).ctypes.data_as(D), 0, c.ctypes.data_as(D))
+        fwd += c
+        L.meo_count_synth(o.h, np.ascontiguousarray(p).ctypes.data_as(D), 1, c.ctypes.data_as(D))
+        der += c
+        H, g, _ = o.normal_equations(prof[0], p, e[4], e[0])
+        H = np.ascontiguousarray(H)
+        g = np.ascontiguousarray(g)
+        L.meo_count_svd_solve(H.ctypes.data_as(D), g.ctypes.data_as(D), 9, 1e-6,
+                              c.ctypes.data_as(D))
+        svd1 += c
+        u, w, v, _ = ob.oracle_svd(H)
+        u = np.ascontiguousarray(u)
+        L.meo_count_svd_solve(u.ctypes.data_as(D), g.ctypes.data_as(D), 9, 1e-6,
+                              c.ctypes.data_as(D))
+        svd2 += c
+    n = len(visited)
+    fwd /= n * nl
+    der /= n * nl
+    svd1 /= n
+    svd2 /= n
+    npar = 9
+    normal = {"add": 4 * (npar * (npar + 1) // 2) + 8 * npar, "mul": 8 * (npar * (npar + 1) // 2)
+              + 8 * npar}  # s += iv*Ji*Jj per Stokes; s -= iv*Ji*(syn-obs)
+    loss = {"add": 8.0, "mul": 8.0}  # diff, diff*diff*iv, += per Stokes
+    return {"nl": nl, "samples": n,
+            "forward_per_lambda": counts(fwd),
+            "jacobian_per_lambda": counts(der),
+            "normal_equations_per_lambda": normal,
+            "loss_per_lambda": loss,
+            "svd_solve_normal_matrix": counts(svd1),
+            "svd_solve_orthogonal": counts(svd2)}
 
 
 if __name__ == "__main__":
