@@ -65,6 +65,15 @@ struct DevBuf {
   }
 };
 
+// A DevBuf that frees its memory when the scope ends, on every return path
+// (the unit entry points' staging buffers; CK returns early on an error).
+struct ScopedBuf : DevBuf {
+  ScopedBuf() = default;
+  ScopedBuf(const ScopedBuf &) = delete;
+  ScopedBuf &operator=(const ScopedBuf &) = delete;
+  ~ScopedBuf() { release(); }
+};
+
 // Alg-916 constants of Faddeeva_init (Src/FADDEEVA.c:406-436) and the region
 // row of the accuracy table (Src/FADDEEVA.c:471-477).
 void fill_voigt_consts(me::DevPlan &P, int nfigures) {
@@ -522,7 +531,7 @@ extern "C" int me_order_by_key(int device, const unsigned char *keys, long n, lo
     return fail(ME_ERR_NODEVICE, "no CUDA device");
   if (device < 0 || device >= nd) return fail(ME_ERR_ARG, "device out of range");
   CK(cudaSetDevice(device));
-  DevBuf dk, dh, dord;
+  ScopedBuf dk, dh, dord;
   CK(dk.ensure((size_t)n));
   CK(dh.ensure((size_t)me::kOrderBuckets * me::kOrderBlocks * sizeof(int)));
   CK(dord.ensure((size_t)n * sizeof(long long)));
@@ -1310,7 +1319,7 @@ extern "C" int me_synthesize_jacobian(me_plan *p, const double *par, long npix, 
   if (npix == 0) return ME_OK;
   CK(cudaSetDevice(p->device));
   const size_t n = (size_t)npix, nl = (size_t)p->P.nl;
-  DevBuf dp, dprof, djac;
+  ScopedBuf dp, dprof, djac;
   CK(dp.ensure(n * 9 * sizeof(double)));
   CK(dprof.ensure(n * 4 * nl * sizeof(double)));
   if (jac) CK(djac.ensure(n * 36 * nl * sizeof(double)));
@@ -1352,7 +1361,7 @@ extern "C" int me_faddeeva(int nfigures, int precision, const double *nu, const 
   me::DevPlan P;
   memset(&P, 0, sizeof(P));
   fill_voigt_consts(P, nfigures);
-  DevBuf dn, da, dh, dl;
+  ScopedBuf dn, da, dh, dl;
   const size_t b = (size_t)n * sizeof(double);
   CK(dn.ensure(b));
   CK(da.ensure(b));
@@ -1381,7 +1390,7 @@ extern "C" int me_faddeeva_weideman(const double *nu, const double *a, long n, d
   memset(&P, 0, sizeof(P));
   fill_voigt_consts(P, 6);
   P.faddeeva = 1;
-  DevBuf dn, da, dh, dl;
+  ScopedBuf dn, da, dh, dl;
   const size_t b = (size_t)n * sizeof(double);
   CK(dn.ensure(b));
   CK(da.ensure(b));
@@ -1403,7 +1412,7 @@ extern "C" int me_svd(const double *a, long nmat, int n, double *u, double *w, d
   if (st) return st;
   if (nmat == 0) return ME_OK;
   const size_t mb = (size_t)nmat * n * n * sizeof(double), wb = (size_t)nmat * n * sizeof(double);
-  DevBuf da, du, dw, dv, dh;
+  ScopedBuf da, du, dw, dv, dh;
   CK(da.ensure(mb));
   CK(du.ensure(mb));
   CK(dv.ensure(mb));
@@ -1434,7 +1443,7 @@ extern "C" int me_svd_u(const double *a, long nmat, int n, int lanes, int fast, 
   if (limit_hits) *limit_hits = 0;
   if (nmat == 0) return ME_OK;
   const size_t mb = (size_t)nmat * n * n * sizeof(double), wb = (size_t)nmat * n * sizeof(double);
-  DevBuf da, du, dw, dh;
+  ScopedBuf da, du, dw, dh;
   CK(da.ensure(mb));
   CK(du.ensure(mb));
   CK(dw.ensure(wb));
@@ -1460,7 +1469,7 @@ extern "C" int me_init_guess(me_plan *p, const double *prof, long npix, double *
   if (npix == 0) return ME_OK;
   CK(cudaSetDevice(p->device));
   const size_t n = (size_t)npix, nl = (size_t)p->P.nl;
-  DevBuf dp, dg, de, ds;
+  ScopedBuf dp, dg, de, ds;
   CK(dp.ensure(n * 4 * nl * sizeof(double)));
   CK(dg.ensure(n * 9 * sizeof(double)));
   CK(de.ensure(n * 5 * sizeof(double)));
