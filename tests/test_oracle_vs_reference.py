@@ -69,3 +69,30 @@ def test_reference_parity_restarts_nr_stream():
 def test_reference_parity_fe6302_weights():
     out = run_case("fe6302_2048x1024", 96, {"num_run": "1"}, 5)
     assert out["exact"] and out["carry"]
+
+
+def test_reference_parity_fixed_hmi_restarts():
+    """A fixed parameter (npar 8), HMI_REF and Nfigures 4, with random
+    restarts from the reference's NR stream, on a fresh map."""
+    out = run_case("fe15648_64x64", 96, {"Bmod_fixed": "YES", "HMI_REF": "YES",
+                                         "Btheta_Regularization": "NO", "Nfigures": "4",
+                                         "num_run": "2", "chisq_criteria": "0.5"}, 4242)
+    assert out["exact"] and out["carry"]
+
+
+def test_reference_parity_regularisations_restarts():
+    """Regularisation of eta0 and the Doppler width beside the default theta
+    term (the carried LM chi^2 decides the ratio), Nfigures 5, restarts."""
+    out = run_case("fe15648_64x64", 96, {"Eta_Regularization": "YES, 10.0, 2e-3",
+                                         "Dopp_Regularization": "YES, 60, 1e-3",
+                                         "Nfigures": "5", "num_run": "2",
+                                         "chisq_criteria": "0.5"}, 777)
+    assert out["exact"] and out["carry"]
+
+
+def test_reference_parity_bench_configuration():
+    """The headline map's configuration (num_run 5, chisq_criteria 1.5,
+    widened Doppler and damping bounds) on a fresh sample."""
+    out = run_case("fe15648_1024x1024", 48, {"Bounds_Dopp": "100, 400",
+                                              "Bounds_Damp": "0.05, 1.0"}, 99)
+    assert out["exact"] and out["carry"]
